@@ -1,0 +1,489 @@
+// assemple_system_matrix on the device (src/pb_class.cpp:2053-2159): the
+// box-method operator of bimpp's bim3a_laplacian_frac + bim3a_reaction_frac
+// (or bim3a_reaction with a Stern layer) + bim3a_rhs + bim3a_dirichlet_bc,
+// written straight into a SELL-C-sigma matrix.
+//
+// Each matrix row is gathered by one thread from the node's incidence list
+// (octant, corner), so no atomics touch the values.  Per incidence the thread
+// rebuilds the octant's local coefficients it needs (the corner's 3 edge
+// conductances, the lumped reaction, V/8 * rho) and spreads them over the
+// independent nodes behind each local corner (a hanging corner over its parents
+// with weight 1/num_parents: A = P^T K P).  Pass 1 counts each row's distinct
+// columns, the SELL layout is derived from those lengths (rows sorted by length
+// inside windows of sigma rows, slices of C rows padded to a multiple of 4
+// columns), pass 2 writes values and columns in SELL numbering.  Dirichlet
+// nodes become identity rows and are eliminated from the other rows into the
+// right-hand side, which keeps the matrix symmetric.
+#include <algorithm>
+#include <cub/cub.cuh>
+
+#include "pbgpu_internal.cuh"
+
+namespace pbgpu {
+
+struct AsmView {
+  const int64_t* inc_ptr;
+  const uint32_t* inc;
+  const int4* oct;
+  const int32_t* oct_nodes;
+  const int4* hang_par;
+  const int8_t* hang_np;
+  const double* eps;
+  const double* react;
+  const double* react_cell;
+  const double* rho;
+  const double* frac;
+  const int32_t* border_pos;
+  const uint8_t* dirichlet;
+  const double* gval;
+  int64_t n;
+  int stern;
+  double lo[3], len[3];
+};
+
+__device__ __forceinline__ double corner_val(const double* __restrict__ v, int32_t nd, const AsmView& A) {
+  if (nd < A.n) return v[nd];
+  const int64_t h = nd - A.n;
+  const int4 p = A.hang_par[h];
+  const int np = A.hang_np[h];
+  double t = 0.0;
+  t += v[p.x] / np;
+  t += v[p.y] / np;
+  if (np == 4) {
+    t += v[p.z] / np;
+    t += v[p.w] / np;
+  }
+  return t;
+}
+
+// Independent nodes behind node id nd, with weights.
+__device__ __forceinline__ int expand(int32_t nd, const AsmView& A, int32_t g[4], double w[4]) {
+  if (nd < A.n) {
+    g[0] = nd;
+    w[0] = 1.0;
+    return 1;
+  }
+  const int64_t h = nd - A.n;
+  const int4 p = A.hang_par[h];
+  const int np = A.hang_np[h];
+  g[0] = p.x;
+  g[1] = p.y;
+  g[2] = p.z;
+  g[3] = p.w;
+  const double wi = 1.0 / np;
+  for (int j = 0; j < 4; ++j) w[j] = wi;
+  return np;
+}
+
+// Small sorted (column, value) accumulator held by one thread.
+struct RowAcc {
+  int32_t col[kMaxRow];
+  double val[kMaxRow];
+  int m = 0;
+  bool overflow = false;
+  __device__ __forceinline__ void add(int32_t c, double v) {
+    int j = m - 1;
+    while (j >= 0 && col[j] > c) --j;
+    if (j >= 0 && col[j] == c) {
+      val[j] += v;
+      return;
+    }
+    if (m == kMaxRow) {
+      overflow = true;
+      return;
+    }
+    for (int k = m - 1; k > j; --k) {
+      col[k + 1] = col[k];
+      val[k + 1] = val[k];
+    }
+    col[j + 1] = c;
+    val[j + 1] = v;
+    ++m;
+  }
+};
+
+// Gather row i of A and its right-hand side entry (before Dirichlet handling).
+__device__ void gather_row(int64_t i, const AsmView& A, RowAcc& R, double& rhs) {
+  rhs = 0.0;
+  for (int64_t e = A.inc_ptr[i]; e < A.inc_ptr[i + 1]; ++e) {
+    const uint32_t t = A.inc[e];
+    const int64_t o = t >> 3;
+    const int a = (int)(t & 7);
+    const int4 q = A.oct[o];
+    const int32_t s = 1 << (kRootLog - q.w);
+    const int32_t qc[3] = {q.x, q.y, q.z};
+    double h[3];
+    for (int d = 0; d < 3; ++d) h[d] = coord(A.lo[d], A.len[d], qc[d] + s) - coord(A.lo[d], A.len[d], qc[d]);
+    const double area_h[3] = {h[1] * h[2] / h[0] * 0.25, h[0] * h[2] / h[1] * 0.25, h[0] * h[1] / h[2] * 0.25};
+    const double v8 = h[0] * h[1] * h[2] * 0.125;
+    const int32_t bp = A.border_pos[o];
+    const int32_t nda = A.oct_nodes[t];
+    const double wa = nda < A.n ? 1.0 : 1.0 / A.hang_np[nda - A.n];
+    const double ea = corner_val(A.eps, nda, A);
+    // the 3 edges at corner a, in ascending edge id (the order the local
+    // matrix accumulates them in)
+    int ed[3], ax[3];
+    for (int d = 0; d < 3; ++d) {
+      ed[d] = edge_of(a, d);
+      ax[d] = d;
+    }
+    for (int u = 0; u < 3; ++u)
+      for (int v = u + 1; v < 3; ++v)
+        if (ed[v] < ed[u]) {
+          int tmp = ed[u];
+          ed[u] = ed[v];
+          ed[v] = tmp;
+          tmp = ax[u];
+          ax[u] = ax[v];
+          ax[v] = tmp;
+        }
+    double cond[3], kaa = 0.0, wr = 1.0;
+    int32_t ndb[3];
+    for (int u = 0; u < 3; ++u) {
+      const int d = ax[u];
+      const int b = a ^ (1 << d);
+      ndb[u] = A.oct_nodes[8 * o + b];
+      const double eb = corner_val(A.eps, ndb[u], A);
+      const double f = bp >= 0 ? A.frac[12 * (int64_t)bp + ed[u]] : 0.5;
+      const bool first = ((a >> d) & 1) == 0;  // a is the edge's first node
+      const double c = first ? wha(ea, eb, f) * area_h[d] : wha(eb, ea, f) * area_h[d];
+      cond[u] = c;
+      kaa += c;
+      wr *= first ? fmin(1.0, 2.0 * f) : fmin(1.0, 2.0 * (1.0 - f));
+    }
+    if (A.stern)
+      kaa += A.react_cell[o] * v8;
+    else
+      kaa += corner_val(A.react, nda, A) * v8 * wr;
+    int32_t g[4];
+    double w[4];
+    int ng = expand(nda, A, g, w);
+    for (int j = 0; j < ng; ++j) R.add(g[j], wa * kaa * w[j]);
+    for (int u = 0; u < 3; ++u) {
+      ng = expand(ndb[u], A, g, w);
+      const double kab = 0.0 - cond[u];
+      for (int j = 0; j < ng; ++j) R.add(g[j], wa * kab * w[j]);
+    }
+    const double fc = v8 * corner_val(A.rho, nda, A);
+    rhs += wa * fc;
+  }
+}
+
+// Pass 1: number of stored columns of each row.
+__global__ void k_row_len(AsmView A, int32_t* __restrict__ rowlen, int* __restrict__ overflow) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  if (A.dirichlet[i]) {
+    rowlen[i] = 1;
+    return;
+  }
+  RowAcc R;
+  double rhs;
+  gather_row(i, A, R, rhs);
+  if (R.overflow) atomicExch(overflow, 1);
+  int m = 0;
+  for (int j = 0; j < R.m; ++j) m += A.dirichlet[R.col[j]] ? 0 : 1;
+  rowlen[i] = m;
+}
+
+struct SellOut {
+  const int64_t* slice_ptr;
+  const int32_t* slice_w;
+  const int32_t* iperm;
+  int32_t* scol;
+  double* sval;
+  double* b;
+  double* dinv;
+  int C;
+};
+
+__device__ __forceinline__ int64_t sell_index(const SellOut& S, int64_t p, int j) {
+  const int64_t sl = p / S.C;
+  const int lane = (int)(p % S.C);
+  return S.slice_ptr[sl] + (int64_t)(j >> 2) * 4 * S.C + lane * 4 + (j & 3);
+}
+
+// Pass 2: values, columns (SELL numbering), right-hand side, 1/diagonal.
+__global__ void k_row_fill(AsmView A, SellOut S) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const int64_t p = S.iperm[i];
+  const int W = S.slice_w[p / S.C];
+  int j = 0;
+  if (A.dirichlet[i]) {
+    const int64_t k = sell_index(S, p, j++);
+    S.scol[k] = (int32_t)p;
+    S.sval[k] = 1.0;
+    S.b[p] = A.gval[i];
+    S.dinv[p] = 1.0;
+  } else {
+    RowAcc R;
+    double rhs;
+    gather_row(i, A, R, rhs);
+    double diag = 1.0;
+    for (int u = 0; u < R.m; ++u) {
+      const int32_t cn = R.col[u];
+      if (A.dirichlet[cn]) {
+        rhs -= R.val[u] * A.gval[cn];
+        continue;
+      }
+      if (cn == i) diag = R.val[u];
+      const int64_t k = sell_index(S, p, j++);
+      S.scol[k] = S.iperm[cn];
+      S.sval[k] = R.val[u];
+    }
+    S.b[p] = rhs;
+    S.dinv[p] = 1.0 / diag;
+  }
+  for (; j < W; ++j) {
+    const int64_t k = sell_index(S, p, j);
+    S.scol[k] = (int32_t)p;
+    S.sval[k] = 0.0;
+  }
+}
+
+// Padding rows past n in the last slice.
+__global__ void k_pad_rows(SellOut S, int64_t n, int64_t n_pad) {
+  const int64_t p = n + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= n_pad) return;
+  const int W = S.slice_w[p / S.C];
+  for (int j = 0; j < W; ++j) {
+    const int64_t k = sell_index(S, p, j);
+    S.scol[k] = (int32_t)p;
+    S.sval[k] = 0.0;
+  }
+  S.b[p] = 0.0;
+  S.dinv[p] = 0.0;
+}
+
+// Dirichlet flags and values (src/pb_class.cpp:2113-2149, 3531-3571).
+__global__ void k_dirichlet(const int4* __restrict__ node_xyz, int64_t n, int bc, double3 lo, double3 len,
+                            const double4* __restrict__ atoms, int64_t na, double eps_in, double eps_out, double kappa,
+                            uint8_t* __restrict__ dir, double* __restrict__ gval) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 p = node_xyz[i];
+  const bool onb = bc != 0 && (p.w & 1);
+  dir[i] = onb;
+  double g = 0.0;
+  if (onb) {
+    const double x = coord(lo.x, len.x, p.x), y = coord(lo.y, len.y, p.y), z = coord(lo.z, len.z, p.z);
+    if (bc == 2) {
+      for (int64_t a = 0; a < na; ++a) {
+        const double4 A = atoms[a];
+        const double d = norm3d(A.x - x, A.y - y, A.z - z);
+        g += A.w * exp(-kappa * d) / (d * eps_out);
+      }
+    } else if (bc == 3) {
+      const double rs = 2.0;
+      const double pout = eps_out * (1.0 + kappa * rs), pin = eps_in * rs;
+      const double d = norm3d(x, y, z);
+      g = d <= rs ? 1.0 / (pout * rs) + (rs - d) / (pin * d) : exp(kappa * (rs - d)) / (d * pout);
+    }
+  }
+  gval[i] = g;
+}
+
+// Sort key for SELL-C-sigma: window, then longer rows first, then node id
+// (radix sort is stable, so equal keys keep node order).
+__global__ void k_sigma_keys(const int32_t* __restrict__ rowlen, int64_t n, int sigma, uint64_t* __restrict__ key,
+                             int32_t* __restrict__ id) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t L = (uint32_t)min(rowlen[i], 0xffff);
+  key[i] = ((uint64_t)(i / sigma) << 16) | (uint64_t)(0xffff - L);
+  id[i] = (int32_t)i;
+}
+
+__global__ void k_identity(int32_t* __restrict__ perm, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) perm[i] = (int32_t)i;
+}
+
+__global__ void k_iperm(const int32_t* __restrict__ perm, int64_t n, int32_t* __restrict__ iperm) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p < n) iperm[perm[p]] = (int32_t)p;
+}
+
+__global__ void k_slice_width(const int32_t* __restrict__ perm, const int32_t* __restrict__ rowlen, int64_t n,
+                              int64_t n_slices, int C, int32_t* __restrict__ w, int64_t* __restrict__ elems) {
+  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= n_slices) return;
+  int mx = 1;
+  for (int l = 0; l < C; ++l) {
+    const int64_t p = s * C + l;
+    if (p < n) mx = max(mx, rowlen[perm[p]]);
+  }
+  mx = (mx + 3) & ~3;
+  w[s] = mx;
+  elems[s] = (int64_t)mx * C;
+}
+
+int run_assemble(Context* c, const pbgpu_sell_opts* o) {
+  if (!c->have_markers) return c->fail(PBGPU_ERR_STATE, "assemble: create_markers has not run");
+  if (!c->have_density) return c->fail(PBGPU_ERR_STATE, "assemble: create_density_map has not run");
+  int C = (o && o->chunk > 0) ? o->chunk : 32;
+  int sigma = (o && o->sigma > 0) ? o->sigma : C;
+  if (C % 32 != 0 || C > 1024) return c->fail(PBGPU_ERR_ARG, "SELL chunk must be a multiple of 32, at most 1024");
+  if (sigma % C != 0 && sigma != 1) return c->fail(PBGPU_ERR_ARG, "SELL sigma must be 1 or a multiple of the chunk");
+  c->C = C;
+  c->sigma = sigma;
+  const int64_t n = c->n;
+  const double3 lo = make_double3(c->lo[0], c->lo[1], c->lo[2]);
+  const double3 len = make_double3(c->len[0], c->len[1], c->len[2]);
+  PBGPU_CUDA(c, c->dirichlet.alloc(n));
+  PBGPU_CUDA(c, c->gval.alloc(n));
+  k_dirichlet<<<grid_for(n, 128), 128, 0, c->stream>>>(c->node_xyz.get(), n, c->model.bc_type, lo, len,
+                                                        c->atoms.get(), c->na, c->eps_in, c->eps_out, c->kappa,
+                                                        c->dirichlet.get(), c->gval.get());
+  PBGPU_CUDA(c, cudaGetLastError());
+
+  AsmView A;
+  A.inc_ptr = c->inc_ptr.get();
+  A.inc = c->inc.get();
+  A.oct = c->oct.get();
+  A.oct_nodes = c->oct_nodes.get();
+  A.hang_par = c->hang_par.get();
+  A.hang_np = c->hang_np.get();
+  A.eps = c->eps.get();
+  A.react = c->react.get();
+  A.react_cell = c->model.stern_layer_surf == 1 ? c->react_cell.get() : nullptr;
+  A.rho = c->rho.get();
+  A.frac = c->frac.get();
+  A.border_pos = c->border_pos.get();
+  A.dirichlet = c->dirichlet.get();
+  A.gval = c->gval.get();
+  A.n = n;
+  A.stern = c->model.stern_layer_surf == 1;
+  for (int d = 0; d < 3; ++d) {
+    A.lo[d] = c->lo[d];
+    A.len[d] = c->len[d];
+  }
+
+  PBGPU_CUDA(c, c->rowlen.alloc(n));
+  DBuf<int> ovf;
+  PBGPU_CUDA(c, ovf.alloc(1));
+  PBGPU_CUDA(c, cudaMemsetAsync(ovf.get(), 0, sizeof(int), c->stream));
+  k_row_len<<<grid_for(n, 128), 128, 0, c->stream>>>(A, c->rowlen.get(), ovf.get());
+  PBGPU_CUDA(c, cudaGetLastError());
+  int h_ovf = 0;
+  PBGPU_CUDA(c, cudaMemcpyAsync(&h_ovf, ovf.get(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (h_ovf) return c->fail(PBGPU_ERR_CAPACITY, "assemble: a matrix row has more than kMaxRow columns");
+
+  // SELL-C-sigma permutation
+  const int64_t n_slices = (n + C - 1) / C, n_pad = n_slices * C;
+  PBGPU_CUDA(c, c->perm.alloc(n_pad));
+  PBGPU_CUDA(c, c->iperm.alloc(n_pad));
+  if (sigma > 1) {
+    DBuf<uint64_t> k0, k1;
+    DBuf<int32_t> id0;
+    PBGPU_CUDA(c, k0.alloc(n));
+    PBGPU_CUDA(c, k1.alloc(n));
+    PBGPU_CUDA(c, id0.alloc(n));
+    k_sigma_keys<<<grid_for(n, 256), 256, 0, c->stream>>>(c->rowlen.get(), n, sigma, k0.get(), id0.get());
+    PBGPU_CUDA(c, cudaGetLastError());
+    size_t bytes = 0;
+    PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0.get(), k1.get(), id0.get(), c->perm.get(), (int)n,
+                                                  0, 64, c->stream));
+    PBGPU_CUDA(c, ensure_tmp(c, bytes));
+    PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(c->tmp.get(), bytes, k0.get(), k1.get(), id0.get(), c->perm.get(),
+                                                  (int)n, 0, 64, c->stream));
+    PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  } else {
+    k_identity<<<grid_for(n, 256), 256, 0, c->stream>>>(c->perm.get(), n);
+    PBGPU_CUDA(c, cudaGetLastError());
+  }
+  k_iperm<<<grid_for(n, 256), 256, 0, c->stream>>>(c->perm.get(), n, c->iperm.get());
+  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_CUDA(c, c->slice_w.alloc(n_slices));
+  PBGPU_CUDA(c, c->slice_ptr.alloc(n_slices + 1));
+  DBuf<int64_t> elems;
+  PBGPU_CUDA(c, elems.alloc(n_slices + 1));
+  PBGPU_CUDA(c, cudaMemsetAsync(elems.get(), 0, (n_slices + 1) * sizeof(int64_t), c->stream));
+  k_slice_width<<<grid_for(n_slices, 128), 128, 0, c->stream>>>(c->perm.get(), c->rowlen.get(), n, n_slices, C,
+                                                                 c->slice_w.get(), elems.get());
+  PBGPU_CUDA(c, cudaGetLastError());
+  size_t bytes = 0;
+  PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, bytes, elems.get(), c->slice_ptr.get(), n_slices + 1, c->stream));
+  PBGPU_CUDA(c, ensure_tmp(c, bytes));
+  PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(c->tmp.get(), bytes, elems.get(), c->slice_ptr.get(), n_slices + 1,
+                                              c->stream));
+  int64_t total = 0;
+  PBGPU_CUDA(c, cudaMemcpyAsync(&total, c->slice_ptr.get() + n_slices, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                c->stream));
+  // nnz = sum of row lengths
+  DBuf<int64_t> nnz_d;
+  PBGPU_CUDA(c, nnz_d.alloc(1));
+  bytes = 0;
+  PBGPU_CUDA(c, cub::DeviceReduce::Sum(nullptr, bytes, c->rowlen.get(), nnz_d.get(), n, c->stream));
+  PBGPU_CUDA(c, ensure_tmp(c, bytes));
+  PBGPU_CUDA(c, cub::DeviceReduce::Sum(c->tmp.get(), bytes, c->rowlen.get(), nnz_d.get(), n, c->stream));
+  int64_t nnz = 0;
+  PBGPU_CUDA(c, cudaMemcpyAsync(&nnz, nnz_d.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->n_slices = n_slices;
+  c->sell_len = total;
+  c->nnz = nnz;
+  PBGPU_CUDA(c, c->scol.alloc(total));
+  PBGPU_CUDA(c, c->sval.alloc(total));
+  PBGPU_CUDA(c, c->b.alloc(n_pad));
+  PBGPU_CUDA(c, c->dinv.alloc(n_pad));
+  SellOut S{c->slice_ptr.get(), c->slice_w.get(), c->iperm.get(), c->scol.get(), c->sval.get(), c->b.get(),
+            c->dinv.get(), C};
+  k_row_fill<<<grid_for(n, 128), 128, 0, c->stream>>>(A, S);
+  PBGPU_CUDA(c, cudaGetLastError());
+  if (n_pad > n) {
+    k_pad_rows<<<grid_for(n_pad - n, 128), 128, 0, c->stream>>>(S, n, n_pad);
+    PBGPU_CUDA(c, cudaGetLastError());
+  }
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->have_system = true;
+  c->have_phi = false;
+  return PBGPU_OK;
+}
+
+// CSR (node order, ascending columns) of the assembled system, for parity checks.
+int export_system(Context* c, int64_t* nnz_out, int64_t* row_ptr, int32_t* col, double* val, double* rhs) {
+  if (!c->have_system) return c->fail(PBGPU_ERR_STATE, "get_system: assemble has not run");
+  if (nnz_out) *nnz_out = c->nnz;
+  if (!row_ptr && !col && !val && !rhs) return PBGPU_OK;
+  const int64_t n = c->n, n_pad = c->n_slices * c->C;
+  std::vector<int64_t> sp(c->n_slices + 1);
+  std::vector<int32_t> sw(c->n_slices), perm(n_pad), iperm(n_pad), rl(n), sc(c->sell_len);
+  std::vector<double> sv(c->sell_len), bb(n_pad);
+  PBGPU_CUDA(c, cudaMemcpyAsync(sp.data(), c->slice_ptr.get(), sp.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaMemcpyAsync(sw.data(), c->slice_w.get(), sw.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaMemcpyAsync(perm.data(), c->perm.get(), n * 4, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaMemcpyAsync(iperm.data(), c->iperm.get(), n * 4, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaMemcpyAsync(rl.data(), c->rowlen.get(), n * 4, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaMemcpyAsync(sc.data(), c->scol.get(), sc.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaMemcpyAsync(sv.data(), c->sval.get(), sv.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaMemcpyAsync(bb.data(), c->b.get(), n_pad * 8, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int C = c->C;
+  int64_t w = 0;
+  if (row_ptr) row_ptr[0] = 0;
+  std::vector<std::pair<int32_t, double>> row;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t p = iperm[i];
+    const int64_t s = p / C;
+    const int lane = (int)(p % C);
+    row.clear();
+    for (int j = 0; j < rl[i]; ++j) {
+      const int64_t k = sp[s] + (int64_t)(j >> 2) * 4 * C + lane * 4 + (j & 3);
+      row.push_back({perm[sc[k]], sv[k]});
+    }
+    std::sort(row.begin(), row.end());
+    for (auto& e : row) {
+      if (col) col[w] = e.first;
+      if (val) val[w] = e.second;
+      ++w;
+    }
+    if (row_ptr) row_ptr[i + 1] = w;
+    if (rhs) rhs[i] = bb[p];
+  }
+  return PBGPU_OK;
+}
+
+}  // namespace pbgpu

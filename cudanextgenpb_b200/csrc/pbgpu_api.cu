@@ -1,0 +1,445 @@
+// extern "C" entry points of libpbgpu (include/pbgpu.h).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "pbgpu_internal.cuh"
+
+namespace pbgpu {
+
+int cuda_fail(Context* c, cudaError_t e, const char* what) {
+  c->err = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();  // clear a sticky-free error so the context stays usable
+  return e == cudaErrorMemoryAllocation ? PBGPU_ERR_OOM : PBGPU_ERR_CUDA;
+}
+
+cudaError_t ensure_tmp(Context* c, size_t bytes) { return c->tmp.alloc(bytes > 0 ? bytes : 1); }
+
+template <typename T>
+static int upload(Context* c, DBuf<T>& d, const T* h, size_t count) {
+  PBGPU_CUDA(c, d.alloc(count > 0 ? count : 1));
+  if (count) PBGPU_CUDA(c, cudaMemcpyAsync(d.get(), h, count * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+  return PBGPU_OK;
+}
+
+static void invalidate_from_mesh(Context* c) {
+  c->have_markers = c->have_incidence = c->have_density = c->have_system = c->have_phi = false;
+}
+
+// Stage timing with CUDA events on the context stream.
+struct StageTimer {
+  Context* c;
+  int idx;
+  cudaEvent_t a = nullptr, b = nullptr;
+  StageTimer(Context* ctx, int i) : c(ctx), idx(i) {
+    if (cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess) cudaEventRecord(a, c->stream);
+  }
+  ~StageTimer() {
+    if (a && b) {
+      cudaEventRecord(b, c->stream);
+      if (cudaEventSynchronize(b) == cudaSuccess) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        c->stage_ms[idx] = ms;
+      }
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+int build_ray_hash_from(Context* c, int axis, const uint64_t* d_keys);
+
+}  // namespace pbgpu
+
+using namespace pbgpu;
+
+#define CTX_CHECK(ctx) \
+  if (!(ctx)) return PBGPU_ERR_ARG;
+#define SET_DEVICE(C)                                       \
+  do {                                                      \
+    cudaError_t _e = cudaSetDevice((C)->device);            \
+    if (_e != cudaSuccess) return cuda_fail((C), _e, "cudaSetDevice"); \
+  } while (0)
+
+extern "C" {
+
+int pbgpu_version(void) { return 1; }
+
+int pbgpu_ctx_create(pbgpu_ctx** out, int device, void* cuda_stream) {
+  if (!out) return PBGPU_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return PBGPU_ERR_CUDA;
+  }
+  if (device < 0 || device >= ndev) return PBGPU_ERR_ARG;
+  pbgpu_ctx* h = new (std::nothrow) pbgpu_ctx();
+  if (!h) return PBGPU_ERR_OOM;
+  Context* c = &h->c;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete h;
+    return PBGPU_ERR_CUDA;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->sm_count = prop.multiProcessorCount;
+  if (cuda_stream) {
+    c->stream = static_cast<cudaStream_t>(cuda_stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete h;
+      return PBGPU_ERR_CUDA;
+    }
+    c->own_stream = true;
+  }
+  if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaMallocHost(&c->ks_host, sizeof(KrylovScalars)) != cudaSuccess) {
+    pbgpu_ctx_destroy(h);
+    return PBGPU_ERR_CUDA;
+  }
+  *out = h;
+  return PBGPU_OK;
+}
+
+void pbgpu_ctx_destroy(pbgpu_ctx* h) {
+  if (!h) return;
+  Context* c = &h->c;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ks_host) cudaFreeHost(c->ks_host);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete h;  // DBuf destructors free device memory
+}
+
+const char* pbgpu_last_error(const pbgpu_ctx* h) { return h ? h->c.err.c_str() : "null context"; }
+
+int pbgpu_set_mesh(pbgpu_ctx* h, const pbgpu_mesh* m) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (!m || m->n_oct <= 0 || m->n_nodes <= 0 || !m->oct_xyz || !m->oct_level || !m->oct_nodes || !m->node_xyz)
+    return c->fail(PBGPU_ERR_ARG, "set_mesh: empty or null mesh arrays");
+  if (m->n_hang > 0 && (!m->hang_np || !m->hang_par)) return c->fail(PBGPU_ERR_ARG, "set_mesh: null hanging arrays");
+  if (m->n_nodes + m->n_hang >= (int64_t(1) << 31)) return c->fail(PBGPU_ERR_ARG, "set_mesh: too many nodes");
+  for (int a = 0; a < 3; ++a)
+    if (!(m->hi[a] > m->lo[a])) return c->fail(PBGPU_ERR_ARG, "set_mesh: empty domain box");
+  SET_DEVICE(c);
+  const int64_t no = m->n_oct, n = m->n_nodes, nh = m->n_hang;
+  // validate node ids and pack octants / nodes as int4
+  std::vector<int4> oct(no), nodes(n), hp(nh > 0 ? nh : 1);
+  for (int64_t o = 0; o < no; ++o) {
+    const int lv = m->oct_level[o];
+    if (lv < 0 || lv > 18) return c->fail(PBGPU_ERR_ARG, "set_mesh: octant level out of range");
+    oct[o] = make_int4(m->oct_xyz[3 * o], m->oct_xyz[3 * o + 1], m->oct_xyz[3 * o + 2], lv);
+  }
+  for (int64_t t = 0; t < 8 * no; ++t)
+    if (m->oct_nodes[t] < 0 || m->oct_nodes[t] >= n + nh) return c->fail(PBGPU_ERR_ARG, "set_mesh: bad node id");
+  for (int64_t i = 0; i < n; ++i) {
+    const int32_t* p = m->node_xyz + 3 * i;
+    int flag = 0;
+    for (int a = 0; a < 3; ++a) {
+      if (p[a] < 0 || p[a] > kRoot) return c->fail(PBGPU_ERR_ARG, "set_mesh: node coordinate out of range");
+      if (p[a] == 0 || p[a] == kRoot) flag = 1;
+    }
+    nodes[i] = make_int4(p[0], p[1], p[2], flag);
+  }
+  for (int64_t j = 0; j < nh; ++j) {
+    const int np = m->hang_np[j];
+    if (np != 2 && np != 4) return c->fail(PBGPU_ERR_ARG, "set_mesh: hanging node needs 2 or 4 parents");
+    int32_t par[4];
+    for (int k = 0; k < 4; ++k) {
+      par[k] = k < np ? m->hang_par[4 * j + k] : m->hang_par[4 * j];
+      if (par[k] < 0 || par[k] >= n) return c->fail(PBGPU_ERR_ARG, "set_mesh: hanging parent is not an independent node");
+    }
+    hp[j] = make_int4(par[0], par[1], par[2], par[3]);
+  }
+  invalidate_from_mesh(c);
+  c->n_oct = no;
+  c->n = n;
+  c->nh = nh;
+  for (int a = 0; a < 3; ++a) {
+    c->lo[a] = m->lo[a];
+    c->len[a] = m->hi[a] - m->lo[a];
+  }
+  c->tol = m->locate_tol;
+  int st;
+  if ((st = upload(c, c->oct, oct.data(), no)) != PBGPU_OK) return st;
+  if ((st = upload(c, c->oct_nodes, m->oct_nodes, 8 * no)) != PBGPU_OK) return st;
+  if ((st = upload(c, c->node_xyz, nodes.data(), n)) != PBGPU_OK) return st;
+  if ((st = upload(c, c->hang_par, hp.data(), nh > 0 ? nh : 1)) != PBGPU_OK) return st;
+  std::vector<int8_t> np(nh > 0 ? nh : 1, 2);
+  if (nh) std::memcpy(np.data(), m->hang_np, nh);
+  if ((st = upload(c, c->hang_np, np.data(), np.size())) != PBGPU_OK) return st;
+  PBGPU_CUDA(c, c->oct_key.alloc(no));
+  launch_oct_keys(c->oct.get(), no, c->oct_key.get(), c->stream);
+  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->have_mesh = true;
+  return PBGPU_OK;
+}
+
+int pbgpu_set_rays(pbgpu_ctx* h, int axis, const pbgpu_rays* r) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (axis < 0 || axis > 2 || !r || r->n_rays < 0) return c->fail(PBGPU_ERR_ARG, "set_rays: bad axis or table");
+  if (r->n_rays > 0 && (!r->keys || !r->ptr || !r->inters || !r->normals))
+    return c->fail(PBGPU_ERR_ARG, "set_rays: null arrays");
+  if (r->n_rays >= (int64_t(1) << 31)) return c->fail(PBGPU_ERR_ARG, "set_rays: too many rays");
+  SET_DEVICE(c);
+  const int64_t nr = r->n_rays;
+  const int64_t nc = nr > 0 ? r->ptr[nr] : 0;
+  if (nr > 0) {
+    if (r->ptr[0] != 0) return c->fail(PBGPU_ERR_ARG, "set_rays: ptr[0] must be 0");
+    for (int64_t j = 0; j < nr; ++j) {
+      if (r->ptr[j + 1] < r->ptr[j]) return c->fail(PBGPU_ERR_ARG, "set_rays: ptr not ascending");
+      if (j && r->keys[j] <= r->keys[j - 1]) return c->fail(PBGPU_ERR_ARG, "set_rays: keys not strictly ascending");
+    }
+  }
+  Rays& R = c->rays[axis];
+  R.n = nr;
+  int st;
+  if ((st = upload(c, R.ptr, r->ptr, nr + 1)) != PBGPU_OK) return st;
+  if ((st = upload(c, R.inters, r->inters, nc)) != PBGPU_OK) return st;
+  if ((st = upload(c, R.normals, r->normals, 3 * nc)) != PBGPU_OK) return st;
+  DBuf<uint64_t> keys;
+  if ((st = upload(c, keys, r->keys, nr)) != PBGPU_OK) return st;
+  if ((st = build_ray_hash_from(c, axis, keys.get())) != PBGPU_OK) return st;
+  c->have_rays[axis] = true;
+  c->have_markers = c->have_system = c->have_phi = false;
+  return PBGPU_OK;
+}
+
+int pbgpu_set_atoms(pbgpu_ctx* h, int64_t na, const double* pos, const double* q) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (na < 0 || (na > 0 && (!pos || !q))) return c->fail(PBGPU_ERR_ARG, "set_atoms: bad arrays");
+  if (na >= (int64_t(1) << 27)) return c->fail(PBGPU_ERR_ARG, "set_atoms: too many atoms");
+  SET_DEVICE(c);
+  std::vector<double4> a(na > 0 ? na : 1);
+  for (int64_t i = 0; i < na; ++i) a[i] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], q[i]);
+  int st = upload(c, c->atoms, a.data(), na);
+  if (st != PBGPU_OK) return st;
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->na = na;
+  c->have_atoms = true;
+  c->have_density = c->have_system = c->have_phi = false;
+  return PBGPU_OK;
+}
+
+int pbgpu_set_model(pbgpu_ctx* h, const pbgpu_model* m) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (!m) return c->fail(PBGPU_ERR_ARG, "set_model: null");
+  if (!(m->e_in > 0) || !(m->e_out > 0) || !(m->T > 0) || m->ionic_strength < 0)
+    return c->fail(PBGPU_ERR_ARG, "set_model: dielectric constants and T must be positive, ionic strength >= 0");
+  if (m->bc_type < 0 || m->bc_type > 3) return c->fail(PBGPU_ERR_ARG, "set_model: bc_type must be 0..3");
+  c->model = *m;
+  // physical constants and scalings of src/pb_class.cpp:1800-1806 (same
+  // evaluation order)
+  const double e_0 = 8.85418781762e-12, kb = 1.380649e-23, e = 1.602176634e-19, N_av = 6.022e23, Angs = 1e-10;
+  c->eps_in = 4.0 * kPi * e_0 * m->e_in * kb * m->T * Angs / (e * e);
+  c->eps_out = 4.0 * kPi * e_0 * m->e_out * kb * m->T * Angs / (e * e);
+  const double C_0 = 1.0e3 * N_av * m->ionic_strength;
+  c->k2 = 2.0 * C_0 * Angs * Angs * e * e / (e_0 * m->e_out * kb * m->T);
+  c->kappa = std::sqrt(c->k2);
+  c->have_model = true;
+  c->have_markers = c->have_system = c->have_phi = false;
+  return PBGPU_OK;
+}
+
+int pbgpu_create_markers(pbgpu_ctx* h) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (!c->have_mesh || !c->have_model || !c->have_rays[0] || !c->have_rays[1] || !c->have_rays[2])
+    return c->fail(PBGPU_ERR_STATE, "create_markers: mesh, model and the 3 ray tables are required");
+  SET_DEVICE(c);
+  StageTimer t(c, 0);
+  c->have_system = c->have_phi = false;
+  return run_markers(c);
+}
+
+int pbgpu_create_density_map(pbgpu_ctx* h) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (!c->have_mesh || !c->have_atoms) return c->fail(PBGPU_ERR_STATE, "create_density_map: mesh and atoms are required");
+  SET_DEVICE(c);
+  StageTimer t(c, 1);
+  c->have_system = c->have_phi = false;
+  return run_density(c);
+}
+
+int pbgpu_assemble(pbgpu_ctx* h, const pbgpu_sell_opts* o) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  SET_DEVICE(c);
+  StageTimer t(c, 2);
+  return run_assemble(c, o);
+}
+
+int pbgpu_solve(pbgpu_ctx* h, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  SET_DEVICE(c);
+  StageTimer t(c, 3);
+  return run_solve(c, o, st);
+}
+
+int pbgpu_phi_on_atoms(pbgpu_ctx* h, double* out) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (!out && c->na > 0) return c->fail(PBGPU_ERR_ARG, "phi_on_atoms: null output");
+  SET_DEVICE(c);
+  StageTimer t(c, 4);
+  return run_phi_atoms(c, out);
+}
+
+int pbgpu_energy(pbgpu_ctx* h, int fast, pbgpu_energy_out* out) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (!out) return c->fail(PBGPU_ERR_ARG, "energy: null output");
+  SET_DEVICE(c);
+  StageTimer t(c, 5);
+  return run_energy(c, fast, out);
+}
+
+void pbgpu_default_solver_opts(pbgpu_solver_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->method = PBGPU_BICGSTAB;
+  o->precond = PBGPU_PRECOND_JACOBI;
+  o->precision = PBGPU_FP64;
+  o->tol = 1e-6;
+  o->max_iter = 10000;
+  o->inner_tol = 1e-5;
+  o->max_outer = 50;
+  o->check_every = 16;
+}
+
+int pbgpu_parse_lis_options(const char* options, pbgpu_solver_opts* out) {
+  if (!out) return PBGPU_ERR_ARG;
+  pbgpu_default_solver_opts(out);
+  // LIS defaults (-i bicg is LIS's own default solver; NextGenPB passes -i)
+  if (!options) return PBGPU_OK;
+  std::istringstream in(options);
+  std::vector<std::string> tok;
+  for (std::string t; in >> t;) tok.push_back(t);
+  for (size_t i = 0; i < tok.size(); ++i) {
+    const std::string& k = tok[i];
+    const bool has = i + 1 < tok.size();
+    if ((k == "-i" || k == "-solver") && has) {
+      const std::string v = tok[++i];
+      if (v == "cg" || v == "1" || v == "cr" || v == "5")
+        out->method = PBGPU_CG;
+      else
+        out->method = PBGPU_BICGSTAB;  // bicg, cgs, bicgstab, bicgsafe, gmres, ...
+    } else if ((k == "-p" || k == "-precon") && has) {
+      const std::string v = tok[++i];
+      if (v == "none" || v == "0")
+        out->precond = PBGPU_PRECOND_NONE;
+      else if (v == "jacobi" || v == "1")
+        out->precond = PBGPU_PRECOND_JACOBI;
+      else
+        out->precond = PBGPU_PRECOND_BLOCK_JACOBI;
+    } else if (k == "-tol" && has) {
+      const double t = std::strtod(tok[++i].c_str(), nullptr);
+      if (!(t > 0)) return PBGPU_ERR_ARG;
+      out->tol = t;
+    } else if (k == "-maxiter" && has) {
+      const long m = std::strtol(tok[++i].c_str(), nullptr, 10);
+      if (m <= 0) return PBGPU_ERR_ARG;
+      out->max_iter = (int)m;
+    } else if (k == "-f" && has) {
+      const std::string v = tok[++i];
+      if (v == "mixed" || v == "float" || v == "quad") out->precision = v == "quad" ? PBGPU_FP64 : PBGPU_MIXED;
+    } else if (has && k.size() > 1 && k[0] == '-' && tok[i + 1][0] != '-') {
+      ++i;  // other LIS options (-print, -conv_cond, -tol_w, -ssor_omega ...) take one value
+    }
+  }
+  return PBGPU_OK;
+}
+
+int pbgpu_get_node_coeffs(pbgpu_ctx* h, double* eps, double* react) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (!c->have_markers) return c->fail(PBGPU_ERR_STATE, "get_node_coeffs: create_markers has not run");
+  SET_DEVICE(c);
+  if (eps) PBGPU_CUDA(c, cudaMemcpyAsync(eps, c->eps.get(), c->n * 8, cudaMemcpyDeviceToHost, c->stream));
+  if (react) PBGPU_CUDA(c, cudaMemcpyAsync(react, c->react.get(), c->n * 8, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PBGPU_OK;
+}
+
+int pbgpu_get_markers(pbgpu_ctx* h, double* marker, int64_t* n_border, int32_t* border) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (!c->have_markers) return c->fail(PBGPU_ERR_STATE, "get_markers: create_markers has not run");
+  SET_DEVICE(c);
+  if (n_border) *n_border = c->nb;
+  if (marker) {
+    std::vector<uint8_t> m(c->n_oct);
+    PBGPU_CUDA(c, cudaMemcpyAsync(m.data(), c->marker.get(), c->n_oct, cudaMemcpyDeviceToHost, c->stream));
+    PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int64_t o = 0; o < c->n_oct; ++o) marker[o] = m[o] == 0 ? 0.0 : (m[o] == 1 ? 0.5 : 1.0);
+  }
+  if (border && c->nb)
+    PBGPU_CUDA(c, cudaMemcpyAsync(border, c->border.get(), c->nb * 4, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PBGPU_OK;
+}
+
+int pbgpu_get_fractions(pbgpu_ctx* h, double* frac) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (!c->have_markers) return c->fail(PBGPU_ERR_STATE, "get_fractions: create_markers has not run");
+  if (!frac) return c->fail(PBGPU_ERR_ARG, "get_fractions: null output");
+  SET_DEVICE(c);
+  if (c->nb) PBGPU_CUDA(c, cudaMemcpyAsync(frac, c->frac.get(), 12 * c->nb * 8, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PBGPU_OK;
+}
+
+int pbgpu_get_density(pbgpu_ctx* h, double* rho, double* vol_patch) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (!c->have_density) return c->fail(PBGPU_ERR_STATE, "get_density: create_density_map has not run");
+  SET_DEVICE(c);
+  if (rho) PBGPU_CUDA(c, cudaMemcpyAsync(rho, c->rho.get(), c->n * 8, cudaMemcpyDeviceToHost, c->stream));
+  if (vol_patch) PBGPU_CUDA(c, cudaMemcpyAsync(vol_patch, c->vol_patch.get(), c->n * 8, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PBGPU_OK;
+}
+
+int pbgpu_get_system(pbgpu_ctx* h, int64_t* nnz, int64_t* row_ptr, int32_t* col, double* val, double* rhs) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  SET_DEVICE(c);
+  return export_system(c, nnz, row_ptr, col, val, rhs);
+}
+
+int pbgpu_get_phi(pbgpu_ctx* h, double* phi) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  if (!c->have_phi) return c->fail(PBGPU_ERR_STATE, "get_phi: solve has not run");
+  if (!phi) return c->fail(PBGPU_ERR_ARG, "get_phi: null output");
+  SET_DEVICE(c);
+  PBGPU_CUDA(c, cudaMemcpyAsync(phi, c->phi.get(), c->n * 8, cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PBGPU_OK;
+}
+
+int pbgpu_get_stage_ms(pbgpu_ctx* h, double ms[6]) {
+  CTX_CHECK(h);
+  if (!ms) return PBGPU_ERR_ARG;
+  for (int i = 0; i < 6; ++i) ms[i] = h->c.stage_ms[i];
+  return PBGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,267 @@
+// Internal declarations of libpbgpu: the context, device buffers and the
+// device-side helpers shared by the kernels.  B200 (sm_100a) only.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/pbgpu.h"
+
+namespace pbgpu {
+
+constexpr int kRootLog = 19;
+constexpr int32_t kRoot = 1 << kRootLog;
+constexpr int kMaxRow = 96;         // distinct columns a matrix row may hold
+constexpr int kMaxIncidence = 160;  // (octant, corner) incidences of one node
+constexpr uint64_t kEmptyKey = ~0ull;
+
+// ---------------------------------------------------------------------------
+// Device buffer owned by a context.
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    release();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    else p = nullptr;
+    return e;
+  }
+  T* get() const { return p; }
+};
+
+struct Rays {
+  int64_t n = 0;          // rays with crossings
+  int64_t cap = 0;        // hash capacity (power of two)
+  int cap_log = 0;
+  DBuf<uint64_t> hkeys;   // open-addressing table of ray keys
+  DBuf<int32_t> hval;     // ray index of each slot
+  DBuf<int64_t> ptr;
+  DBuf<double> inters;
+  DBuf<double> normals;
+};
+
+// Krylov scalars kept on the device (one struct, updated by the last block of
+// each reducing kernel).
+struct KrylovScalars {
+  double rz, rz_new, pq, alpha, beta, omega, rho, rr, bb, ss, ts, tt, rv;
+  double tol2;            // tol^2 * ||b||^2
+  int iter, max_iter, done, status, s_conv;
+  unsigned int ticket[8]; // last-block tickets, one per reducing kernel
+};
+
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double stage_ms[6] = {0, 0, 0, 0, 0, 0};
+
+  // ---- mesh
+  int64_t n_oct = 0, n = 0, nh = 0;
+  double lo[3] = {0, 0, 0}, len[3] = {0, 0, 0}, tol = 0;
+  DBuf<int4> oct;            // x, y, z, level
+  DBuf<uint64_t> oct_key;    // Morton key of the lower corner
+  DBuf<int32_t> oct_nodes;   // 8 per octant
+  DBuf<int4> node_xyz;       // x, y, z, boundary flag
+  DBuf<int4> hang_par;       // 4 parents, -1 padded
+  DBuf<int8_t> hang_np;
+  bool have_mesh = false;
+
+  Rays rays[3];
+  bool have_rays[3] = {false, false, false};
+
+  // ---- atoms
+  int64_t na = 0;
+  DBuf<double4> atoms;       // x, y, z, q
+  bool have_atoms = false;
+
+  // ---- model
+  pbgpu_model model{};
+  double eps_in = 0, eps_out = 0, k2 = 0, kappa = 0;
+  bool have_model = false;
+
+  // ---- markers
+  DBuf<uint8_t> inside;      // per node
+  DBuf<double> eps, react;   // per node
+  DBuf<uint8_t> marker;      // per octant: 0 in, 1 border, 2 out
+  DBuf<double> react_cell;   // per octant (Stern layer)
+  DBuf<int32_t> border;      // border octants, ascending
+  DBuf<int32_t> border_pos;  // octant -> border position or -1
+  DBuf<double> frac;         // 12 per border octant
+  int64_t nb = 0;
+  bool have_markers = false;
+
+  // ---- incidence (node -> (octant, corner))
+  DBuf<int64_t> inc_ptr;
+  DBuf<uint32_t> inc;
+  bool have_incidence = false;
+
+  // ---- density
+  DBuf<double> vol_patch, rho;
+  DBuf<int32_t> atom_oct;    // octant of each atom or -1
+  bool have_density = false;
+
+  // ---- system in SELL-C-sigma (rows permuted; vectors live in SELL order)
+  int C = 32, sigma = 32;
+  int64_t n_slices = 0, nnz = 0, sell_len = 0;
+  DBuf<int64_t> slice_ptr;   // element offset of each slice
+  DBuf<int32_t> slice_w;     // width (multiple of 4) of each slice
+  DBuf<int32_t> perm;        // SELL position -> node
+  DBuf<int32_t> iperm;       // node -> SELL position
+  DBuf<int32_t> scol;        // column (SELL numbering)
+  DBuf<double> sval;
+  DBuf<float> sval32;        // fp32 copy for the mixed-precision inner solve
+  DBuf<double> b;            // right-hand side (SELL order)
+  DBuf<double> dinv;         // 1 / diagonal (SELL order)
+  DBuf<int32_t> rowlen;      // per node
+  DBuf<uint8_t> dirichlet;   // per node
+  DBuf<double> gval;         // Dirichlet value per node
+  bool have_system = false;
+
+  // ---- solve
+  DBuf<double> x, r, p, q, z, rh, v, s, t, ph, sh;   // fp64 work vectors (SELL order)
+  DBuf<float> x32, r32, p32, q32, b32, dinv32;       // fp32 inner vectors
+  DBuf<double> partials;     // block partial sums
+  DBuf<KrylovScalars> ks;
+  KrylovScalars* ks_host = nullptr;   // pinned mirror
+  DBuf<double> phi;          // node order
+  bool have_phi = false;
+  int sm_count = 148;
+
+  // ---- energy scratch
+  DBuf<double4> elem_a;      // element position + coefficient
+  DBuf<double4> elem_b;      // element normal (triangle vertices)
+  DBuf<int32_t> elem_cnt;
+  DBuf<double> energy_part;
+
+  // ---- scratch for CUB
+  DBuf<uint8_t> tmp;
+
+  int fail(int code, const std::string& msg) {
+    err = msg;
+    return code;
+  }
+};
+
+int cuda_fail(Context* c, cudaError_t e, const char* what);
+
+#define PBGPU_CUDA(ctx, expr)                                   \
+  do {                                                          \
+    cudaError_t _e = (expr);                                    \
+    if (_e != cudaSuccess) return ::pbgpu::cuda_fail((ctx), _e, #expr); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Device helpers.
+
+// lo + len * (i * 2^-19) with one rounding per operation, never contracted.
+__device__ __forceinline__ double coord(double lo, double len, int32_t i) {
+  return __dadd_rn(lo, __dmul_rn(len, (double)i * 0x1p-19));
+}
+
+__device__ __forceinline__ uint64_t ray_key(int32_t a, int32_t b) {
+  return ((uint64_t)(uint32_t)a << 20) | (uint64_t)(uint32_t)b;
+}
+
+__device__ __forceinline__ uint64_t hash_slot(uint64_t key, int cap_log) {
+  return (key * 0x9E3779B97F4A7C15ull) >> (64 - cap_log);
+}
+
+// Ray index of `key` or -1.
+__device__ __forceinline__ int32_t ray_find(const uint64_t* __restrict__ hk, const int32_t* __restrict__ hv,
+                                            int64_t cap, int cap_log, uint64_t key) {
+  if (cap == 0) return -1;
+  uint64_t s = hash_slot(key, cap_log);
+  for (int64_t probe = 0; probe < cap; ++probe) {
+    const uint64_t k = hk[s];
+    if (k == key) return hv[s];
+    if (k == kEmptyKey) return -1;
+    s = (s + 1) & (uint64_t)(cap - 1);
+  }
+  return -1;
+}
+
+struct RayView {
+  const uint64_t* hk;
+  const int32_t* hv;
+  const int64_t* ptr;
+  const double* inters;
+  const double* normals;
+  int64_t cap;
+  int cap_log;
+};
+
+inline RayView ray_view(const Rays& r) {
+  return RayView{r.hkeys.get(), r.hval.get(), r.ptr.get(), r.inters.get(), r.normals.get(), r.cap, r.cap_log};
+}
+
+// Which axis edge e runs along, and its two corners (reference edge table,
+// include/pb_class.h:190-207).
+__device__ __constant__ static const int8_t d_edge_nodes[24] = {0, 1, 1, 3, 2, 3, 0, 2, 4, 5, 5, 7,
+                                                                  6, 7, 4, 6, 0, 4, 1, 5, 3, 7, 2, 6};
+__device__ __constant__ static const int8_t d_edge_axis[12] = {0, 1, 0, 1, 0, 1, 0, 1, 2, 2, 2, 2};
+
+// Edges meeting at corner c: the edge along axis a is the one whose corner
+// pair is (c with bit a cleared, c with bit a set).
+__device__ __forceinline__ int edge_of(int c, int axis) {
+  // lower corner of the edge along `axis` through c
+  const int lowc = c & ~(1 << axis);
+  // edges along x: 0 (0-1), 2 (2-3), 4 (4-5), 6 (6-7)  -> by lowc>>1
+  // edges along y: 3 (0-2), 1 (1-3), 7 (4-6), 5 (5-7)
+  // edges along z: 8 (0-4), 9 (1-5), 11 (2-6), 10 (3-7)
+  if (axis == 0) return 2 * (lowc >> 1);
+  if (axis == 1) {
+    const int t = (lowc & 1) | ((lowc >> 2) << 1);  // (x bit, z bit)
+    const int tbl[4] = {3, 1, 7, 5};
+    return tbl[t];
+  }
+  const int tbl[4] = {8, 9, 11, 10};
+  return tbl[lowc & 3];
+}
+
+__device__ __forceinline__ double wha(double e1, double e2, double f) { return 1.0 / (f / e1 + (1 - f) / e2); }
+
+// physical constants of the reference (include/pb_class.h:47-54)
+constexpr double kPi = 3.14159265358979323846;
+
+// ---------------------------------------------------------------------------
+// Stage entry points (implemented per .cu file).
+int build_ray_hash_from(Context* c, int axis, const uint64_t* d_keys);
+int run_markers(Context* c);
+int build_incidence(Context* c);
+int run_density(Context* c);
+int run_assemble(Context* c, const pbgpu_sell_opts* o);
+int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st);
+int run_phi_atoms(Context* c, double* out);
+int run_energy(Context* c, int fast, pbgpu_energy_out* out);
+int export_system(Context* c, int64_t* nnz, int64_t* row_ptr, int32_t* col, double* val, double* rhs);
+
+// scratch for CUB temporaries
+cudaError_t ensure_tmp(Context* c, size_t bytes);
+// Morton keys of the octants' lower corners
+void launch_oct_keys(const int4* oct, int64_t n_oct, uint64_t* key, cudaStream_t s);
+
+inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }
+
+}  // namespace pbgpu
+
+struct pbgpu_ctx {
+  pbgpu::Context c;
+};

@@ -1,0 +1,293 @@
+"""Python face of the PB path: the host problem (pbhost) and the GPU path (pbgpu).
+
+``Problem`` mirrors the reference's set-up half of ``poisson_boltzmann``
+(parse_options, read_atoms_from_pqr, create_mesh, init_tmesh*, refine_surface;
+src/pb_class.cpp:39-1745) and exposes the mesh, ray and atom arrays that feed
+the GPU.  ``GpuPath`` mirrors the hot half (create_markers, create_density_map,
+assemple_system_matrix, lis_compute_electric_potential,
+write_potential_on_atoms_fast, energy / energy_fast) one call per reference
+member function, through the C ABI of include/pbgpu.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+
+class PBError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("pbgpu status %d: %s" % (code, msg))
+        self.code = code
+
+
+def _arr(ptr, count, dtype):
+    if count == 0:
+        return np.zeros(0, dtype=dtype)
+    return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dtype, copy=True)
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Problem:
+    """Options + atoms + octree + surface rays, built by libpbhost."""
+
+    def __init__(self, options_text: str | None = None, options_file: str | None = None):
+        self._lib = N.load_host()
+        self._h = self._lib.pbhost_create()
+        if not self._h:
+            raise MemoryError("pbhost_create failed")
+        if options_file:
+            self._check(self._lib.pbhost_load_options_file(self._h, options_file.encode()))
+        if options_text:
+            self._check(self._lib.pbhost_load_options_text(self._h, options_text.encode()))
+
+    def _check(self, st):
+        if st != 0:
+            raise PBError(st, self._lib.pbhost_last_error(self._h).decode())
+
+    def close(self):
+        if self._h:
+            self._lib.pbhost_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_option(self, key: str, value):
+        self._check(self._lib.pbhost_set_option(self._h, key.encode(), str(value).encode()))
+
+    def read_pqr(self, path: str):
+        self._check(self._lib.pbhost_read_pqr(self._h, path.encode()))
+
+    def set_atoms(self, pos, charge, radius):
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        q = np.ascontiguousarray(charge, dtype=np.float64)
+        r = np.ascontiguousarray(radius, dtype=np.float64)
+        self._check(self._lib.pbhost_set_atoms(self._h, len(q), _dptr(pos), _dptr(q), _dptr(r)))
+
+    def build(self):
+        self._check(self._lib.pbhost_build_problem(self._h))
+        return self
+
+    def info(self) -> dict:
+        inf = N.PbhostInfo()
+        self._check(self._lib.pbhost_get_info(self._h, C.byref(inf)))
+        out = {}
+        for k, _ in inf._fields_:
+            v = getattr(inf, k)
+            out[k] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+    def mesh_struct(self) -> N.PbgpuMesh:
+        m = N.PbgpuMesh()
+        self._check(self._lib.pbhost_get_mesh(self._h, C.byref(m)))
+        return m
+
+    def rays_struct(self, axis: int) -> N.PbgpuRays:
+        r = N.PbgpuRays()
+        self._check(self._lib.pbhost_get_rays(self._h, axis, C.byref(r)))
+        return r
+
+    def mesh(self) -> dict:
+        m = self.mesh_struct()
+        return {
+            "n_oct": m.n_oct, "n_nodes": m.n_nodes, "n_hang": m.n_hang,
+            "oct_xyz": _arr(m.oct_xyz, 3 * m.n_oct, np.int32).reshape(-1, 3),
+            "oct_level": _arr(m.oct_level, m.n_oct, np.int8),
+            "oct_nodes": _arr(m.oct_nodes, 8 * m.n_oct, np.int32).reshape(-1, 8),
+            "node_xyz": _arr(m.node_xyz, 3 * m.n_nodes, np.int32).reshape(-1, 3),
+            "hang_np": _arr(m.hang_np, m.n_hang, np.int8),
+            "hang_par": _arr(m.hang_par, 4 * m.n_hang, np.int32).reshape(-1, 4),
+            "lo": np.array(list(m.lo)), "hi": np.array(list(m.hi)), "locate_tol": m.locate_tol,
+        }
+
+    def rays(self, axis: int) -> dict:
+        r = self.rays_struct(axis)
+        ptr = _arr(r.ptr, r.n_rays + 1, np.int64)
+        nc = int(ptr[-1]) if r.n_rays else 0
+        return {"keys": _arr(r.keys, r.n_rays, np.uint64), "ptr": ptr, "inters": _arr(r.inters, nc, np.float64),
+                "normals": _arr(r.normals, 3 * nc, np.float64).reshape(-1, 3)}
+
+    def atoms(self):
+        n = self.info()["n_atoms"]
+        pos = np.zeros((n, 3))
+        q = np.zeros(n)
+        r = np.zeros(n)
+        self._check(self._lib.pbhost_get_atoms(self._h, _dptr(pos), _dptr(q), _dptr(r)))
+        return pos, q, r
+
+    def model(self) -> N.PbgpuModel:
+        m = N.PbgpuModel()
+        self._check(self._lib.pbhost_get_model(self._h, C.byref(m)))
+        return m
+
+    def solver_opts(self) -> N.PbgpuSolverOpts:
+        o = N.PbgpuSolverOpts()
+        self._check(self._lib.pbhost_get_solver_opts(self._h, C.byref(o)))
+        return o
+
+    def run_gpu(self):
+        """The whole path through the host mirror's run_gpu_path (the driver order)."""
+        e, s = N.PbgpuEnergyOut(), N.PbgpuSolveStats()
+        st = self._lib.pbhost_run_gpu(self._h, C.byref(e), C.byref(s))
+        if st not in (0, N.PBGPU_NOT_CONVERGED):
+            raise PBError(st, self._lib.pbhost_last_error(self._h).decode())
+        return e.as_dict(), s
+
+
+def solver_opts(method="cg", tol=1e-8, max_iter=20000, precision="fp64", inner_tol=1e-5, check_every=16,
+                max_outer=50) -> N.PbgpuSolverOpts:
+    o = N.PbgpuSolverOpts()
+    N.load_gpu().pbgpu_default_solver_opts(C.byref(o))
+    o.method = {"cg": N.PBGPU_CG, "bicgstab": N.PBGPU_BICGSTAB}[method]
+    o.precision = {"fp64": N.PBGPU_FP64, "mixed": N.PBGPU_MIXED}[precision]
+    o.tol, o.max_iter, o.inner_tol, o.check_every, o.max_outer = tol, max_iter, inner_tol, check_every, max_outer
+    return o
+
+
+def parse_lis_options(text: str) -> N.PbgpuSolverOpts:
+    o = N.PbgpuSolverOpts()
+    st = N.load_gpu().pbgpu_parse_lis_options(text.encode(), C.byref(o))
+    if st != 0:
+        raise PBError(st, "bad LIS option string: %r" % text)
+    return o
+
+
+class GpuPath:
+    """One pbgpu context: the reference's hot-path member functions on the GPU."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self._lib = N.load_gpu()
+        self._ctx = C.c_void_p()
+        st = self._lib.pbgpu_ctx_create(C.byref(self._ctx), device, C.c_void_p(stream) if stream else None)
+        if st != 0:
+            raise PBError(st, "pbgpu_ctx_create failed (no CUDA device?)")
+        self.n = self.n_oct = self.n_atoms = 0
+
+    def _check(self, st, ok=(0,)):
+        if st not in ok:
+            raise PBError(st, self._lib.pbgpu_last_error(self._ctx).decode())
+        return st
+
+    def close(self):
+        if self._ctx:
+            self._lib.pbgpu_ctx_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- inputs
+    def load(self, prob: Problem):
+        m = prob.mesh_struct()
+        self._check(self._lib.pbgpu_set_mesh(self._ctx, C.byref(m)))
+        for a in range(3):
+            r = prob.rays_struct(a)
+            self._check(self._lib.pbgpu_set_rays(self._ctx, a, C.byref(r)))
+        pos, q, _ = prob.atoms()
+        self.set_atoms(pos, q)
+        md = prob.model()
+        self._check(self._lib.pbgpu_set_model(self._ctx, C.byref(md)))
+        self.n, self.n_oct = m.n_nodes, m.n_oct
+        return self
+
+    def set_atoms(self, pos, q):
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        self._check(self._lib.pbgpu_set_atoms(self._ctx, len(q), _dptr(pos), _dptr(q)))
+        self.n_atoms = len(q)
+
+    def set_model(self, model: N.PbgpuModel):
+        self._check(self._lib.pbgpu_set_model(self._ctx, C.byref(model)))
+
+    # ---- path
+    def create_markers(self):
+        self._check(self._lib.pbgpu_create_markers(self._ctx))
+
+    def create_density_map(self):
+        self._check(self._lib.pbgpu_create_density_map(self._ctx))
+
+    def assemble(self, chunk=32, sigma=None):
+        o = N.PbgpuSellOpts(chunk, sigma if sigma is not None else chunk)
+        self._check(self._lib.pbgpu_assemble(self._ctx, C.byref(o)))
+
+    def solve(self, opts: N.PbgpuSolverOpts | None = None, allow_not_converged=False):
+        s = N.PbgpuSolveStats()
+        ok = (0, N.PBGPU_NOT_CONVERGED) if allow_not_converged else (0,)
+        self._check(self._lib.pbgpu_solve(self._ctx, C.byref(opts) if opts else None, C.byref(s)), ok)
+        return s
+
+    def phi_on_atoms(self):
+        out = np.zeros(self.n_atoms)
+        self._check(self._lib.pbgpu_phi_on_atoms(self._ctx, _dptr(out)))
+        return out
+
+    def energy(self, fast=False) -> dict:
+        e = N.PbgpuEnergyOut()
+        self._check(self._lib.pbgpu_energy(self._ctx, 1 if fast else 0, C.byref(e)))
+        return e.as_dict()
+
+    # ---- read-back
+    def node_coeffs(self):
+        eps, react = np.zeros(self.n), np.zeros(self.n)
+        self._check(self._lib.pbgpu_get_node_coeffs(self._ctx, _dptr(eps), _dptr(react)))
+        return eps, react
+
+    def markers(self):
+        marker = np.zeros(self.n_oct)
+        nb = C.c_int64()
+        self._check(self._lib.pbgpu_get_markers(self._ctx, _dptr(marker), C.byref(nb), None))
+        border = np.zeros(nb.value, dtype=np.int32)
+        self._check(self._lib.pbgpu_get_markers(self._ctx, None, C.byref(nb),
+                                                border.ctypes.data_as(C.POINTER(C.c_int32))))
+        return marker, border
+
+    def fractions(self, n_border):
+        f = np.zeros(12 * n_border)
+        self._check(self._lib.pbgpu_get_fractions(self._ctx, _dptr(f)))
+        return f.reshape(-1, 12)
+
+    def density(self):
+        rho, vp = np.zeros(self.n), np.zeros(self.n)
+        self._check(self._lib.pbgpu_get_density(self._ctx, _dptr(rho), _dptr(vp)))
+        return rho, vp
+
+    def system(self):
+        nnz = C.c_int64()
+        self._check(self._lib.pbgpu_get_system(self._ctx, C.byref(nnz), None, None, None, None))
+        rp = np.zeros(self.n + 1, dtype=np.int64)
+        col = np.zeros(nnz.value, dtype=np.int32)
+        val = np.zeros(nnz.value)
+        rhs = np.zeros(self.n)
+        self._check(self._lib.pbgpu_get_system(self._ctx, C.byref(nnz), rp.ctypes.data_as(C.POINTER(C.c_int64)),
+                                               col.ctypes.data_as(C.POINTER(C.c_int32)), _dptr(val), _dptr(rhs)))
+        return rp, col, val, rhs
+
+    def phi(self):
+        out = np.zeros(self.n)
+        self._check(self._lib.pbgpu_get_phi(self._ctx, _dptr(out)))
+        return out
+
+    def stage_ms(self):
+        ms = (C.c_double * 6)()
+        self._check(self._lib.pbgpu_get_stage_ms(self._ctx, ms))
+        return dict(zip(["markers", "density", "assemble", "solve", "phi_atoms", "energy"], list(ms)))
+
+    def run(self, opts=None, fast=False, chunk=32, sigma=None):
+        """create_markers .. energy in the driver's order; returns (energy dict, solve stats)."""
+        self.create_markers()
+        self.create_density_map()
+        self.assemble(chunk, sigma)
+        st = self.solve(opts)
+        return self.energy(fast), st

@@ -1,0 +1,195 @@
+/*
+ * pbgpu — C ABI of the B200 (sm_100a) assemble/solve/post-process path for the
+ * linearized Poisson–Boltzmann equation on a 2:1-balanced octree with hanging
+ * nodes (NextGenPB's box-method discretisation).
+ *
+ * The calls replace, one for one, the pb_class member functions on the
+ * reference's hot path (reference paths relative to the NextGenPB tree):
+ *
+ *   pbgpu_create_markers      poisson_boltzmann::create_markers          src/pb_class.cpp:1793-1941
+ *   pbgpu_create_density_map  poisson_boltzmann::create_density_map      src/pb_class.cpp:1944-2050
+ *   pbgpu_assemble            poisson_boltzmann::assemple_system_matrix  src/pb_class.cpp:2053-2159
+ *                             (bimpp bim3a_rhs / bim3a_laplacian_frac / bim3a_reaction_frac /
+ *                              bim3a_dirichlet_bc and cube_fraction_intersection :2422-2532)
+ *   pbgpu_solve               poisson_boltzmann::lis_compute_electric_potential   :2244-2329
+ *                             poisson_boltzmann::mumps_compute_electric_potential :2200-2239
+ *   pbgpu_phi_on_atoms        poisson_boltzmann::write_potential_on_atoms_fast    :2333-2417
+ *   pbgpu_energy              poisson_boltzmann::energy / energy_fast              :2791-3338
+ *
+ * Conventions (all plain C types; no framework types cross this boundary):
+ *   - Every call returns an int status (PBGPU_OK = 0).  On failure
+ *     pbgpu_last_error(ctx) holds a one-line message.
+ *   - Host arrays are owned by the caller and copied during the call; device
+ *     memory is owned by the context.
+ *   - A context is bound to one device and one CUDA stream.  Calls on one context
+ *     must be serialised by the caller; distinct contexts are independent.
+ *   - Node indices: 0 .. n_nodes-1 are independent nodes (the unknowns);
+ *     n_nodes + h names hanging node h, whose value is the mean of its 2
+ *     (edge-hanging) or 4 (face-hanging) independent parents.
+ *   - Integer coordinates are in units of 2^-19 of the root octant (p4est's
+ *     P8EST_ROOT_LEN), corner c of an octant at lower + bits(c) * size with
+ *     x in bit 0, y in bit 1, z in bit 2.  Physical coordinates are
+ *     lo[a] + (hi[a] - lo[a]) * (i * 2^-19), evaluated without fused multiply-add.
+ */
+#ifndef PBGPU_H
+#define PBGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  PBGPU_OK = 0,
+  PBGPU_ERR_ARG = 1,          /* bad argument / size */
+  PBGPU_ERR_CUDA = 2,         /* CUDA runtime error */
+  PBGPU_ERR_OOM = 3,          /* device allocation failed */
+  PBGPU_ERR_STATE = 4,        /* call order: a prerequisite stage has not run */
+  PBGPU_ERR_CAPACITY = 5,     /* a fixed-size structure overflowed (row too long, ...) */
+  PBGPU_NOT_CONVERGED = 10,   /* Krylov iteration hit max_iter (result kept) */
+  PBGPU_BREAKDOWN = 11,       /* Krylov breakdown (rho or omega ~ 0) or non-finite value */
+  PBGPU_TIMEOUT = 12          /* a bounded device-side wait gave up */
+};
+
+enum { PBGPU_CG = 0, PBGPU_BICGSTAB = 1 };
+enum { PBGPU_PRECOND_NONE = 0, PBGPU_PRECOND_JACOBI = 1, PBGPU_PRECOND_BLOCK_JACOBI = 2 };
+enum { PBGPU_FP64 = 0, PBGPU_MIXED = 1 };
+
+typedef struct pbgpu_ctx pbgpu_ctx;
+
+/* Octree mesh (the tmesh_3d the reference builds with p4est). Octants in Morton order. */
+typedef struct {
+  int64_t n_oct;
+  const int32_t* oct_xyz;    /* 3*n_oct: lower corner, integer coordinates */
+  const int8_t* oct_level;   /* n_oct */
+  const int32_t* oct_nodes;  /* 8*n_oct: node of each corner (>= n_nodes: hanging) */
+  int64_t n_nodes;           /* independent nodes = unknowns */
+  const int32_t* node_xyz;   /* 3*n_nodes */
+  int64_t n_hang;
+  const int8_t* hang_np;     /* n_hang: 2 or 4 */
+  const int32_t* hang_par;   /* 4*n_hang: parents (ascending, -1 padded) */
+  double lo[3], hi[3];       /* domain box: tree vertices 0 and 7 */
+  double locate_tol;         /* p4esttol * box edge, atom search tolerance (src/pb_class.cpp:3636-3640) */
+} pbgpu_mesh;
+
+/* Crossings of the axis-aligned rays of one axis (NanoShaper's crossings_t).
+ * Only rays with at least one crossing are listed; a missing ray has none.
+ * key = (a << 20) | b with (a, b) the integer coordinates of the two transverse
+ * axes in ascending axis order.  keys ascending. */
+typedef struct {
+  int64_t n_rays;
+  const uint64_t* keys;      /* n_rays */
+  const int64_t* ptr;        /* n_rays + 1 */
+  const double* inters;      /* ptr[n_rays], ascending within a ray */
+  const double* normals;     /* 3*ptr[n_rays], outward unit normals (x, y, z) */
+} pbgpu_rays;
+
+/* Model parameters ([model] and [surface] sections of options.prm). */
+typedef struct {
+  double e_in, e_out;        /* molecular / solvent dielectric constants */
+  double ionic_strength;     /* mol/L */
+  double T;                  /* K */
+  int bc_type;               /* 1: phi = 0; 2: Coulomb/Debye sum; 3: analytic Born sphere */
+  int stern_layer_surf;      /* 1: ion-free Stern layer of thickness stern_layer */
+  double stern_layer;
+  int calc_energy;           /* 0 none, 1 polarisation, 2 polarisation + ionic */
+  int calc_coulombic;        /* 1: Coulomb energy */
+} pbgpu_model;
+
+typedef struct {
+  int chunk;                 /* SELL slice height C (multiple of 32; 0 = default 32) */
+  int sigma;                 /* sorting window in rows (multiple of chunk; 0 = default) */
+} pbgpu_sell_opts;
+
+typedef struct {
+  int method;                /* PBGPU_CG or PBGPU_BICGSTAB */
+  int precond;               /* PBGPU_PRECOND_* */
+  int precision;             /* PBGPU_FP64 or PBGPU_MIXED */
+  double tol;                /* stop when ||b - A x||_2 <= tol * ||b||_2 */
+  int max_iter;              /* inner iteration cap */
+  double inner_tol;          /* PBGPU_MIXED: residual reduction per fp32 inner solve */
+  int max_outer;             /* PBGPU_MIXED: refinement steps cap */
+  int check_every;           /* iterations between host polls of the device convergence flag */
+} pbgpu_solver_opts;
+
+typedef struct {
+  int status;
+  int iterations;            /* inner iterations (all refinement steps) */
+  int outer;                 /* fp64 refinement steps (PBGPU_MIXED) */
+  double rel_residual;       /* ||b - A x||_2 / ||b||_2 recomputed in fp64 at exit */
+  double device_ms;          /* device time of the solve (CUDA events on the context stream) */
+} pbgpu_solve_stats;
+
+typedef struct {
+  double energy_pol;         /* polarisation energy [kT] */
+  double energy_react;       /* direct ionic energy [kT] (calc_energy == 2) */
+  double energy_coul;        /* Coulomb energy [kT] (calc_coulombic == 1) */
+  double charge_flux;        /* flux charge [e], Gauss-law check */
+  double net_charge;         /* sum of atomic charges [e] */
+  double sum;                /* energy_pol + energy_react + energy_coul */
+} pbgpu_energy_out;
+
+/* ---- context ---------------------------------------------------------- */
+int pbgpu_ctx_create(pbgpu_ctx** out, int device, void* cuda_stream /* NULL: own stream */);
+void pbgpu_ctx_destroy(pbgpu_ctx* ctx);
+const char* pbgpu_last_error(const pbgpu_ctx* ctx);
+int pbgpu_version(void);
+
+/* ---- inputs ------------------------------------------------------------ */
+/* Mesh of tmesh_3d after refine_surface (src/poisson_boltzmann.cpp:181-186). */
+int pbgpu_set_mesh(pbgpu_ctx* ctx, const pbgpu_mesh* mesh);
+/* Ray crossings of one axis (0, 1, 2): ray_cache_t::rays (include/raytracer.h:37-85). */
+int pbgpu_set_rays(pbgpu_ctx* ctx, int axis, const pbgpu_rays* rays);
+/* Atoms: pos_atoms / charge_atoms (include/pb_class.h:68-72). */
+int pbgpu_set_atoms(pbgpu_ctx* ctx, int64_t n_atoms, const double* pos /* 3n */, const double* charge);
+int pbgpu_set_model(pbgpu_ctx* ctx, const pbgpu_model* model);
+
+/* ---- the path ------------------------------------------------------------ */
+/* create_markers (src/pb_class.cpp:1793-1941): node in/out by z-ray parity,
+ * epsilon_nodes / reaction_nodes, octant marker 0 / 0.5 / 1, border_quad. */
+int pbgpu_create_markers(pbgpu_ctx* ctx);
+/* create_density_map (src/pb_class.cpp:1944-2050): patch volumes, atom search,
+ * trilinear charge projection to rho_fixed. */
+int pbgpu_create_density_map(pbgpu_ctx* ctx);
+/* assemple_system_matrix (src/pb_class.cpp:2053-2159): edge fractions of border
+ * octants, box-method Laplacian with harmonic edge coefficients, kappa^2
+ * reaction, hanging-node elimination, Dirichlet conditions -> SELL-C-sigma
+ * matrix and right-hand side on the device.  opts may be NULL. */
+int pbgpu_assemble(pbgpu_ctx* ctx, const pbgpu_sell_opts* opts);
+/* lis_/mumps_compute_electric_potential: Krylov solve of the assembled system,
+ * x0 = 0.  stats may be NULL. Returns PBGPU_NOT_CONVERGED / PBGPU_BREAKDOWN with
+ * the last iterate kept. */
+int pbgpu_solve(pbgpu_ctx* ctx, const pbgpu_solver_opts* opts, pbgpu_solve_stats* stats);
+/* write_potential_on_atoms_fast (src/pb_class.cpp:2333-2417): phi at every atom
+ * found in the mesh (trilinear in its octant); NaN for atoms outside. */
+int pbgpu_phi_on_atoms(pbgpu_ctx* ctx, double* phi_atoms /* n_atoms */);
+/* energy (fast = 0, src/pb_class.cpp:2791-3063) or energy_fast (fast = 1, :3066-3338). */
+int pbgpu_energy(pbgpu_ctx* ctx, int fast, pbgpu_energy_out* out);
+
+/* Parse a LIS option string ("-i bicgstab -p jacobi -tol 1.e-8 ...") into
+ * solver options, the way lis_solver_set_option is fed at src/pb_class.cpp:2313.
+ * Unsupported LIS solvers map to the nearest supported one (cgs, bicg, bicgsafe,
+ * gmres -> bicgstab; cr -> cg); ssor/ilu/sainv map to block Jacobi. */
+int pbgpu_parse_lis_options(const char* options, pbgpu_solver_opts* out);
+void pbgpu_default_solver_opts(pbgpu_solver_opts* out);
+
+/* ---- read-back (parity checks and downstream output) -------------------- */
+int pbgpu_get_node_coeffs(pbgpu_ctx* ctx, double* epsilon_nodes, double* reaction_nodes);
+/* marker per octant (0, 0.5, 1); border octants ascending. */
+int pbgpu_get_markers(pbgpu_ctx* ctx, double* marker, int64_t* n_border, int32_t* border /* may be NULL */);
+/* 12 edge fractions per border octant, in border order (reference edge order). */
+int pbgpu_get_fractions(pbgpu_ctx* ctx, double* frac);
+int pbgpu_get_density(pbgpu_ctx* ctx, double* rho_fixed, double* vol_patch);
+/* Assembled system in CSR, node order, columns ascending.  Call with col = NULL
+ * to get nnz only. */
+int pbgpu_get_system(pbgpu_ctx* ctx, int64_t* nnz, int64_t* row_ptr, int32_t* col, double* val, double* rhs);
+int pbgpu_get_phi(pbgpu_ctx* ctx, double* phi);
+/* Device time of the last call of each stage (ms): markers, density, assemble,
+ * solve, phi_on_atoms, energy. */
+int pbgpu_get_stage_ms(pbgpu_ctx* ctx, double ms[6]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PBGPU_H */

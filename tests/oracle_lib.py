@@ -1,0 +1,172 @@
+"""ctypes access to the CPU oracle (oracle/lib/liboracle.so) — test infrastructure.
+
+Only tests, __graft_entry__.smoke() and bench.py's CPU baseline use this.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from cudanextgenpb_b200 import _native as N
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "lib", "liboracle.so")
+
+P = C.POINTER
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError("oracle not built: run __graft_entry__.build()")
+        L = C.CDLL(ORACLE_SO)
+        sp = C.c_void_p
+        L.oracle_create.restype = sp
+        L.oracle_create.argtypes = [P(N.PbgpuMesh), P(N.PbgpuRays), C.c_int64, P(C.c_double), P(C.c_double),
+                                    P(N.PbgpuModel)]
+        L.oracle_destroy.argtypes = [sp]
+        for f in ("oracle_markers", "oracle_density", "oracle_assemble"):
+            getattr(L, f).argtypes = [sp]
+        L.oracle_solve.argtypes = [sp, C.c_int, C.c_double, C.c_int, C.c_int, P(C.c_double)]
+        L.oracle_phi_on_atoms.argtypes = [sp, P(C.c_double)]
+        L.oracle_energy.argtypes = [sp, C.c_int, P(N.PbgpuEnergyOut)]
+        L.oracle_get_node_coeffs.argtypes = [sp, P(C.c_double), P(C.c_double)]
+        L.oracle_get_markers.argtypes = [sp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
+        L.oracle_get_fractions.argtypes = [sp, P(C.c_double)]
+        L.oracle_get_density.argtypes = [sp, P(C.c_double), P(C.c_double)]
+        L.oracle_get_system.argtypes = [sp, P(C.c_int64), P(C.c_int64), P(C.c_int32), P(C.c_double), P(C.c_double)]
+        L.oracle_get_phi.argtypes = [sp, P(C.c_double)]
+        L.oracle_set_phi.argtypes = [sp, P(C.c_double)]
+        L.oracle_set_system.argtypes = [sp, C.c_int64, P(C.c_int64), P(C.c_int32), P(C.c_double), P(C.c_double)]
+        L.oracle_spmv.argtypes = [sp, P(C.c_double), P(C.c_double), C.c_int]
+        L.oracle_time_cg_iterations.restype = C.c_double
+        L.oracle_time_cg_iterations.argtypes = [sp, C.c_int, C.c_int]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(P(C.c_double))
+
+
+class Oracle:
+    """The CPU restatement of the reference path on one problem's inputs."""
+
+    def __init__(self, prob):
+        self.L = load()
+        m = prob.mesh_struct()
+        rays = (N.PbgpuRays * 3)(*[prob.rays_struct(a) for a in range(3)])
+        pos, q, _ = prob.atoms()
+        self.pos, self.q = np.ascontiguousarray(pos), np.ascontiguousarray(q)
+        md = prob.model()
+        self.s = self.L.oracle_create(C.byref(m), rays, len(q), _d(self.pos), _d(self.q), C.byref(md))
+        if not self.s:
+            raise RuntimeError("oracle_create failed")
+        self.n, self.n_oct, self.na = m.n_nodes, m.n_oct, len(q)
+
+    def close(self):
+        if self.s:
+            self.L.oracle_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ok(self, st):
+        if st != 0:
+            raise RuntimeError("oracle status %d" % st)
+
+    def markers(self):
+        self._ok(self.L.oracle_markers(self.s))
+        marker = np.zeros(self.n_oct)
+        nb = C.c_int64()
+        self._ok(self.L.oracle_get_markers(self.s, _d(marker), C.byref(nb), None))
+        border = np.zeros(nb.value, dtype=np.int32)
+        self._ok(self.L.oracle_get_markers(self.s, None, C.byref(nb), border.ctypes.data_as(P(C.c_int32))))
+        return marker, border
+
+    def node_coeffs(self):
+        e, r = np.zeros(self.n), np.zeros(self.n)
+        self._ok(self.L.oracle_get_node_coeffs(self.s, _d(e), _d(r)))
+        return e, r
+
+    def fractions(self, nb):
+        f = np.zeros(12 * nb)
+        self._ok(self.L.oracle_get_fractions(self.s, _d(f)))
+        return f.reshape(-1, 12)
+
+    def density(self):
+        self._ok(self.L.oracle_density(self.s))
+        rho, vp = np.zeros(self.n), np.zeros(self.n)
+        self._ok(self.L.oracle_get_density(self.s, _d(rho), _d(vp)))
+        return rho, vp
+
+    def assemble(self):
+        self._ok(self.L.oracle_assemble(self.s))
+        return self.system()
+
+    def system(self):
+        nnz = C.c_int64()
+        self._ok(self.L.oracle_get_system(self.s, C.byref(nnz), None, None, None, None))
+        rp = np.zeros(self.n + 1, dtype=np.int64)
+        col = np.zeros(nnz.value, dtype=np.int32)
+        val = np.zeros(nnz.value)
+        rhs = np.zeros(self.n)
+        self._ok(self.L.oracle_get_system(self.s, None, rp.ctypes.data_as(P(C.c_int64)),
+                                          col.ctypes.data_as(P(C.c_int32)), _d(val), _d(rhs)))
+        return rp, col, val, rhs
+
+    def set_system(self, rp, col, val, rhs):
+        rp = np.ascontiguousarray(rp, dtype=np.int64)
+        col = np.ascontiguousarray(col, dtype=np.int32)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        self._ok(self.L.oracle_set_system(self.s, self.n, rp.ctypes.data_as(P(C.c_int64)),
+                                          col.ctypes.data_as(P(C.c_int32)), _d(val), _d(rhs)))
+
+    def solve(self, method="cg", tol=1e-12, max_iter=100000, threads=0):
+        rel = C.c_double()
+        it = self.L.oracle_solve(self.s, 0 if method == "cg" else 1, tol, max_iter, threads, C.byref(rel))
+        if it < 0:
+            raise RuntimeError("oracle_solve failed")
+        phi = np.zeros(self.n)
+        self._ok(self.L.oracle_get_phi(self.s, _d(phi)))
+        return phi, it, rel.value
+
+    def set_phi(self, phi):
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        self._ok(self.L.oracle_set_phi(self.s, _d(phi)))
+
+    def phi_on_atoms(self):
+        out = np.zeros(self.na)
+        self._ok(self.L.oracle_phi_on_atoms(self.s, _d(out)))
+        return out
+
+    def energy(self, fast=False):
+        e = N.PbgpuEnergyOut()
+        self._ok(self.L.oracle_energy(self.s, 1 if fast else 0, C.byref(e)))
+        return e.as_dict()
+
+    def spmv(self, x, threads=0):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(self.n)
+        self._ok(self.L.oracle_spmv(self.s, _d(x), _d(y), threads))
+        return y
+
+    def time_cg(self, iters, threads=0):
+        return self.L.oracle_time_cg_iterations(self.s, iters, threads)
+
+    def run(self, method="cg", tol=1e-12, fast=False):
+        """markers -> density -> assemble -> solve -> energy."""
+        self.markers()
+        self.density()
+        self.assemble()
+        phi, it, rel = self.solve(method, tol)
+        return self.energy(fast), phi, it, rel
