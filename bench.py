@@ -1,0 +1,451 @@
+"""Benchmark of the PB assemble/solve/energy path (one JSON line on rank 0).
+
+A step is one complete PB solve of one molecule through the GPU path:
+create_markers -> create_density_map -> assemble (SELL-C-sigma) -> Krylov solve
+-> potential at atoms -> energy.  Default workload (the plain-FP64 2,000-atom
+configuration): a seeded synthetic globular molecule, 2,000 atoms on a lattice
+subset inside an 18 A sphere, net charge -3 e, mesh_shape 0 at scale 2/A with 3
+surface refinement levels, Jacobi-CG to a relative residual of 1e-8.
+
+value   solves/s with mesh, rays and atoms already resident in HBM.
+e2e     the same, through the C ABI from pinned host buffers: every step uploads
+        the inputs (pbgpu_set_mesh / set_rays / set_atoms / set_model) and reads
+        back the potential at the atoms and the energies.
+Multi-GPU (torchrun): one process per GPU, each solving its own copy of the
+molecule (independent solves, no data-path collective); timing is the max over
+ranks.  --impl reference times the CPU restatement of the reference path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "PB solves/s + p50/p99 latency vs plain FP64 GPU solve at <=1e-6 energy err"
+FALLBACK_HBM_GBS = 6650.0
+
+WORKLOADS = {
+    # name: (n_atoms, radius, net charge, seed, scale, levels)
+    "mol2000": (2000, 18.0, -3.0, 2000, 2.0, 3),
+    "mol300": (300, 11.0, -3.0, 300, 2.0, 2),
+    "mol60": (60, 7.0, -3.0, 60, 2.0, 1),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def spmv_traffic():
+    """DRAM bytes per SpMV launch from the committed ncu summary, scaled to the
+    bench workload by nnz when the capture was on a smaller case."""
+    p = os.path.join(ROOT, "profiles", "spmv_traffic.json")
+    try:
+        return json.load(open(p))
+    except Exception:
+        return None
+
+
+def build_problem(name):
+    from cudanextgenpb_b200 import configs
+    na, rad, net, seed, scale, levels = WORKLOADS[name]
+    prob = configs.make_globular_problem(na, rad, net, seed, scale=scale, levels=levels)
+    t0 = time.time()
+    prob.build()
+    log("host problem %s built in %.1fs: %s" % (name, time.time() - t0,
+                                                 {k: prob.info()[k] for k in ("n_oct", "n_nodes", "n_hang")}))
+    return prob
+
+
+def pinned_inputs(prob):
+    """Copies of the mesh / ray / atom host arrays in pinned memory, and the
+    pbgpu structures pointing at them."""
+    import ctypes as C
+
+    import torch
+
+    from cudanextgenpb_b200 import _native as N
+    keep = []
+
+    def pin(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        keep.append(t)
+        return t
+
+    def ptr(t, ct):
+        return C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ct))
+
+    m = prob.mesh()
+    ms = N.PbgpuMesh()
+    ms.n_oct, ms.n_nodes, ms.n_hang = m["n_oct"], m["n_nodes"], m["n_hang"]
+    t = pin(m["oct_xyz"].reshape(-1)); ms.oct_xyz = ptr(t, C.c_int32)
+    t = pin(m["oct_level"]); ms.oct_level = ptr(t, C.c_int8)
+    t = pin(m["oct_nodes"].reshape(-1)); ms.oct_nodes = ptr(t, C.c_int32)
+    t = pin(m["node_xyz"].reshape(-1)); ms.node_xyz = ptr(t, C.c_int32)
+    t = pin(m["hang_np"] if m["n_hang"] else np.zeros(1, np.int8)); ms.hang_np = ptr(t, C.c_int8)
+    t = pin(m["hang_par"].reshape(-1) if m["n_hang"] else np.zeros(4, np.int32)); ms.hang_par = ptr(t, C.c_int32)
+    for a in range(3):
+        ms.lo[a], ms.hi[a] = m["lo"][a], m["hi"][a]
+    ms.locate_tol = m["locate_tol"]
+    h2d = sum(int(x.numel() * x.element_size()) for x in keep)
+    rays = []
+    for a in range(3):
+        r = prob.rays(a)
+        rs = N.PbgpuRays()
+        rs.n_rays = len(r["keys"])
+        k0 = len(keep)
+        t = pin(r["keys"].view(np.int64)); rs.keys = ptr(t, C.c_uint64)
+        t = pin(r["ptr"]); rs.ptr = ptr(t, C.c_int64)
+        t = pin(r["inters"]); rs.inters = ptr(t, C.c_double)
+        t = pin(r["normals"].reshape(-1)); rs.normals = ptr(t, C.c_double)
+        h2d += sum(int(x.numel() * x.element_size()) for x in keep[k0:])
+        rays.append(rs)
+    pos, q, _ = prob.atoms()
+    tp, tq = pin(pos.reshape(-1)), pin(q)
+    h2d += int(tp.numel() * 8 + tq.numel() * 8)
+    return {"mesh": ms, "rays": rays, "pos": ptr(tp, C.c_double), "q": ptr(tq, C.c_double), "na": len(q),
+            "model": prob.model(), "keep": keep, "h2d_bytes": h2d}
+
+
+def run_ours(args, rank, world, local):
+    import ctypes as C
+
+    import torch
+
+    from cudanextgenpb_b200 import GpuPath, solver_opts
+    from cudanextgenpb_b200 import _native as N
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    prob = build_problem(args.workload)
+    stream = torch.cuda.Stream()
+    g = GpuPath(local, stream=stream.cuda_stream).load(prob)
+    opts = solver_opts("cg", tol=args.tol, max_iter=50000)
+    info = prob.info()
+
+    def step():
+        g.create_markers()
+        g.create_density_map()
+        g.assemble(args.chunk, args.sigma)
+        st = g.solve(opts)
+        pa = g.phi_on_atoms()
+        e = g.energy(False)
+        return st, e, pa
+
+    # warm-up
+    for _ in range(args.warmup):
+        st, e, _ = step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    g.set_profiling(True)
+    g.reset_counters()
+    clocks = Clocks(local)
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    lat = []
+    energies = []
+    iters = []
+    t_start.record(stream)
+    for _ in range(args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        st, e, _ = step()
+        b.record(stream)
+        b.synchronize()
+        lat.append(a.elapsed_time(b))
+        energies.append(e["sum"])
+        iters.append(st.iterations)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = t_start.elapsed_time(t_end)
+    cnt = g.counters()
+    stage = g.stage_ms()
+    g.set_profiling(False)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+
+    # end to end through the C ABI from pinned host buffers
+    lib = N.load_gpu()
+    pin = pinned_inputs(prob)
+    ctx = g._ctx
+    out_atoms = torch.empty(pin["na"], dtype=torch.float64).pin_memory()
+    e_out = N.PbgpuEnergyOut()
+
+    def e2e_step():
+        assert lib.pbgpu_set_mesh(ctx, C.byref(pin["mesh"])) == 0
+        for a in range(3):
+            assert lib.pbgpu_set_rays(ctx, a, C.byref(pin["rays"][a])) == 0
+        assert lib.pbgpu_set_atoms(ctx, pin["na"], pin["pos"], pin["q"]) == 0
+        assert lib.pbgpu_set_model(ctx, C.byref(pin["model"])) == 0
+        assert lib.pbgpu_create_markers(ctx) == 0
+        assert lib.pbgpu_create_density_map(ctx) == 0
+        so = N.PbgpuSellOpts(args.chunk, args.sigma)
+        assert lib.pbgpu_assemble(ctx, C.byref(so)) == 0
+        s = N.PbgpuSolveStats()
+        assert lib.pbgpu_solve(ctx, C.byref(opts), C.byref(s)) == 0
+        assert lib.pbgpu_phi_on_atoms(ctx, C.cast(C.c_void_p(out_atoms.data_ptr()), C.POINTER(C.c_double))) == 0
+        assert lib.pbgpu_energy(ctx, 0, C.byref(e_out)) == 0
+
+    e2e_step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+
+    result = None
+    if rank == 0:
+        value = world * args.steps / (ms / 1e3)
+        e2e = world * args.steps / (ms_e2e / 1e3)
+        peak, peak_kind = measured_peak()
+        spmv_avg_ms = cnt["spmv_ms"] / max(cnt["spmv_launches"], 1)
+        achieved = cnt["spmv_bytes"] / (spmv_avg_ms / 1e3) / 1e9 if cnt["spmv_launches"] else None
+        tr = spmv_traffic()
+        traffic = None
+        if tr:
+            traffic = tr["dram_bytes_per_launch"] * (info_nnz(g) / tr["nnz"]) if tr.get("nnz") else None
+        result = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "solves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic",
+            "config": {
+                "workload": workload_desc(args.workload, info),
+                "n_dof": info["n_nodes"], "n_octants": info["n_oct"], "n_hanging": info["n_hang"],
+                "n_atoms": info["n_atoms"], "nnz": info_nnz(g), "cg_iterations": int(np.median(iters)),
+                "tol": args.tol, "sell": {"C": args.chunk, "sigma": args.sigma},
+                "energy_kT": energies[-1],
+                "dof_iterations_per_s": world * info["n_nodes"] * float(np.median(iters)) / (ms / 1e3 / args.steps),
+                "stage_ms": stage,
+                "l2": "inputs larger than L2 (126 MB): every step streams the mesh, matrix and vectors from HBM",
+                "parallelism": "replicas (one independent solve per GPU)",
+            },
+            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": pin["h2d_bytes"],
+                    "d2h_bytes_per_step": int(8 * pin["na"] + 48)},
+            "roofline": {"kernel": "k_cg_spmv<double> (SELL-C-sigma SpMV fused with p.Ap)", "bound": "hbm",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": cnt["spmv_bytes"],
+                         "avg_launch_ms": spmv_avg_ms, "launches_timed": cnt["spmv_launches"]},
+            "gpu_launches": cnt["launches"],
+            "clocks": ck,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline(prob, g, int(np.median(iters)), args)
+    g.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def info_nnz(g):
+    import ctypes as C
+    nnz = C.c_int64()
+    g._lib.pbgpu_get_system(g._ctx, C.byref(nnz), None, None, None, None)
+    return int(nnz.value)
+
+
+def workload_desc(name, info):
+    na, rad, net, seed, scale, levels = WORKLOADS[name]
+    return ("synthetic globular molecule: %d atoms (FCC-lattice subset in a %.0f A sphere, net %+g e, seed %d), "
+            "mesh_shape 0 scale %g/A, %d surface levels -> %d DoF; FP64 Jacobi-CG" %
+            (na, rad, net, seed, scale, levels, info["n_nodes"]))
+
+
+def cpu_baseline(prob, g, gpu_iters, args):
+    """The oracle's Jacobi-CG on the same assembled system, all host cores: a
+    bounded sample of iterations, scaled to solves/s with the GPU's iteration
+    count.  Assembly and energy are not timed on the CPU side."""
+    from oracle_lib import Oracle
+    o = Oracle(prob)
+    rp, col, val, rhs = g.system()
+    o.set_system(rp, col, val, rhs)
+    threads = os.cpu_count() or 1
+    it = args.cpu_iters
+    t = o.time_cg(it, threads)
+    per_iter = t / it
+    o.close()
+    return {"value": 1.0 / (per_iter * gpu_iters), "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": "%d Jacobi-CG iterations of the CPU oracle on the same %d-DoF system (%.2f s, %.1f ms/iter), "
+                      "scaled by the GPU's %d iterations per solve; assembly and energy excluded"
+                      % (it, g.n, t, 1e3 * per_iter, gpu_iters)}
+
+
+def run_reference(args, rank, world):
+    """CPU restatement of the reference path (oracle port), rank 0 only."""
+    if rank != 0:
+        return None
+    from oracle_lib import Oracle
+    prob = build_problem(args.workload)
+    info = prob.info()
+    o = Oracle(prob)
+    t0 = time.time()
+    o.markers()
+    o.density()
+    o.assemble()
+    t_setup = time.time() - t0
+    # iterations the full solve needs, from a converged CPU solve on a small sample budget
+    phi, iters, rel = o.solve("cg", args.tol, max_iter=args.cpu_iters)
+    threads = os.cpu_count() or 1
+    samples = []
+    for _ in range(args.warmup):
+        o.time_cg(args.cpu_iters, threads)
+    for _ in range(args.steps):
+        samples.append(o.time_cg(args.cpu_iters, threads) / args.cpu_iters)
+    per_iter = float(np.median(samples))
+    need = args.ref_iters if args.ref_iters else iters
+    sec = t_setup + per_iter * need
+    v = 1.0 / sec
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_desc(args.workload, info), "n_dof": info["n_nodes"]},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port",
+                             "sample": "CPU oracle: markers+density+assembly timed once (%.2f s), %d Jacobi-CG "
+                                       "iterations per step timed, scaled to %d iterations per solve"
+                                       % (t_setup, args.cpu_iters, need)},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mol2000", choices=sorted(WORKLOADS))
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--chunk", type=int, default=32)
+    ap.add_argument("--sigma", type=int, default=32)
+    ap.add_argument("--cpu-iters", type=int, default=30)
+    ap.add_argument("--ref-iters", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_env()
+    from cudanextgenpb_b200 import build as b
+    if rank == 0:
+        b.build_all()
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+    else:
+        res = run_ours(args, rank, world, local)
+    if rank == 0 and res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -54,6 +54,11 @@ class PbgpuEnergyOut(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class PbgpuCounters(C.Structure):
+    _fields_ = [("launches", i64), ("spmv_launches", i64), ("spmv_ms", dbl), ("spmv_bytes", dbl),
+                ("krylov_iterations", i64)]
+
+
 class PbhostInfo(C.Structure):
     _fields_ = [("mesh_shape", C.c_int), ("unilevel", C.c_int), ("minlevel", C.c_int), ("maxlevel", C.c_int),
                 ("outlevel", C.c_int), ("scale_level", C.c_int), ("loc_refinement", C.c_int), ("scale", dbl),
@@ -96,6 +101,9 @@ PBGPU_FUNCS = {
     "pbgpu_get_system": (C.c_int, [ctx_p, P(i64), P(i64), P(i32), P(dbl), P(dbl)]),
     "pbgpu_get_phi": (C.c_int, [ctx_p, P(dbl)]),
     "pbgpu_get_stage_ms": (C.c_int, [ctx_p, P(dbl)]),
+    "pbgpu_set_profiling": (C.c_int, [ctx_p, C.c_int]),
+    "pbgpu_get_counters": (C.c_int, [ctx_p, P(PbgpuCounters)]),
+    "pbgpu_reset_counters": (C.c_int, [ctx_p]),
 }
 
 host_p = C.c_void_p

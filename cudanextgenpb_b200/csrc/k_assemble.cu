@@ -295,6 +295,13 @@ __global__ void k_sigma_keys(const int32_t* __restrict__ rowlen, int64_t n, int 
   id[i] = (int32_t)i;
 }
 
+__global__ void k_sum_rowlen(const int32_t* __restrict__ rowlen, int64_t n, unsigned long long* __restrict__ total) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  unsigned long long v = i < n ? (unsigned long long)rowlen[i] : 0ull;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(total, v);
+}
+
 __global__ void k_identity(int32_t* __restrict__ perm, int64_t n) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) perm[i] = (int32_t)i;
@@ -336,7 +343,7 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   k_dirichlet<<<grid_for(n, 128), 128, 0, c->stream>>>(c->node_xyz.get(), n, c->model.bc_type, lo, len,
                                                         c->atoms.get(), c->na, c->eps_in, c->eps_out, c->kappa,
                                                         c->dirichlet.get(), c->gval.get());
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
 
   AsmView A;
   A.inc_ptr = c->inc_ptr.get();
@@ -365,7 +372,7 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   PBGPU_CUDA(c, ovf.alloc(1));
   PBGPU_CUDA(c, cudaMemsetAsync(ovf.get(), 0, sizeof(int), c->stream));
   k_row_len<<<grid_for(n, 128), 128, 0, c->stream>>>(A, c->rowlen.get(), ovf.get());
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   int h_ovf = 0;
   PBGPU_CUDA(c, cudaMemcpyAsync(&h_ovf, ovf.get(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -382,20 +389,21 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
     PBGPU_CUDA(c, k1.alloc(n));
     PBGPU_CUDA(c, id0.alloc(n));
     k_sigma_keys<<<grid_for(n, 256), 256, 0, c->stream>>>(c->rowlen.get(), n, sigma, k0.get(), id0.get());
-    PBGPU_CUDA(c, cudaGetLastError());
+    PBGPU_LAUNCHED(c);
     size_t bytes = 0;
     PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0.get(), k1.get(), id0.get(), c->perm.get(), (int)n,
                                                   0, 64, c->stream));
     PBGPU_CUDA(c, ensure_tmp(c, bytes));
     PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(c->tmp.get(), bytes, k0.get(), k1.get(), id0.get(), c->perm.get(),
                                                   (int)n, 0, 64, c->stream));
+    c->launches += cub_radix_launches(n, 64);
     PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   } else {
     k_identity<<<grid_for(n, 256), 256, 0, c->stream>>>(c->perm.get(), n);
-    PBGPU_CUDA(c, cudaGetLastError());
+    PBGPU_LAUNCHED(c);
   }
   k_iperm<<<grid_for(n, 256), 256, 0, c->stream>>>(c->perm.get(), n, c->iperm.get());
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   PBGPU_CUDA(c, c->slice_w.alloc(n_slices));
   PBGPU_CUDA(c, c->slice_ptr.alloc(n_slices + 1));
   DBuf<int64_t> elems;
@@ -403,22 +411,22 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   PBGPU_CUDA(c, cudaMemsetAsync(elems.get(), 0, (n_slices + 1) * sizeof(int64_t), c->stream));
   k_slice_width<<<grid_for(n_slices, 128), 128, 0, c->stream>>>(c->perm.get(), c->rowlen.get(), n, n_slices, C,
                                                                  c->slice_w.get(), elems.get());
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   size_t bytes = 0;
   PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, bytes, elems.get(), c->slice_ptr.get(), n_slices + 1, c->stream));
   PBGPU_CUDA(c, ensure_tmp(c, bytes));
   PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(c->tmp.get(), bytes, elems.get(), c->slice_ptr.get(), n_slices + 1,
                                               c->stream));
+  c->launches += kCubScanLaunches;
   int64_t total = 0;
   PBGPU_CUDA(c, cudaMemcpyAsync(&total, c->slice_ptr.get() + n_slices, sizeof(int64_t), cudaMemcpyDeviceToHost,
                                 c->stream));
   // nnz = sum of row lengths
-  DBuf<int64_t> nnz_d;
+  DBuf<unsigned long long> nnz_d;
   PBGPU_CUDA(c, nnz_d.alloc(1));
-  bytes = 0;
-  PBGPU_CUDA(c, cub::DeviceReduce::Sum(nullptr, bytes, c->rowlen.get(), nnz_d.get(), n, c->stream));
-  PBGPU_CUDA(c, ensure_tmp(c, bytes));
-  PBGPU_CUDA(c, cub::DeviceReduce::Sum(c->tmp.get(), bytes, c->rowlen.get(), nnz_d.get(), n, c->stream));
+  PBGPU_CUDA(c, cudaMemsetAsync(nnz_d.get(), 0, sizeof(unsigned long long), c->stream));
+  k_sum_rowlen<<<grid_for(n, 256), 256, 0, c->stream>>>(c->rowlen.get(), n, nnz_d.get());
+  PBGPU_LAUNCHED(c);
   int64_t nnz = 0;
   PBGPU_CUDA(c, cudaMemcpyAsync(&nnz, nnz_d.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -432,10 +440,10 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   SellOut S{c->slice_ptr.get(), c->slice_w.get(), c->iperm.get(), c->scol.get(), c->sval.get(), c->b.get(),
             c->dinv.get(), C};
   k_row_fill<<<grid_for(n, 128), 128, 0, c->stream>>>(A, S);
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   if (n_pad > n) {
     k_pad_rows<<<grid_for(n_pad - n, 128), 128, 0, c->stream>>>(S, n, n_pad);
-    PBGPU_CUDA(c, cudaGetLastError());
+    PBGPU_LAUNCHED(c);
   }
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   c->have_system = true;

@@ -104,12 +104,13 @@ int build_incidence(Context* c) {
   PBGPU_CUDA(c, cudaMemsetAsync(cnt.get(), 0, (n + 1) * sizeof(int32_t), c->stream));
   k_inc_count<<<grid_for(n8, 256), 256, 0, c->stream>>>(c->oct_nodes.get(), n8, n, c->hang_par.get(),
                                                          c->hang_np.get(), cnt.get());
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   PBGPU_CUDA(c, c->inc_ptr.alloc(n + 1));
   size_t bytes = 0;
   PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt.get(), c->inc_ptr.get(), n + 1, c->stream));
   PBGPU_CUDA(c, ensure_tmp(c, bytes));
   PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(c->tmp.get(), bytes, cnt.get(), c->inc_ptr.get(), n + 1, c->stream));
+  c->launches += kCubScanLaunches;
   int64_t total = 0;
   PBGPU_CUDA(c, cudaMemcpyAsync(&total, c->inc_ptr.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -117,9 +118,9 @@ int build_incidence(Context* c) {
   PBGPU_CUDA(c, cudaMemsetAsync(cnt.get(), 0, (n + 1) * sizeof(int32_t), c->stream));
   k_inc_fill<<<grid_for(n8, 256), 256, 0, c->stream>>>(c->oct_nodes.get(), n8, n, c->hang_par.get(), c->hang_np.get(),
                                                         c->inc_ptr.get(), cnt.get(), c->inc.get());
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   k_inc_sort<<<grid_for(n, 128), 128, 0, c->stream>>>(c->inc_ptr.get(), c->inc.get(), n);
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   c->have_incidence = true;
   return PBGPU_OK;
@@ -289,13 +290,13 @@ int run_density(Context* c) {
   PBGPU_CUDA(c, c->rho.alloc(n));
   k_vol_patch<<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->inc_ptr.get(), c->inc.get(), c->oct.get(),
                                                         c->oct_nodes.get(), c->hang_np.get(), g, c->vol_patch.get());
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   PBGPU_CUDA(c, cudaMemsetAsync(c->rho.get(), 0, n * sizeof(double), c->stream));
   PBGPU_CUDA(c, c->atom_oct.alloc(na > 0 ? na : 1));
   if (na > 0) {
     k_locate_atoms<<<grid_for(na, 128), 128, 0, c->stream>>>(c->atoms.get(), na, c->oct_key.get(), c->oct.get(),
                                                               c->n_oct, g, c->tol, c->atom_oct.get());
-    PBGPU_CUDA(c, cudaGetLastError());
+    PBGPU_LAUNCHED(c);
     const int64_t m = 32 * na;
     DBuf<uint64_t> k0, k1;
     DBuf<double> v0, v1;
@@ -306,15 +307,16 @@ int run_density(Context* c) {
     k_charge_contrib<<<grid_for(8 * na, 128), 128, 0, c->stream>>>(
         c->atoms.get(), na, c->atom_oct.get(), c->oct.get(), c->oct_nodes.get(), n, c->hang_par.get(),
         c->hang_np.get(), c->vol_patch.get(), g, k0.get(), v0.get());
-    PBGPU_CUDA(c, cudaGetLastError());
+    PBGPU_LAUNCHED(c);
     size_t bytes = 0;
     PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0.get(), k1.get(), v0.get(), v1.get(), (int)m, 0,
                                                   64, c->stream));
     PBGPU_CUDA(c, ensure_tmp(c, bytes));
     PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(c->tmp.get(), bytes, k0.get(), k1.get(), v0.get(), v1.get(), (int)m,
                                                   0, 64, c->stream));
+    c->launches += cub_radix_launches(m, 64);
     k_segment_sum<<<grid_for(m, 256), 256, 0, c->stream>>>(k1.get(), v1.get(), m, c->rho.get());
-    PBGPU_CUDA(c, cudaGetLastError());
+    PBGPU_LAUNCHED(c);
     PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   }
   c->have_density = true;

@@ -365,7 +365,7 @@ int run_phi_atoms(Context* c, double* out) {
   PBGPU_CUDA(c, d.alloc(c->na));
   EnergyView E = energy_view(c, 0);
   k_phi_atoms<<<grid_for(c->na, 128), 128, 0, c->stream>>>(c->atoms.get(), c->na, c->atom_oct.get(), E, d.get());
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   PBGPU_CUDA(c, cudaMemcpyAsync(out, d.get(), c->na * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   return PBGPU_OK;
@@ -435,12 +435,13 @@ int run_energy(Context* c, int fast, pbgpu_energy_out* out) {
     PBGPU_CUDA(c, cudaMemsetAsync(nf.get() + nb, 0, sizeof(int32_t), c->stream));
     PBGPU_CUDA(c, cudaMemsetAsync(nt.get() + nb, 0, sizeof(int32_t), c->stream));
     k_energy_count<<<grid_for(nb, 128), 128, 0, c->stream>>>(E, nf.get(), nt.get());
-    PBGPU_CUDA(c, cudaGetLastError());
+    PBGPU_LAUNCHED(c);
     size_t bytes = 0;
     PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, bytes, nf.get(), of.get(), nb + 1, c->stream));
     PBGPU_CUDA(c, ensure_tmp(c, bytes));
     PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(c->tmp.get(), bytes, nf.get(), of.get(), nb + 1, c->stream));
     PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(c->tmp.get(), bytes, nt.get(), ot.get(), nb + 1, c->stream));
+    c->launches += 2 * kCubScanLaunches;
     int64_t nflux = 0, ntri = 0;
     PBGPU_CUDA(c, cudaMemcpyAsync(&nflux, of.get() + nb, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
     PBGPU_CUDA(c, cudaMemcpyAsync(&ntri, ot.get() + nb, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
@@ -450,27 +451,27 @@ int run_energy(Context* c, int fast, pbgpu_energy_out* out) {
     PBGPU_CUDA(c, tv.alloc(ntri > 0 ? ntri : 1));
     PBGPU_CUDA(c, tn.alloc(ntri > 0 ? ntri : 1));
     k_energy_fill<<<grid_for(nb, 128), 128, 0, c->stream>>>(E, of.get(), ot.get(), fl.get(), tv.get(), tn.get());
-    PBGPU_CUDA(c, cudaGetLastError());
+    PBGPU_LAUNCHED(c);
     double* P = c->energy_part.get();
     if (nflux) {
       k_flux_total<<<nblk, kTile, 0, c->stream>>>(fl.get(), nflux, P);
-      PBGPU_CUDA(c, cudaGetLastError());
+      PBGPU_LAUNCHED(c);
       if ((st = sum_partials(c, P, nblk, &charge_pol)) != PBGPU_OK) return st;
       if (m) {
         k_nbody_flux<<<nblk, kTile, 0, c->stream>>>(fl.get(), nflux, dq.get(), m, P);
-        PBGPU_CUDA(c, cudaGetLastError());
+        PBGPU_LAUNCHED(c);
         if ((st = sum_partials(c, P, nblk, &first_int)) != PBGPU_OK) return st;
       }
     }
     if (ionic && ntri && m) {
       k_nbody_tri<<<nblk, kTile, 0, c->stream>>>(tv.get(), tn.get(), ntri, dq.get(), m, P);
-      PBGPU_CUDA(c, cudaGetLastError());
+      PBGPU_LAUNCHED(c);
       if ((st = sum_partials(c, P, nblk, &second_int)) != PBGPU_OK) return st;
     }
   }
   if (c->model.calc_coulombic == 1 && m > 1) {
     k_coulomb<<<nblk, kTile, 0, c->stream>>>(dq.get(), m, c->energy_part.get());
-    PBGPU_CUDA(c, cudaGetLastError());
+    PBGPU_LAUNCHED(c);
     if ((st = sum_partials(c, c->energy_part.get(), nblk, &coul)) != PBGPU_OK) return st;
     coul *= 1.0 / c->eps_in;
   }

@@ -446,32 +446,57 @@ static int krylov(Context* c, int method, const KrylovVecs<T>& K, double tol, in
   else
     k_bicg_init<T><<<G, kBlock, 0, c->stream>>>(n, K.b, K.x, K.r, K.rh, K.p, K.v, ks, part, tol);
   PBGPU_CUDA(c, cudaGetLastError());
+  c->launches += 1;
+  // With profiling on, events recorded around every SpMV launch become event
+  // nodes of the graph; the elapsed times of the launches that did work are
+  // summed after each chunk.
+  const int spmv_per_it = method == PBGPU_CG ? 1 : 2;
+  std::vector<cudaEvent_t> ev;
+  if (c->profiling) {
+    ev.resize(2 * spmv_per_it * check_every);
+    for (cudaEvent_t& e : ev) PBGPU_CUDA(c, cudaEventCreate(&e));
+  }
+  auto mark = [&](int k, int which, int end) {
+    if (c->profiling) cudaEventRecord(ev[2 * (k * spmv_per_it + which) + end], c->stream);
+  };
   // the chunk of iterations is captured once and replayed
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   PBGPU_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   for (int k = 0; k < check_every; ++k) {
     if (method == PBGPU_CG) {
+      mark(k, 0, 0);
       k_cg_spmv<T><<<G, kBlock, 0, c->stream>>>(K.A, K.p, K.q, ks, part);
+      mark(k, 0, 1);
       k_cg_update<T><<<G, kBlock, 0, c->stream>>>(n, K.x, K.r, K.p, K.q, K.dinv, ks, part);
       k_cg_pupdate<T><<<G, kBlock, 0, c->stream>>>(n, K.p, K.r, K.dinv, ks);
     } else {
       k_bicg_p<T><<<G, kBlock, 0, c->stream>>>(n, K.p, K.ph, K.r, K.v, K.dinv, ks);
+      mark(k, 0, 0);
       k_bicg_v<T><<<G, kBlock, 0, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
+      mark(k, 0, 1);
       k_bicg_s<T><<<G, kBlock, 0, c->stream>>>(n, K.r, K.v, K.s, K.sh, K.dinv, ks, part);
+      mark(k, 1, 0);
       k_bicg_t<T><<<G, kBlock, 0, c->stream>>>(K.A, K.sh, K.t, K.s, ks, part);
+      mark(k, 1, 1);
       k_bicg_x<T><<<G, kBlock, 0, c->stream>>>(n, K.x, K.r, K.ph, K.sh, K.s, K.t, K.rh, ks, part);
     }
   }
   cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
-  if (ce != cudaSuccess) return cuda_fail(c, ce, "cudaStreamEndCapture");
+  if (ce != cudaSuccess) {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    return cuda_fail(c, ce, "cudaStreamEndCapture");
+  }
   ce = cudaGraphInstantiate(&exec, graph, 0);
   if (ce != cudaSuccess) {
     cudaGraphDestroy(graph);
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
     return cuda_fail(c, ce, "cudaGraphInstantiate");
   }
+  const int kernels_per_chunk = (method == PBGPU_CG ? 3 : 5) * check_every;
   int rc = PBGPU_OK;
   const int max_chunks = max_iter / check_every + 2;
+  int prev_iter = 0;
   for (int chunk = 0; chunk < max_chunks; ++chunk) {
     ce = cudaGraphLaunch(exec, c->stream);
     if (ce == cudaSuccess)
@@ -481,12 +506,33 @@ static int krylov(Context* c, int method, const KrylovVecs<T>& K, double tol, in
       rc = cuda_fail(c, ce, "krylov chunk");
       break;
     }
+    c->launches += kernels_per_chunk;
+    const int now = c->ks_host->iter;
+    if (c->profiling) {
+      // iteration k of this chunk did its SpMV(s) when it is below the count
+      // of completed iterations; the t-SpMV of a BiCGStab iteration that
+      // stopped on ||s|| did not run
+      for (int k = 0; k < check_every && prev_iter + k < now; ++k)
+        for (int w = 0; w < spmv_per_it; ++w) {
+          if (w == 1 && prev_iter + k == now - 1 && c->ks_host->s_conv) continue;
+          float ms = 0.f;
+          if (cudaEventElapsedTime(&ms, ev[2 * (k * spmv_per_it + w)], ev[2 * (k * spmv_per_it + w) + 1]) ==
+              cudaSuccess) {
+            c->spmv_ms += ms;
+            c->spmv_launches += 1;
+          }
+        }
+    }
+    prev_iter = now;
     if (c->ks_host->done) break;
   }
   cudaGraphExecDestroy(exec);
   cudaGraphDestroy(graph);
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
   if (rc != PBGPU_OK) return rc;
   *iters = c->ks_host->iter;
+  c->krylov_iters += c->ks_host->iter;
+  c->spmv_bytes = (double)c->nnz * (sizeof(T) + 4) + 2.0 * (double)c->n * sizeof(T);
   *status = c->ks_host->done ? c->ks_host->status : PBGPU_NOT_CONVERGED;
   return PBGPU_OK;
 }
@@ -532,7 +578,8 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
     const int G = grid_blocks(c, c->sell_len);
     k_to_f32<<<G, kBlock, 0, c->stream>>>(c->sell_len, c->sval.get(), c->sval32.get());
     k_to_f32<<<grid_blocks(c, n_pad), kBlock, 0, c->stream>>>(n_pad, c->dinv.get(), c->dinv32.get());
-    PBGPU_CUDA(c, cudaGetLastError());
+    c->launches += 1;
+    PBGPU_LAUNCHED(c);
     SellT<float> A32{c->slice_ptr.get(), c->slice_w.get(), c->scol.get(), c->sval32.get(), n_pad, c->C};
     PBGPU_CUDA(c, cudaMemsetAsync(c->x.get(), 0, n_pad * sizeof(double), c->stream));
     const int max_outer = opt.max_outer > 0 ? opt.max_outer : 50;
@@ -560,7 +607,7 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
       // r = b - A x in fp64, handed to the inner solve in fp32
       k_residual<<<grid_blocks(c, n_pad), kBlock, 0, c->stream>>>(A64, n, c->b.get(), c->x.get(), nullptr,
                                                                   c->b32.get(), c->ks.get(), c->partials.get());
-      PBGPU_CUDA(c, cudaGetLastError());
+      PBGPU_LAUNCHED(c);
       PBGPU_CUDA(c, cudaMemcpyAsync(c->ks_host, c->ks.get(), sizeof(KrylovScalars), cudaMemcpyDeviceToHost, c->stream));
       PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
       const double rr = c->ks_host->rr, bb = c->ks_host->bb;
@@ -584,18 +631,18 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
         break;
       }
       k_axpy_f32<<<grid_blocks(c, n_pad), kBlock, 0, c->stream>>>(n_pad, c->x.get(), c->x32.get());
-      PBGPU_CUDA(c, cudaGetLastError());
+      PBGPU_LAUNCHED(c);
     }
   }
   PBGPU_CUDA(c, cudaEventRecord(c->ev1, c->stream));
   // true residual in fp64
   k_residual<<<grid_blocks(c, n_pad), kBlock, 0, c->stream>>>(A64, n, c->b.get(), c->x.get(), nullptr, nullptr,
                                                               c->ks.get(), c->partials.get());
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   PBGPU_CUDA(c, cudaMemcpyAsync(c->ks_host, c->ks.get(), sizeof(KrylovScalars), cudaMemcpyDeviceToHost, c->stream));
   PBGPU_CUDA(c, c->phi.alloc(n));
   k_gather_phi<<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->iperm.get(), c->x.get(), c->phi.get());
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   float ms = 0;
   PBGPU_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));

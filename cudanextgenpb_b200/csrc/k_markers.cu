@@ -51,7 +51,7 @@ int build_ray_hash_from(Context* c, int axis, const uint64_t* d_keys) {
   PBGPU_CUDA(c, cudaMemsetAsync(ovf.get(), 0, sizeof(int), c->stream));
   k_hash_insert<<<grid_for(R.n, 256), 256, 0, c->stream>>>(d_keys, R.n, R.hkeys.get(), R.hval.get(), R.cap, R.cap_log,
                                                            ovf.get());
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   int h_ovf = 0;
   PBGPU_CUDA(c, cudaMemcpyAsync(&h_ovf, ovf.get(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -173,13 +173,13 @@ int run_markers(Context* c) {
   k_classify_nodes<<<grid_for(n, 256), 256, 0, c->stream>>>(
       c->node_xyz.get(), n, ray_view(c->rays[2]), c->lo[2], c->len[2], c->eps_in, c->eps_out, react_out, stern,
       c->model.stern_layer, c->inside.get(), c->eps.get(), c->react.get());
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   DBuf<uint8_t> flags;
   PBGPU_CUDA(c, flags.alloc(no));
   k_octant_markers<<<grid_for(no, 256), 256, 0, c->stream>>>(c->oct_nodes.get(), no, n, c->inside.get(), stern,
                                                               react_out, c->marker.get(), flags.get(),
                                                               stern ? c->react_cell.get() : nullptr);
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   // border list in ascending octant order
   DBuf<int32_t> sel;
   DBuf<int64_t> nsel;
@@ -190,6 +190,7 @@ int run_markers(Context* c) {
   PBGPU_CUDA(c, cub::DeviceSelect::Flagged(nullptr, bytes, idx, flags.get(), sel.get(), nsel.get(), no, c->stream));
   PBGPU_CUDA(c, ensure_tmp(c, bytes));
   PBGPU_CUDA(c, cub::DeviceSelect::Flagged(c->tmp.get(), bytes, idx, flags.get(), sel.get(), nsel.get(), no, c->stream));
+  c->launches += kCubSelectLaunches;
   int64_t nb = 0;
   PBGPU_CUDA(c, cudaMemcpyAsync(&nb, nsel.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -199,7 +200,7 @@ int run_markers(Context* c) {
   PBGPU_CUDA(c, cudaMemsetAsync(c->border_pos.get(), 0xff, no * sizeof(int32_t), c->stream));
   if (nb) {
     k_border_pos<<<grid_for(nb, 256), 256, 0, c->stream>>>(c->border.get(), nb, c->border_pos.get());
-    PBGPU_CUDA(c, cudaGetLastError());
+    PBGPU_LAUNCHED(c);
   }
   PBGPU_CUDA(c, c->frac.alloc(nb > 0 ? 12 * nb : 12));
   if (nb) {
@@ -208,7 +209,7 @@ int run_markers(Context* c) {
     k_fractions<<<grid_for(12 * nb, 256), 256, 0, c->stream>>>(c->oct.get(), c->border.get(), nb, ray_view(c->rays[0]),
                                                                 ray_view(c->rays[1]), ray_view(c->rays[2]), lo, len,
                                                                 c->frac.get());
-    PBGPU_CUDA(c, cudaGetLastError());
+    PBGPU_LAUNCHED(c);
   }
   // flags/sel are freed at scope exit: make sure the stream is done with them
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));

@@ -180,7 +180,7 @@ int pbgpu_set_mesh(pbgpu_ctx* h, const pbgpu_mesh* m) {
   if ((st = upload(c, c->hang_np, np.data(), np.size())) != PBGPU_OK) return st;
   PBGPU_CUDA(c, c->oct_key.alloc(no));
   launch_oct_keys(c->oct.get(), no, c->oct_key.get(), c->stream);
-  PBGPU_CUDA(c, cudaGetLastError());
+  PBGPU_LAUNCHED(c);
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   c->have_mesh = true;
   return PBGPU_OK;
@@ -439,6 +439,32 @@ int pbgpu_get_stage_ms(pbgpu_ctx* h, double ms[6]) {
   CTX_CHECK(h);
   if (!ms) return PBGPU_ERR_ARG;
   for (int i = 0; i < 6; ++i) ms[i] = h->c.stage_ms[i];
+  return PBGPU_OK;
+}
+
+int pbgpu_set_profiling(pbgpu_ctx* h, int on) {
+  CTX_CHECK(h);
+  h->c.profiling = on != 0;
+  return PBGPU_OK;
+}
+
+int pbgpu_get_counters(pbgpu_ctx* h, pbgpu_counters* out) {
+  CTX_CHECK(h);
+  if (!out) return PBGPU_ERR_ARG;
+  const Context& c = h->c;
+  out->launches = c.launches;
+  out->spmv_launches = c.spmv_launches;
+  out->spmv_ms = c.spmv_ms;
+  out->spmv_bytes = c.spmv_bytes;
+  out->krylov_iterations = c.krylov_iters;
+  return PBGPU_OK;
+}
+
+int pbgpu_reset_counters(pbgpu_ctx* h) {
+  CTX_CHECK(h);
+  Context& c = h->c;
+  c.launches = c.spmv_launches = c.krylov_iters = 0;
+  c.spmv_ms = 0.0;
   return PBGPU_OK;
 }
 

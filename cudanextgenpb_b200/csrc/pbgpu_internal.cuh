@@ -154,6 +154,14 @@ struct Context {
   // ---- scratch for CUB
   DBuf<uint8_t> tmp;
 
+  // ---- measurement
+  bool profiling = false;
+  int64_t launches = 0;       // kernels launched (CUB device algorithms count their kernels)
+  int64_t spmv_launches = 0;
+  double spmv_ms = 0.0;
+  double spmv_bytes = 0.0;
+  int64_t krylov_iters = 0;
+
   int fail(int code, const std::string& msg) {
     err = msg;
     return code;
@@ -167,6 +175,21 @@ int cuda_fail(Context* c, cudaError_t e, const char* what);
     cudaError_t _e = (expr);                                    \
     if (_e != cudaSuccess) return ::pbgpu::cuda_fail((ctx), _e, #expr); \
   } while (0)
+
+// After a kernel launch: count it and check the launch.
+#define PBGPU_LAUNCHED(ctx)                          \
+  do {                                               \
+    (ctx)->launches += 1;                            \
+    PBGPU_CUDA(ctx, cudaGetLastError());             \
+  } while (0)
+
+// Kernels launched by one CUB device-wide call (CUB of CUDA 12.9): scans and
+// flagged selects run an init kernel and a sweep kernel; a radix sort of 64-bit
+// keys runs one single-tile kernel for small inputs, otherwise a histogram, an
+// exclusive-sum and one onesweep pass per 8 key bits.
+constexpr int kCubScanLaunches = 2;
+constexpr int kCubSelectLaunches = 2;
+inline int cub_radix_launches(int64_t n, int bits) { return n <= 3584 ? 1 : 2 + (bits + 7) / 8; }
 
 // ---------------------------------------------------------------------------
 // Device helpers.

@@ -284,6 +284,17 @@ class GpuPath:
         self._check(self._lib.pbgpu_get_stage_ms(self._ctx, ms))
         return dict(zip(["markers", "density", "assemble", "solve", "phi_atoms", "energy"], list(ms)))
 
+    def set_profiling(self, on=True):
+        self._check(self._lib.pbgpu_set_profiling(self._ctx, 1 if on else 0))
+
+    def counters(self) -> dict:
+        c = N.PbgpuCounters()
+        self._check(self._lib.pbgpu_get_counters(self._ctx, C.byref(c)))
+        return {k: getattr(c, k) for k, _ in c._fields_}
+
+    def reset_counters(self):
+        self._check(self._lib.pbgpu_reset_counters(self._ctx))
+
     def run(self, opts=None, fast=False, chunk=32, sigma=None):
         """create_markers .. energy in the driver's order; returns (energy dict, solve stats)."""
         self.create_markers()

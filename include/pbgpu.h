@@ -189,6 +189,22 @@ int pbgpu_get_phi(pbgpu_ctx* ctx, double* phi);
  * solve, phi_on_atoms, energy. */
 int pbgpu_get_stage_ms(pbgpu_ctx* ctx, double ms[6]);
 
+/* Measurement counters (no counterpart in the reference, which has no GPU
+ * path): kernels launched by this context, and — while profiling is on — the
+ * SpMV launches of the Krylov solves with their summed device time from CUDA
+ * events recorded around each launch, and the algorithmic bytes one SpMV moves
+ * (nnz * (value + index) + 2 * n * value). */
+typedef struct {
+  int64_t launches;
+  int64_t spmv_launches;
+  double spmv_ms;
+  double spmv_bytes;
+  int64_t krylov_iterations;
+} pbgpu_counters;
+int pbgpu_set_profiling(pbgpu_ctx* ctx, int on);
+int pbgpu_get_counters(pbgpu_ctx* ctx, pbgpu_counters* out);
+int pbgpu_reset_counters(pbgpu_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,125 @@
+"""The CPU oracle against known answers: the analytic Born / Debye-Hueckel energy
+of a charged sphere, Gauss's law, and self-consistency checks.  The reference
+ships no tests or golden outputs of its own, so these are the pins."""
+import json
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+from cudanextgenpb_b200 import configs
+from oracle_lib import Oracle
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.fixture(scope="module")
+def born():
+    prob = configs.make_born_problem(5, 6).build()
+    o = Oracle(prob)
+    o.markers()
+    o.density()
+    sysm = o.assemble()
+    return prob, o, sysm
+
+
+def test_born_constants_match_reference_values():
+    eps_in, eps_out, k = configs.scaled_constants()
+    # values of the reference's units at T = 298.15 K, I = 0.145 M
+    assert abs(eps_in - 0.0035685016236776) < 1e-15
+    assert abs(eps_out - 0.1427400649471059) < 1e-14
+    assert abs(k - 0.1239941973227606) < 1e-14
+    assert abs(configs.born_energy() - (-68.65400844521548)) < 1e-11
+    assert abs(configs.born_energy(ionic=0.0) - (-68.30597984954667)) < 1e-11
+
+
+def test_born_energy_vs_analytic(born):
+    prob, o, _ = born
+    phi, it, rel = o.solve("bicgstab", 1e-12)
+    assert rel < 1e-11
+    e = o.energy()
+    ref = configs.born_energy()
+    assert abs(e["sum"] - ref) / abs(ref) < 5e-4
+    # the polarisation part is the salt-free Born energy
+    assert abs(e["energy_pol"] - configs.born_energy(ionic=0.0)) / 68.3 < 1e-5
+    # Gauss's law: the flux through the dielectric jump carries the enclosed charge
+    assert abs(e["charge_flux"] - 1.0) < 1e-9
+    assert e["net_charge"] == 1.0 and e["energy_coul"] == 0.0
+
+
+def test_born_energy_converges():
+    errs = []
+    for u, m in ((4, 5), (5, 6), (6, 7)):
+        prob = configs.make_born_problem(u, m).build()
+        o = Oracle(prob)
+        e, _, _, _ = o.run("cg", 1e-12)
+        errs.append(abs(e["sum"] - configs.born_energy()))
+    assert errs[2] < errs[1] < errs[0]
+    assert errs[1] / errs[2] > 2.5  # second order in h
+
+
+def test_matrix_symmetric_and_dirichlet_rows(born):
+    prob, o, (rp, col, val, rhs) = born
+    n = len(rp) - 1
+    A = sp.csr_matrix((val, col, rp), shape=(n, n))
+    assert abs(A - A.T).max() < 1e-12 * abs(A).max()
+    m = prob.mesh()
+    onb = np.any((m["node_xyz"] == 0) | (m["node_xyz"] == 1 << 19), axis=1)
+    d = np.diff(rp)
+    assert np.all(d[onb] == 1) and np.allclose(A.diagonal()[onb], 1.0)
+    # positive diagonal; rows of a uniform region hold the 7-point stencil
+    assert np.all(A.diagonal() > 0)
+    assert np.median(d[~onb]) == 7
+    # Dirichlet columns are eliminated from the other rows
+    cols_of_interior = col[np.repeat(~onb, d)]
+    assert not np.any(onb[cols_of_interior])
+
+
+def test_krylov_vs_direct(born):
+    prob, o, (rp, col, val, rhs) = born
+    n = len(rp) - 1
+    A = sp.csc_matrix(sp.csr_matrix((val, col, rp), shape=(n, n)))
+    x = spla.spsolve(A, rhs)
+    for meth in ("cg", "bicgstab"):
+        phi, it, rel = o.solve(meth, 1e-12)
+        assert np.linalg.norm(phi - x) / np.linalg.norm(x) < 1e-9
+
+
+def test_energy_fast_equals_energy_on_uniform_mesh():
+    # no surface refinement: a uniform mesh without hanging nodes
+    prob = configs.make_born_problem(5, 5).build()
+    assert prob.info()["n_hang"] == 0
+    o = Oracle(prob)
+    e, phi, it, rel = o.run("cg", 1e-12)
+    ef = o.energy(fast=True)
+    for k in ("energy_pol", "energy_react", "charge_flux"):
+        assert ef[k] == pytest.approx(e[k], rel=1e-14, abs=1e-14)
+
+
+def test_density_conserves_charge(born):
+    prob, o, _ = born
+    rho, vp = o.density()
+    # the box integral of rho returns 4 pi q
+    assert abs((rho * vp).sum() / (4 * np.pi) - 1.0) < 1e-12
+    assert abs(vp.sum() - 16.0 ** 3) < 1e-9
+
+
+def test_golden_born_fixture(born):
+    """Regression pin of the oracle against its committed Born fixture
+    (tests/golden/make_golden.py writes it)."""
+    path = os.path.join(HERE, "golden", "born_u5_m6.json")
+    g = json.load(open(path))
+    prob, o, (rp, col, val, rhs) = born
+    info = prob.info()
+    assert [info["n_oct"], info["n_nodes"], info["n_hang"]] == g["mesh_counts"]
+    marker, border = o.markers()
+    assert len(border) == g["n_border"]
+    assert int(rp[-1]) == g["nnz"]
+    assert abs(val.sum() - g["sum_val"]) <= 1e-12 * abs(g["sum_val"])
+    assert abs(rhs.sum() - g["sum_rhs"]) <= 1e-12 * abs(g["sum_rhs"])
+    phi, it, rel = o.solve("cg", 1e-12)
+    e = o.energy()
+    for k in ("energy_pol", "energy_react", "charge_flux"):
+        assert e[k] == pytest.approx(g["energy"][k], rel=1e-9)
