@@ -204,8 +204,9 @@ def run_ours(args, rank, world, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     prob = build_problem(args.workload)
-    stream = torch.cuda.Stream()
-    g = GpuPath(local, stream=stream.cuda_stream).load(prob)
+    g = GpuPath(local).load(prob)
+    # time on the context's own stream
+    stream = torch.cuda.ExternalStream(g.stream_ptr(), device=local)
     opts = solver_opts("cg", tol=args.tol, max_iter=50000)
     info = prob.info()
 

@@ -82,6 +82,7 @@ PBGPU_FUNCS = {
     "pbgpu_ctx_create": (C.c_int, [P(ctx_p), C.c_int, C.c_void_p]),
     "pbgpu_ctx_destroy": (None, [ctx_p]),
     "pbgpu_last_error": (C.c_char_p, [ctx_p]),
+    "pbgpu_ctx_stream": (C.c_void_p, [ctx_p]),
     "pbgpu_set_mesh": (C.c_int, [ctx_p, P(PbgpuMesh)]),
     "pbgpu_set_rays": (C.c_int, [ctx_p, C.c_int, P(PbgpuRays)]),
     "pbgpu_set_atoms": (C.c_int, [ctx_p, i64, P(dbl), P(dbl)]),

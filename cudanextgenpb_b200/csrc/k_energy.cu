@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kTile) k_nbody_flux(const double4* __restrict_
         s += A.w * rsqrt(dx * dx + dy * dy + dz * dz);
       }
     }
-    acc += E.w * s;
+    if (e < ne) acc += E.w * s;  // idle lanes sit at the origin and may hit an atom there
   }
   typedef cub::BlockReduce<double, kTile> BR;
   __shared__ typename BR::TempStorage tmp;
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(kTile) k_nbody_tri(const double4* __restrict__
         s += A.w * (dx * N.x + dy * N.y + dz * N.z) * (ri * ri * ri);
       }
     }
-    acc += V.w * s;
+    if (e < ne) acc += V.w * s;
   }
   typedef cub::BlockReduce<double, kTile> BR;
   __shared__ typename BR::TempStorage tmp;

@@ -36,18 +36,19 @@ struct StageTimer {
   Context* c;
   int idx;
   cudaEvent_t a = nullptr, b = nullptr;
+  bool ok = false;
   StageTimer(Context* ctx, int i) : c(ctx), idx(i) {
-    if (cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess) cudaEventRecord(a, c->stream);
+    ok = cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess &&
+         cudaEventRecord(a, c->stream) == cudaSuccess;
+    if (!ok) cudaGetLastError();  // timing only: leave no error behind
   }
   ~StageTimer() {
-    if (a && b) {
-      cudaEventRecord(b, c->stream);
-      if (cudaEventSynchronize(b) == cudaSuccess) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, a, b);
-        c->stage_ms[idx] = ms;
-      }
-    }
+    float ms = 0;
+    if (ok && cudaEventRecord(b, c->stream) == cudaSuccess && cudaEventSynchronize(b) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, a, b) == cudaSuccess)
+      c->stage_ms[idx] = ms;
+    else
+      cudaGetLastError();
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
   }
@@ -121,6 +122,8 @@ void pbgpu_ctx_destroy(pbgpu_ctx* h) {
 }
 
 const char* pbgpu_last_error(const pbgpu_ctx* h) { return h ? h->c.err.c_str() : "null context"; }
+
+void* pbgpu_ctx_stream(const pbgpu_ctx* h) { return h ? static_cast<void*>(h->c.stream) : nullptr; }
 
 int pbgpu_set_mesh(pbgpu_ctx* h, const pbgpu_mesh* m) {
   CTX_CHECK(h);

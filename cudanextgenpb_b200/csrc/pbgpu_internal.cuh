@@ -170,10 +170,12 @@ struct Context {
 
 int cuda_fail(Context* c, cudaError_t e, const char* what);
 
-#define PBGPU_CUDA(ctx, expr)                                   \
-  do {                                                          \
-    cudaError_t _e = (expr);                                    \
-    if (_e != cudaSuccess) return ::pbgpu::cuda_fail((ctx), _e, #expr); \
+#define PBGPU_STR2(x) #x
+#define PBGPU_STR(x) PBGPU_STR2(x)
+#define PBGPU_CUDA(ctx, expr)                                                                            \
+  do {                                                                                                   \
+    cudaError_t _e = (expr);                                                                             \
+    if (_e != cudaSuccess) return ::pbgpu::cuda_fail((ctx), _e, __FILE__ ":" PBGPU_STR(__LINE__) " " #expr); \
   } while (0)
 
 // After a kernel launch: count it and check the launch.

@@ -482,11 +482,10 @@ std::vector<uint8_t> poisson_boltzmann::corner_inside_z(const std::vector<uint8_
     for (int64_t i = 0; i < n; ++i) {
       const Octant q = tmsh.leaves[i];
       const int32_t s = q.size();
-      for (int c = 0; c < 8; ++c) {
-        if (hm[i] >> c & 1) continue;
-        const uint64_t key = ray_key(q.x + (c & 1) * s, q.y + ((c >> 1) & 1) * s);
-        if (ray_cache.parity_known(2, key)) continue;
-        mine.push_back(key);
+      for (int col = 0; col < 4; ++col) {  // corners col and col + 4 share the z column
+        if ((hm[i] >> col & 1) && (hm[i] >> (col + 4) & 1)) continue;
+        const uint64_t key = ray_key(q.x + (col & 1) * s, q.y + ((col >> 1) & 1) * s);
+        if (!ray_cache.parity_known(2, key)) mine.push_back(key);
       }
     }
   }
@@ -498,10 +497,18 @@ std::vector<uint8_t> poisson_boltzmann::corner_inside_z(const std::vector<uint8_
   for (int64_t i = 0; i < n; ++i) {
     const Octant q = tmsh.leaves[i];
     const int32_t s = q.size();
-    for (int c = 0; c < 8; ++c) {
-      if (hm[i] >> c & 1) continue;
-      const int32_t x = q.x + (c & 1) * s, y = q.y + ((c >> 1) & 1) * s, z = q.z + ((c >> 2) & 1) * s;
-      inside[8 * i + c] = (uint8_t)ray_cache.parity(2, ray_key(x, y), dom.coord(2, z));
+    const double z0 = dom.coord(2, q.z), z1 = dom.coord(2, q.z + s);
+    for (int col = 0; col < 4; ++col) {
+      int32_t m = 0;
+      const double* I = ray_cache.crossings(2, ray_key(q.x + (col & 1) * s, q.y + ((col >> 1) & 1) * s), &m);
+      for (int h = 0; h < 2; ++h) {
+        const int c = col + 4 * h;
+        if (hm[i] >> c & 1) continue;
+        const double z = h ? z1 : z0;
+        int k = 0;
+        while (k < m && z >= I[k]) ++k;
+        inside[8 * i + c] = (uint8_t)(k & 1);
+      }
     }
   }
   return inside;
@@ -584,6 +591,7 @@ void poisson_boltzmann::finalize_mesh() {
 }
 
 void poisson_boltzmann::build_problem() {
+  const double t0 = omp_get_wtime();
   create_mesh();
   surf.build(atoms, 0.0);
   ray_cache.clear();
@@ -595,8 +603,14 @@ void poisson_boltzmann::build_problem() {
     init_tmesh_with_refine_box_scale();
   else
     init_tmesh();
+  const double t1 = omp_get_wtime();
   if (loc_refinement == 1 || mesh_shape == 4) refine_surface();
+  const double t2 = omp_get_wtime();
   finalize_mesh();
+  const double t3 = omp_get_wtime();
+  if (verbose)
+    std::cerr << "build_problem: init " << t1 - t0 << " s, refine_surface " << t2 - t1 << " s, nodes+rays "
+              << t3 - t2 << " s, " << tmsh.size() << " octants\n";
 }
 
 // ---------------------------------------------------------------------------

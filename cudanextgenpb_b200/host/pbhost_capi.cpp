@@ -1,6 +1,7 @@
 // C API over the host poisson_boltzmann mirror (include/pbhost.h).
 #include "../../include/pbhost.h"
 
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <stdexcept>
@@ -110,6 +111,8 @@ int pbhost_build_problem(pbhost* h) {
     h->err = "no atoms";
     return PBGPU_ERR_STATE;
   }
+  const char* v = std::getenv("PBHOST_VERBOSE");
+  h->pb.verbose = (v && *v && *v != '0') ? 1 : 0;
   PBHOST_TRY(h, h->pb.build_problem());
   return PBGPU_OK;
 }

@@ -167,12 +167,61 @@ void SphereUnion::cast(int axis, double u, double v, std::vector<double>& inters
   emit(cur.hi, cur.shi);
 }
 
+static inline uint64_t mix(uint64_t k) { return k * 0x9E3779B97F4A7C15ull; }
+
 void RayCache::clear() {
   for (int a = 0; a < 3; ++a) {
-    map_[a].clear();
+    tab_[a] = Table();
     inters_[a].clear();
     normals_[a].clear();
   }
+}
+
+int64_t RayCache::find(int axis, uint64_t key) const {
+  const Table& T = tab_[axis];
+  if (T.size == 0) return -1;
+  uint64_t s = (mix(key) >> 20) & T.mask;
+  while (true) {
+    const uint64_t k = T.key[s];
+    if (k == key) return (int64_t)s;
+    if (k == ~0ull) return -1;
+    s = (s + 1) & T.mask;
+  }
+}
+
+void RayCache::insert(int axis, uint64_t key, int64_t off, int32_t n) {
+  Table& T = tab_[axis];
+  uint64_t s = (mix(key) >> 20) & T.mask;
+  while (T.key[s] != ~0ull && T.key[s] != key) s = (s + 1) & T.mask;
+  if (T.key[s] == ~0ull) ++T.size;
+  T.key[s] = key;
+  T.off[s] = off;
+  T.n[s] = n;
+}
+
+void RayCache::grow(int axis, int64_t need) {
+  Table& T = tab_[axis];
+  if (2 * need <= (int64_t)T.key.size()) return;
+  uint64_t cap = 1024;
+  while ((int64_t)cap < 2 * need) cap <<= 1;
+  Table old = std::move(T);
+  T = Table();
+  T.key.assign(cap, ~0ull);
+  T.off.assign(cap, 0);
+  T.n.assign(cap, 0);
+  T.mask = cap - 1;
+  for (size_t s = 0; s < old.key.size(); ++s)
+    if (old.key[s] != ~0ull) insert(axis, old.key[s], old.off[s], old.n[s]);
+}
+
+const double* RayCache::crossings(int axis, uint64_t key, int32_t* n) const {
+  const int64_t s = find(axis, key);
+  if (s < 0) {
+    *n = 0;
+    return nullptr;
+  }
+  *n = tab_[axis].n[s];
+  return inters_[axis].data() + tab_[axis].off[s];
 }
 
 void RayCache::ensure(int axis, std::vector<uint64_t> keys) {
@@ -182,7 +231,7 @@ void RayCache::ensure(int axis, std::vector<uint64_t> keys) {
   std::vector<uint64_t> miss;
   miss.reserve(keys.size());
   for (uint64_t k : keys)
-    if (!map_[axis].count(k)) miss.push_back(k);
+    if (find(axis, k) < 0) miss.push_back(k);
   if (miss.empty()) return;
   int t0, t1;
   transverse(axis, t0, t1);
@@ -193,20 +242,20 @@ void RayCache::ensure(int axis, std::vector<uint64_t> keys) {
     const int32_t ia = int32_t(miss[j] >> 20), ib = int32_t(miss[j] & 0xfffff);
     surf->cast(axis, dom->coord(t0, ia), dom->coord(t1, ib), I[j], N[j]);
   }
-  map_[axis].reserve(map_[axis].size() + m);
+  grow(axis, tab_[axis].size + m);
   for (int64_t j = 0; j < m; ++j) {
-    map_[axis][miss[j]] = Ray{(int64_t)inters_[axis].size(), (int32_t)I[j].size()};
+    insert(axis, miss[j], (int64_t)inters_[axis].size(), (int32_t)I[j].size());
     inters_[axis].insert(inters_[axis].end(), I[j].begin(), I[j].end());
     normals_[axis].insert(normals_[axis].end(), N[j].begin(), N[j].end());
   }
 }
 
 int RayCache::parity(int axis, uint64_t key, double x) const {
-  auto it = map_[axis].find(key);
-  if (it == map_[axis].end()) throw std::runtime_error("RayCache::parity: ray not cast");
-  const double* I = inters_[axis].data() + it->second.off;
+  int32_t n = 0;
+  const double* I = crossings(axis, key, &n);
+  if (!I) throw std::runtime_error("RayCache::parity: ray not cast");
   int i = 0;
-  while (i < it->second.n && x >= I[i]) ++i;
+  while (i < n && x >= I[i]) ++i;
   return i & 1;
 }
 
@@ -216,14 +265,14 @@ RayTable RayCache::table(int axis, const std::vector<uint64_t>& keys_in) const {
   keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
   RayTable T;
   for (uint64_t k : keys) {
-    auto it = map_[axis].find(k);
-    if (it == map_[axis].end()) throw std::runtime_error("RayCache::table: ray not cast");
-    if (it->second.n == 0) continue;
+    const int64_t s = find(axis, k);
+    if (s < 0) throw std::runtime_error("RayCache::table: ray not cast");
+    const int32_t n = tab_[axis].n[s];
+    if (n == 0) continue;
     T.keys.push_back(k);
-    const int64_t o = it->second.off;
-    T.inters.insert(T.inters.end(), inters_[axis].begin() + o, inters_[axis].begin() + o + it->second.n);
-    T.normals.insert(T.normals.end(), normals_[axis].begin() + 3 * o,
-                     normals_[axis].begin() + 3 * (o + it->second.n));
+    const int64_t o = tab_[axis].off[s];
+    T.inters.insert(T.inters.end(), inters_[axis].begin() + o, inters_[axis].begin() + o + n);
+    T.normals.insert(T.normals.end(), normals_[axis].begin() + 3 * o, normals_[axis].begin() + 3 * (o + n));
     T.ptr.push_back((int64_t)T.inters.size());
   }
   return T;

@@ -66,7 +66,8 @@ struct RayTable {
 inline uint64_t ray_key(int32_t a, int32_t b) { return (uint64_t(uint32_t(a)) << 20) | uint64_t(uint32_t(b)); }
 
 // Host cache of cast rays.  ensure() casts every missing ray (in parallel);
-// lookups afterwards are read-only.
+// lookups afterwards are read-only and thread-safe.  Rays are kept in a flat
+// open-addressing table (linear probing, load <= 1/2).
 class RayCache {
  public:
   const SphereUnion* surf = nullptr;
@@ -75,17 +76,24 @@ class RayCache {
   // Parity of the crossings at or below x (the reference's is_in_ns_surf,
   // src/pb_class.cpp:769-805): 1 inside, 0 outside.
   int parity(int axis, uint64_t key, double x) const;
-  bool parity_known(int axis, uint64_t key) const { return map_[axis].count(key) != 0; }
+  // Crossings of a cast ray (nullptr when the ray has not been cast).
+  const double* crossings(int axis, uint64_t key, int32_t* n) const;
+  bool parity_known(int axis, uint64_t key) const { return find(axis, key) >= 0; }
   RayTable table(int axis, const std::vector<uint64_t>& keys) const;
   void clear();
 
  private:
-  struct Ray {
-    int64_t off;
-    int32_t n;
-  };
-  std::unordered_map<uint64_t, Ray> map_[3];
+  struct Table {
+    std::vector<uint64_t> key;  // ~0 = empty
+    std::vector<int64_t> off;
+    std::vector<int32_t> n;
+    uint64_t mask = 0;
+    int64_t size = 0;
+  } tab_[3];
   std::vector<double> inters_[3], normals_[3];
+  int64_t find(int axis, uint64_t key) const;
+  void insert(int axis, uint64_t key, int64_t off, int32_t n);
+  void grow(int axis, int64_t need);
 };
 
 }  // namespace pbh

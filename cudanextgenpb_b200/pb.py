@@ -284,6 +284,10 @@ class GpuPath:
         self._check(self._lib.pbgpu_get_stage_ms(self._ctx, ms))
         return dict(zip(["markers", "density", "assemble", "solve", "phi_atoms", "energy"], list(ms)))
 
+    def stream_ptr(self) -> int:
+        """cudaStream_t of this context (e.g. for torch.cuda.ExternalStream)."""
+        return int(self._lib.pbgpu_ctx_stream(self._ctx) or 0)
+
     def set_profiling(self, on=True):
         self._check(self._lib.pbgpu_set_profiling(self._ctx, 1 if on else 0))
 

@@ -135,6 +135,9 @@ int pbgpu_ctx_create(pbgpu_ctx** out, int device, void* cuda_stream /* NULL: own
 void pbgpu_ctx_destroy(pbgpu_ctx* ctx);
 const char* pbgpu_last_error(const pbgpu_ctx* ctx);
 int pbgpu_version(void);
+/* The CUDA stream the context runs on (cudaStream_t), so a caller can order
+ * its own work after the path's.  No counterpart in the reference. */
+void* pbgpu_ctx_stream(const pbgpu_ctx* ctx);
 
 /* ---- inputs ------------------------------------------------------------ */
 /* Mesh of tmesh_3d after refine_surface (src/poisson_boltzmann.cpp:181-186). */
