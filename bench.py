@@ -37,6 +37,8 @@ FALLBACK_HBM_GBS = 6650.0
 WORKLOADS = {
     # name: (n_atoms, radius, net charge, seed, scale, levels)
     "mol2000": (2000, 18.0, -3.0, 2000, 2.0, 3),
+    # same molecule, 2 surface levels: the profiling case (inputs > L2, ~2 GB on device)
+    "mol2000l2": (2000, 18.0, -3.0, 2000, 2.0, 2),
     "mol300": (300, 11.0, -3.0, 300, 2.0, 2),
     "mol60": (60, 7.0, -3.0, 60, 2.0, 1),
 }

@@ -520,16 +520,25 @@ static int krylov(Context* c, int method, const KrylovVecs<T>& K, double tol, in
               cudaSuccess) {
             c->spmv_ms += ms;
             c->spmv_launches += 1;
+          } else {
+            cudaGetLastError();  // measurement only
           }
         }
     }
     prev_iter = now;
     if (c->ks_host->done) break;
   }
-  cudaGraphExecDestroy(exec);
-  cudaGraphDestroy(graph);
-  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  const cudaError_t e_exec = cudaGraphExecDestroy(exec);
+  const cudaError_t e_graph = cudaGraphDestroy(graph);
+  cudaError_t e_ev = cudaSuccess;
+  for (cudaEvent_t e : ev) {
+    const cudaError_t d = cudaEventDestroy(e);
+    if (d != cudaSuccess) e_ev = d;
+  }
   if (rc != PBGPU_OK) return rc;
+  if (e_exec != cudaSuccess) return cuda_fail(c, e_exec, "cudaGraphExecDestroy");
+  if (e_graph != cudaSuccess) return cuda_fail(c, e_graph, "cudaGraphDestroy");
+  if (e_ev != cudaSuccess) return cuda_fail(c, e_ev, "cudaEventDestroy");
   *iters = c->ks_host->iter;
   c->krylov_iters += c->ks_host->iter;
   c->spmv_bytes = (double)c->nnz * (sizeof(T) + 4) + 2.0 * (double)c->n * sizeof(T);

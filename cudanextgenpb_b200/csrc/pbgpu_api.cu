@@ -2,6 +2,8 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <sstream>
@@ -62,10 +64,16 @@ using namespace pbgpu;
 
 #define CTX_CHECK(ctx) \
   if (!(ctx)) return PBGPU_ERR_ARG;
-#define SET_DEVICE(C)                                       \
-  do {                                                      \
-    cudaError_t _e = cudaSetDevice((C)->device);            \
-    if (_e != cudaSuccess) return cuda_fail((C), _e, "cudaSetDevice"); \
+// Select the context's device and clear a non-sticky error that an earlier
+// runtime call of this thread left behind (reported on stderr when PBGPU_DEBUG
+// is set), so it is not blamed on this call's launches.
+#define SET_DEVICE(C)                                                                         \
+  do {                                                                                        \
+    cudaError_t _e = cudaSetDevice((C)->device);                                              \
+    if (_e != cudaSuccess) return cuda_fail((C), _e, "cudaSetDevice");                        \
+    const cudaError_t _stale = cudaGetLastError();                                            \
+    if (_stale != cudaSuccess && std::getenv("PBGPU_DEBUG"))                                  \
+      std::fprintf(stderr, "pbgpu: stale error before %s: %s\n", __func__, cudaGetErrorString(_stale)); \
   } while (0)
 
 extern "C" {

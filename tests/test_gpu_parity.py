@@ -203,6 +203,25 @@ def test_call_order_and_iteration_cap():
     assert st.status == 0
 
 
+def test_repeated_full_path_on_one_context():
+    """The whole path run three times on one context gives the same results
+    (the pattern of a serving loop and of the benchmark's steps)."""
+    prob = CASES["mol60"]().build()
+    g = GpuPath().load(prob)
+    opts = solver_opts("cg", tol=1e-8, max_iter=50000)
+    out = []
+    for _ in range(3):
+        g.create_markers()
+        g.create_density_map()
+        g.assemble(32, 32)
+        st = g.solve(opts)
+        pa = g.phi_on_atoms()
+        e = g.energy(False)
+        out.append((st.iterations, e["sum"], pa.copy()))
+    for it, es, pa in out[1:]:
+        assert it == out[0][0] and es == out[0][1] and np.array_equal(pa, out[0][2])
+
+
 def test_host_driver_path_matches():
     """pbhost_run_gpu (the C++ pb_class mirror's driver order) gives the same energy."""
     prob = configs.make_born_problem(5, 6).build()
