@@ -215,7 +215,7 @@ def run_ours(args, rank, world, local):
     def step():
         g.create_markers()
         g.create_density_map()
-        g.assemble(args.chunk, args.sigma)
+        g.assemble(args.chunk, args.sigma, args.group)
         st = g.solve(opts)
         pa = g.phi_on_atoms()
         e = g.energy(False)
@@ -275,7 +275,7 @@ def run_ours(args, rank, world, local):
         assert lib.pbgpu_set_model(ctx, C.byref(pin["model"])) == 0
         assert lib.pbgpu_create_markers(ctx) == 0
         assert lib.pbgpu_create_density_map(ctx) == 0
-        so = N.PbgpuSellOpts(args.chunk, args.sigma)
+        so = N.PbgpuSellOpts(args.chunk, args.sigma, args.group)
         assert lib.pbgpu_assemble(ctx, C.byref(so)) == 0
         s = N.PbgpuSolveStats()
         assert lib.pbgpu_solve(ctx, C.byref(opts), C.byref(s)) == 0
@@ -432,7 +432,8 @@ def main():
     ap.add_argument("--workload", default="mol2000", choices=sorted(WORKLOADS))
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--chunk", type=int, default=32)
-    ap.add_argument("--sigma", type=int, default=32)
+    ap.add_argument("--sigma", type=int, default=2048)
+    ap.add_argument("--group", type=int, default=1)
     ap.add_argument("--cpu-iters", type=int, default=30)
     ap.add_argument("--ref-iters", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -33,7 +33,7 @@ class PbgpuModel(C.Structure):
 
 
 class PbgpuSellOpts(C.Structure):
-    _fields_ = [("chunk", C.c_int), ("sigma", C.c_int)]
+    _fields_ = [("chunk", C.c_int), ("sigma", C.c_int), ("group", C.c_int)]
 
 
 class PbgpuSolverOpts(C.Structure):
@@ -56,7 +56,7 @@ class PbgpuEnergyOut(C.Structure):
 
 class PbgpuCounters(C.Structure):
     _fields_ = [("launches", i64), ("spmv_launches", i64), ("spmv_ms", dbl), ("spmv_bytes", dbl),
-                ("krylov_iterations", i64)]
+                ("krylov_iterations", i64), ("energy_points", i64), ("energy_pairs", i64)]
 
 
 class PbhostInfo(C.Structure):

@@ -195,12 +195,14 @@ struct SellOut {
   double* b;
   double* dinv;
   int C;
+  int G;  // columns per row stored contiguously (1, 2 or 4)
 };
 
+// Element j of SELL row p: groups of G consecutive columns, lane-interleaved.
 __device__ __forceinline__ int64_t sell_index(const SellOut& S, int64_t p, int j) {
   const int64_t sl = p / S.C;
   const int lane = (int)(p % S.C);
-  return S.slice_ptr[sl] + (int64_t)(j >> 2) * 4 * S.C + lane * 4 + (j & 3);
+  return S.slice_ptr[sl] + (int64_t)(j / S.G) * S.G * S.C + lane * S.G + (j % S.G);
 }
 
 // Pass 2: values, columns (SELL numbering), right-hand side, 1/diagonal.
@@ -313,7 +315,7 @@ __global__ void k_iperm(const int32_t* __restrict__ perm, int64_t n, int32_t* __
 }
 
 __global__ void k_slice_width(const int32_t* __restrict__ perm, const int32_t* __restrict__ rowlen, int64_t n,
-                              int64_t n_slices, int C, int32_t* __restrict__ w, int64_t* __restrict__ elems) {
+                              int64_t n_slices, int C, int G, int32_t* __restrict__ w, int64_t* __restrict__ elems) {
   const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= n_slices) return;
   int mx = 1;
@@ -321,7 +323,7 @@ __global__ void k_slice_width(const int32_t* __restrict__ perm, const int32_t* _
     const int64_t p = s * C + l;
     if (p < n) mx = max(mx, rowlen[perm[p]]);
   }
-  mx = (mx + 3) & ~3;
+  mx = (mx + G - 1) / G * G;
   w[s] = mx;
   elems[s] = (int64_t)mx * C;
 }
@@ -330,11 +332,14 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   if (!c->have_markers) return c->fail(PBGPU_ERR_STATE, "assemble: create_markers has not run");
   if (!c->have_density) return c->fail(PBGPU_ERR_STATE, "assemble: create_density_map has not run");
   int C = (o && o->chunk > 0) ? o->chunk : 32;
-  int sigma = (o && o->sigma > 0) ? o->sigma : C;
+  int sigma = (o && o->sigma > 0) ? o->sigma : 2048;
+  int G = (o && o->group > 0) ? o->group : 1;
   if (C % 32 != 0 || C > 1024) return c->fail(PBGPU_ERR_ARG, "SELL chunk must be a multiple of 32, at most 1024");
   if (sigma % C != 0 && sigma != 1) return c->fail(PBGPU_ERR_ARG, "SELL sigma must be 1 or a multiple of the chunk");
+  if (G != 1 && G != 2 && G != 4) return c->fail(PBGPU_ERR_ARG, "SELL group must be 1, 2 or 4");
   c->C = C;
   c->sigma = sigma;
+  c->G = G;
   const int64_t n = c->n;
   const double3 lo = make_double3(c->lo[0], c->lo[1], c->lo[2]);
   const double3 len = make_double3(c->len[0], c->len[1], c->len[2]);
@@ -409,7 +414,7 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   DBuf<int64_t> elems;
   PBGPU_CUDA(c, elems.alloc(n_slices + 1));
   PBGPU_CUDA(c, cudaMemsetAsync(elems.get(), 0, (n_slices + 1) * sizeof(int64_t), c->stream));
-  k_slice_width<<<grid_for(n_slices, 128), 128, 0, c->stream>>>(c->perm.get(), c->rowlen.get(), n, n_slices, C,
+  k_slice_width<<<grid_for(n_slices, 128), 128, 0, c->stream>>>(c->perm.get(), c->rowlen.get(), n, n_slices, C, G,
                                                                  c->slice_w.get(), elems.get());
   PBGPU_LAUNCHED(c);
   size_t bytes = 0;
@@ -438,7 +443,7 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   PBGPU_CUDA(c, c->b.alloc(n_pad));
   PBGPU_CUDA(c, c->dinv.alloc(n_pad));
   SellOut S{c->slice_ptr.get(), c->slice_w.get(), c->iperm.get(), c->scol.get(), c->sval.get(), c->b.get(),
-            c->dinv.get(), C};
+            c->dinv.get(), C, G};
   k_row_fill<<<grid_for(n, 128), 128, 0, c->stream>>>(A, S);
   PBGPU_LAUNCHED(c);
   if (n_pad > n) {
@@ -479,7 +484,8 @@ int export_system(Context* c, int64_t* nnz_out, int64_t* row_ptr, int32_t* col, 
     const int lane = (int)(p % C);
     row.clear();
     for (int j = 0; j < rl[i]; ++j) {
-      const int64_t k = sp[s] + (int64_t)(j >> 2) * 4 * C + lane * 4 + (j & 3);
+      const int G = c->G;
+      const int64_t k = sp[s] + (int64_t)(j / G) * G * C + lane * G + (j % G);
       row.push_back({perm[sc[k]], sv[k]});
     }
     std::sort(row.begin(), row.end());

@@ -2,14 +2,22 @@
 // (write_potential_on_atoms_fast, src/pb_class.cpp:2333-2417) and the
 // electrostatic energy (energy / energy_fast, :2791-3338).
 //
-// The energy is split in two phases.  (1) One thread per border octant builds
-// the octant's surface elements exactly as the reference walks them: one flux
-// element (point V on each epsilon-jump edge, flux F) per jump edge, and three
-// vertex elements (point V, outward normal N, coefficient phi0 * area / (12 pi))
-// per marching-cubes triangle.  Counts go through a scan so the elements are
-// packed in border order.  (2) The pair sums over elements x charged atoms run
-// as FP64 N-body kernels with the atoms staged in shared memory tiles; block
-// partials are summed in fixed order, so the energy is deterministic.
+// The reference walks every border octant and, for each epsilon-jump edge
+// (flux term) and each marching-cubes triangle vertex (ionic term), sums over
+// all charged atoms.  Every such surface point lies on a ray crossing, and a
+// crossing is shared by the octants around its edge, so the same point enters
+// the pair sum up to ~10 times with different coefficients.  Here:
+//  (1) one thread per border octant evaluates the reference's per-element
+//      coefficients (flux F, and coef * N with coef = phi0 * area / (12 pi) for
+//      a triangle vertex) and adds them into an accumulator of the crossing
+//      they sit on (elements whose edge has no crossing keep their own point);
+//  (2) the used crossings are compacted into a point list (V, F, D);
+//  (3) one FP64 pair kernel over points x charged atoms, atoms staged in shared
+//      memory tiles, evaluates sum_a q_a / r (flux) and sum_a q_a (V - x_a).D / r^3
+//      (ionic) together, with 1/r from a Newton-Raphson reciprocal square root.
+// The point of a crossing is the crossing itself (transverse coordinates of the
+// ray, position along it); the reference recomputes it per edge as
+// x1 + frac * h, which agrees to the last bit or two.
 #include <cub/cub.cuh>
 
 #include "mc_tables.h"
@@ -28,6 +36,14 @@ struct EnergyView {
   const double* eps;
   const double* phi;
   RayView rays[3];
+  int64_t slot_base[3];   // first accumulator slot of each axis' crossings
+  double4* acc;           // per crossing: F, Dx, Dy, Dz
+  uint8_t* used;
+  int32_t* slot_ray;      // ray of each used crossing
+  double4* extra_p;       // elements on edges without a crossing
+  double4* extra_d;
+  unsigned long long* n_extra;
+  int64_t extra_cap;
   int64_t n, nb;
   double lo[3], len[3];
   double eps_out;
@@ -82,15 +98,19 @@ __device__ __forceinline__ int32_t corner_i(const CellCtx& C, int c, int a) {
 }
 
 // normal_intersection (src/pb_class.cpp:2535-2568): updates C.N when a crossing
-// lies on the edge, returns the fraction (0.5 when none).
-__device__ __forceinline__ double normal_intersection(const EnergyView& E, CellCtx& C, int e) {
+// lies on the edge and returns the fraction (0.5 when none); *slot is the
+// global accumulator slot of that crossing or -1.
+__device__ __forceinline__ double normal_intersection(const EnergyView& E, CellCtx& C, int e, int64_t* slot,
+                                                      int32_t* ray) {
   const int axis = d_edge_axis[e], i1 = d_edge_nodes[2 * e], i2 = d_edge_nodes[2 * e + 1];
   const double x1 = coord(E.lo[axis], E.len[axis], corner_i(C, i1, axis));
   const double x2 = coord(E.lo[axis], E.len[axis], corner_i(C, i2, axis));
   const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
   const RayView& R = E.rays[axis];
   double f = 0.5;
+  *slot = -1;
   const int32_t r = ray_find(R.hk, R.hv, R.cap, R.cap_log, ray_key(corner_i(C, i1, t0), corner_i(C, i1, t1)));
+  *ray = r;
   if (r >= 0)
     for (int64_t k = R.ptr[r]; k < R.ptr[r + 1]; ++k) {
       const double I = R.inters[k];
@@ -99,6 +119,7 @@ __device__ __forceinline__ double normal_intersection(const EnergyView& E, CellC
         C.N[1] = R.normals[3 * k + 1];
         C.N[2] = R.normals[3 * k + 2];
         f = (I - x1) / (x2 - x1);
+        *slot = E.slot_base[axis] + k;
       }
     }
   return f;
@@ -118,31 +139,32 @@ __device__ __forceinline__ int cube_index(const CellCtx& C, double eps_out) {
   return k;
 }
 
-// counts of flux elements and triangle-vertex elements per border octant
-__global__ void k_energy_count(EnergyView E, int32_t* __restrict__ nflux, int32_t* __restrict__ ntri) {
-  const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (b >= E.nb) return;
-  CellCtx C;
-  cell_load(E, b, C);
-  int nf = 0;
-  for (int e = 0; e < 12; ++e) nf += C.te[d_edge_nodes[2 * e]] != C.te[d_edge_nodes[2 * e + 1]];
-  int nt = 0;
-  if (E.ionic) {
-    const int k = cube_index(C, E.eps_out);
-    if (k != 0 && k != 255)
-      while (nt < 5 && d_tri[k][3 * nt] >= 0) ++nt;
+__device__ __forceinline__ void add_point(const EnergyView& E, int64_t slot, int32_t ray, const double V[3], double F,
+                                          double Dx, double Dy, double Dz) {
+  if (slot >= 0) {
+    double* a = reinterpret_cast<double*>(E.acc + slot);
+    if (F != 0.0) atomicAdd(a, F);
+    if (Dx != 0.0) atomicAdd(a + 1, Dx);
+    if (Dy != 0.0) atomicAdd(a + 2, Dy);
+    if (Dz != 0.0) atomicAdd(a + 3, Dz);
+    E.used[slot] = 1;
+    E.slot_ray[slot] = ray;
+    return;
   }
-  nflux[b] = nf;
-  ntri[b] = 3 * nt;
+  const unsigned long long i = atomicAdd(E.n_extra, 1ull);
+  if ((int64_t)i < E.extra_cap) {
+    E.extra_p[i] = make_double4(V[0], V[1], V[2], F);
+    E.extra_d[i] = make_double4(Dx, Dy, Dz, 0.0);
+  }
 }
 
-__global__ void k_energy_fill(EnergyView E, const int64_t* __restrict__ off_flux, const int64_t* __restrict__ off_tri,
-                              double4* __restrict__ flux, double4* __restrict__ triv, double4* __restrict__ trin) {
+// (1) per border octant: the reference's element coefficients, accumulated on
+// the crossings they sit on.
+__global__ void k_energy_accumulate(EnergyView E) {
   const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (b >= E.nb) return;
   CellCtx C;
   cell_load(E, b, C);
-  int64_t wf = off_flux[b];
   for (int e = 0; e < 12; ++e) {
     const int i1 = d_edge_nodes[2 * e], i2 = d_edge_nodes[2 * e + 1];
     double dir;
@@ -152,23 +174,26 @@ __global__ void k_energy_fill(EnergyView E, const int64_t* __restrict__ off_flux
       dir = -1;
     else
       continue;
-    const double f = normal_intersection(E, C, e);
+    int64_t slot;
+    int32_t ray;
+    const double f = normal_intersection(E, C, e, &slot, &ray);
     double V[3];
     edge_point(E, C, e, f, V);
     const double F = -(C.tp[i2] - C.tp[i1]) * wha(C.te[i1], C.te[i2], f) * dir * C.area_h[d_edge_axis[e]];
-    flux[wf++] = make_double4(V[0], V[1], V[2], F);
+    add_point(E, slot, ray, V, F, 0.0, 0.0, 0.0);
   }
   if (!E.ionic) return;
   const int k = cube_index(C, E.eps_out);
   if (k == 0 || k == 255) return;
-  int64_t wt = off_tri[b];
   const double inv_4pi = 1.0 / (4.0 * kPi);
   for (int t = 0; t < 5 && d_tri[k][3 * t] >= 0; ++t) {
     double VT[3][3], NT[3][3], ps[3];
+    int64_t sl[3];
+    int32_t ry[3];
     for (int j = 0; j < 3; ++j) {
       const int e = d_tri[k][3 * t + j];
       const int i1 = d_edge_nodes[2 * e], i2 = d_edge_nodes[2 * e + 1];
-      const double f = normal_intersection(E, C, e);
+      const double f = normal_intersection(E, C, e, &sl[j], &ry[j]);
       edge_point(E, C, e, f, VT[j]);
       NT[j][0] = C.N[0];
       NT[j][1] = C.N[1];
@@ -183,56 +208,58 @@ __global__ void k_energy_fill(EnergyView E, const int64_t* __restrict__ off_flux
     const double area =
         0.5 * norm3d(ab[1] * ac[2] - ab[2] * ac[1], ab[0] * ac[2] - ab[2] * ac[0], ab[1] * ac[0] - ab[0] * ac[1]);
     for (int j = 0; j < 3; ++j) {
-      triv[wt] = make_double4(VT[j][0], VT[j][1], VT[j][2], ps[j] * inv_4pi * area / 3.0);
-      trin[wt] = make_double4(NT[j][0], NT[j][1], NT[j][2], 0.0);
-      ++wt;
+      const double coef = ps[j] * inv_4pi * area / 3.0;
+      add_point(E, sl[j], ry[j], VT[j], 0.0, coef * NT[j][0], coef * NT[j][1], coef * NT[j][2]);
     }
   }
+}
+
+// (2) used crossing -> point (transverse coordinates of its ray, position along it)
+__global__ void k_energy_points(const int32_t* __restrict__ used_slots, int64_t m, EnergyView E,
+                                double4* __restrict__ P, double4* __restrict__ D) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int64_t slot = used_slots[i];
+  const int axis = slot >= E.slot_base[2] ? 2 : (slot >= E.slot_base[1] ? 1 : 0);
+  const int64_t k = slot - E.slot_base[axis];
+  const RayView& R = E.rays[axis];
+  const int32_t r = E.slot_ray[slot];
+  const uint64_t key = R.keys[r];
+  const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
+  double V[3];
+  V[axis] = R.inters[k];
+  V[t0] = coord(E.lo[t0], E.len[t0], (int32_t)(key >> 20));
+  V[t1] = coord(E.lo[t1], E.len[t1], (int32_t)(key & 0xfffff));
+  const double4 a = E.acc[slot];
+  P[i] = make_double4(V[0], V[1], V[2], a.x);
+  D[i] = make_double4(a.y, a.z, a.w, 0.0);
+}
+
+// x^{-1/2}: the FP32 hardware estimate refined by two Newton-Raphson steps
+// y <- y (3 - x y^2) / 2 (each step squares the relative error: ~2^-22 ->
+// ~1e-13 -> below double rounding).
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  double y = (double)rsqrtf((float)x);
+  y = y * (1.5 - 0.5 * x * y * y);
+  y = y * (1.5 - 0.5 * x * y * y);
+  return y;
 }
 
 constexpr int kTile = 256;
 
-// sum over elements e of coef_e * sum_a q_a / |x_a - V_e|
-__global__ void __launch_bounds__(kTile) k_nbody_flux(const double4* __restrict__ el, int64_t ne,
-                                                      const double4* __restrict__ atoms, int64_t m,
-                                                      double* __restrict__ partials) {
+// (3) sum over points of F sum_a q_a / r  and  sum_a q_a (V - x_a).D / r^3
+template <bool IONIC>
+__global__ void __launch_bounds__(kTile) k_energy_pairs(const double4* __restrict__ P, const double4* __restrict__ D,
+                                                        int64_t np, const double4* __restrict__ atoms, int64_t m,
+                                                        double* __restrict__ partials) {
   __shared__ double4 tile[kTile];
-  double acc = 0.0;
-  for (int64_t base = blockIdx.x * (int64_t)kTile; base < ne; base += (int64_t)gridDim.x * kTile) {
+  double acc1 = 0.0, acc2 = 0.0, accF = 0.0;
+  for (int64_t base = blockIdx.x * (int64_t)kTile; base < np; base += (int64_t)gridDim.x * kTile) {
     const int64_t e = base + threadIdx.x;
-    const double4 E = e < ne ? el[e] : make_double4(0, 0, 0, 0);
-    double s = 0.0;
-    for (int64_t a0 = 0; a0 < m; a0 += kTile) {
-      __syncthreads();
-      if (a0 + threadIdx.x < m) tile[threadIdx.x] = atoms[a0 + threadIdx.x];
-      __syncthreads();
-      const int lim = (int)min((int64_t)kTile, m - a0);
-#pragma unroll 4
-      for (int j = 0; j < lim; ++j) {
-        const double4 A = tile[j];
-        const double dx = A.x - E.x, dy = A.y - E.y, dz = A.z - E.z;
-        s += A.w * rsqrt(dx * dx + dy * dy + dz * dz);
-      }
-    }
-    if (e < ne) acc += E.w * s;  // idle lanes sit at the origin and may hit an atom there
-  }
-  typedef cub::BlockReduce<double, kTile> BR;
-  __shared__ typename BR::TempStorage tmp;
-  const double tot = BR(tmp).Sum(acc);
-  if (threadIdx.x == 0) partials[blockIdx.x] = tot;
-}
-
-// sum over vertex elements of coef_e * sum_a q_a (V_e - x_a).N_e / |V_e - x_a|^3
-__global__ void __launch_bounds__(kTile) k_nbody_tri(const double4* __restrict__ ev, const double4* __restrict__ en,
-                                                     int64_t ne, const double4* __restrict__ atoms, int64_t m,
-                                                     double* __restrict__ partials) {
-  __shared__ double4 tile[kTile];
-  double acc = 0.0;
-  for (int64_t base = blockIdx.x * (int64_t)kTile; base < ne; base += (int64_t)gridDim.x * kTile) {
-    const int64_t e = base + threadIdx.x;
-    const double4 V = e < ne ? ev[e] : make_double4(0, 0, 0, 0);
-    const double4 N = e < ne ? en[e] : make_double4(0, 0, 0, 0);
-    double s = 0.0;
+    const bool live = e < np;
+    const double4 V = live ? P[e] : make_double4(0, 0, 0, 0);
+    const double4 Dv = (IONIC && live) ? D[e] : make_double4(0, 0, 0, 0);
+    double s1 = 0.0, s2 = 0.0;
     for (int64_t a0 = 0; a0 < m; a0 += kTile) {
       __syncthreads();
       if (a0 + threadIdx.x < m) tile[threadIdx.x] = atoms[a0 + threadIdx.x];
@@ -242,16 +269,29 @@ __global__ void __launch_bounds__(kTile) k_nbody_tri(const double4* __restrict__
       for (int j = 0; j < lim; ++j) {
         const double4 A = tile[j];
         const double dx = V.x - A.x, dy = V.y - A.y, dz = V.z - A.z;
-        const double ri = rsqrt(dx * dx + dy * dy + dz * dz);
-        s += A.w * (dx * N.x + dy * N.y + dz * N.z) * (ri * ri * ri);
+        const double y = rsqrt_nr(dx * dx + dy * dy + dz * dz);
+        s1 += A.w * y;
+        if (IONIC) s2 += A.w * (dx * Dv.x + dy * Dv.y + dz * Dv.z) * (y * y * y);
       }
     }
-    if (e < ne) acc += V.w * s;
+    if (live) {
+      acc1 += V.w * s1;
+      acc2 += s2;
+      accF += V.w;
+    }
   }
   typedef cub::BlockReduce<double, kTile> BR;
   __shared__ typename BR::TempStorage tmp;
-  const double tot = BR(tmp).Sum(acc);
-  if (threadIdx.x == 0) partials[blockIdx.x] = tot;
+  const double t1 = BR(tmp).Sum(acc1);
+  __syncthreads();
+  const double t2 = BR(tmp).Sum(acc2);
+  __syncthreads();
+  const double t3 = BR(tmp).Sum(accF);
+  if (threadIdx.x == 0) {
+    partials[3 * blockIdx.x] = t1;
+    partials[3 * blockIdx.x + 1] = t2;
+    partials[3 * blockIdx.x + 2] = t3;
+  }
 }
 
 // sum_{i<j} q_i q_j / r_ij
@@ -272,21 +312,11 @@ __global__ void __launch_bounds__(kTile) k_coulomb(const double4* __restrict__ a
         if (a0 + j <= i) continue;
         const double4 A = tile[j];
         const double dx = P.x - A.x, dy = P.y - A.y, dz = P.z - A.z;
-        s += A.w * rsqrt(dx * dx + dy * dy + dz * dz);
+        s += A.w * rsqrt_nr(dx * dx + dy * dy + dz * dz);
       }
     }
     if (i < m) acc += P.w * s;
   }
-  typedef cub::BlockReduce<double, kTile> BR;
-  __shared__ typename BR::TempStorage tmp;
-  const double tot = BR(tmp).Sum(acc);
-  if (threadIdx.x == 0) partials[blockIdx.x] = tot;
-}
-
-__global__ void k_flux_total(const double4* __restrict__ flux, int64_t ne, double* __restrict__ partials) {
-  double acc = 0.0;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x)
-    acc += flux[e].w;
   typedef cub::BlockReduce<double, kTile> BR;
   __shared__ typename BR::TempStorage tmp;
   const double tot = BR(tmp).Sum(acc);
@@ -330,12 +360,11 @@ static int ensure_tri(Context* c) {
   signed char tri[256][16];
   pbmc::expand_tri_table(tri);
   PBGPU_CUDA(c, cudaMemcpyToSymbolAsync(d_tri, tri, sizeof(tri), 0, cudaMemcpyHostToDevice, c->stream));
-  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   return PBGPU_OK;
 }
 
 static EnergyView energy_view(Context* c, int fast) {
-  EnergyView E;
+  EnergyView E{};
   E.oct = c->oct.get();
   E.oct_nodes = c->oct_nodes.get();
   E.hang_par = c->hang_par.get();
@@ -343,11 +372,14 @@ static EnergyView energy_view(Context* c, int fast) {
   E.border = c->border.get();
   E.eps = c->eps.get();
   E.phi = c->phi.get();
+  int64_t base = 0;
   for (int a = 0; a < 3; ++a) {
     E.rays[a] = ray_view(c->rays[a]);
     E.lo[a] = c->lo[a];
     E.len[a] = c->len[a];
     E.h0[a] = 0.0;
+    E.slot_base[a] = base;
+    base += c->rays[a].nc;
   }
   E.n = c->n;
   E.nb = c->nb;
@@ -371,13 +403,15 @@ int run_phi_atoms(Context* c, double* out) {
   return PBGPU_OK;
 }
 
-static int sum_partials(Context* c, const double* d, int nblk, double* out) {
-  std::vector<double> h(nblk);
-  PBGPU_CUDA(c, cudaMemcpyAsync(h.data(), d, nblk * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+static int sum_partials(Context* c, const double* d, int nblk, int stride, double* out) {
+  std::vector<double> h((size_t)nblk * stride);
+  PBGPU_CUDA(c, cudaMemcpyAsync(h.data(), d, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
-  double s = 0.0;
-  for (double v : h) s += v;
-  *out = s;
+  for (int k = 0; k < stride; ++k) {
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) s += h[(size_t)b * stride + k];
+    out[k] = s;
+  }
   return PBGPU_OK;
 }
 
@@ -391,8 +425,10 @@ int run_energy(Context* c, int fast, pbgpu_energy_out* out) {
   if (fast && nb > 0) {
     int32_t b0 = 0;
     int4 q;
-    PBGPU_CUDA(c, cudaMemcpy(&b0, c->border.get(), sizeof(int32_t), cudaMemcpyDeviceToHost));
-    PBGPU_CUDA(c, cudaMemcpy(&q, c->oct.get() + b0, sizeof(int4), cudaMemcpyDeviceToHost));
+    PBGPU_CUDA(c, cudaMemcpyAsync(&b0, c->border.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    PBGPU_CUDA(c, cudaMemcpyAsync(&q, c->oct.get() + b0, sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+    PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     const int32_t s = 1 << (kRootLog - q.w);
     const int32_t qc[3] = {q.x, q.y, q.z};
     for (int a = 0; a < 3; ++a) {
@@ -406,7 +442,7 @@ int run_energy(Context* c, int fast, pbgpu_energy_out* out) {
   const double constant_react = (1.0 / c->eps_out) * inv_4pi;
   const bool ionic = E.ionic;
   const bool polar = c->model.calc_energy == 1 || (c->model.calc_energy == 2 && c->kappa < 1.e-5);
-  // charged atoms
+  // charged atoms (|q| > 1e-5, src/pb_class.cpp:2829-2834)
   std::vector<double4> ha(c->na);
   if (c->na) {
     PBGPU_CUDA(c, cudaMemcpyAsync(ha.data(), c->atoms.get(), c->na * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
@@ -423,56 +459,89 @@ int run_energy(Context* c, int fast, pbgpu_energy_out* out) {
   PBGPU_CUDA(c, dq.alloc(m > 0 ? m : 1));
   if (m) PBGPU_CUDA(c, cudaMemcpyAsync(dq.get(), qa.data(), m * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
   const int nblk = c->sm_count * 4;
-  PBGPU_CUDA(c, c->energy_part.alloc(4 * nblk));
+  PBGPU_CUDA(c, c->energy_part.alloc(3 * nblk));
   double first_int = 0.0, second_int = 0.0, charge_pol = 0.0, coul = 0.0;
   if ((polar || ionic) && nb > 0) {
-    DBuf<int32_t> nf, nt;
-    DBuf<int64_t> of, ot;
-    PBGPU_CUDA(c, nf.alloc(nb + 1));
-    PBGPU_CUDA(c, nt.alloc(nb + 1));
-    PBGPU_CUDA(c, of.alloc(nb + 1));
-    PBGPU_CUDA(c, ot.alloc(nb + 1));
-    PBGPU_CUDA(c, cudaMemsetAsync(nf.get() + nb, 0, sizeof(int32_t), c->stream));
-    PBGPU_CUDA(c, cudaMemsetAsync(nt.get() + nb, 0, sizeof(int32_t), c->stream));
-    k_energy_count<<<grid_for(nb, 128), 128, 0, c->stream>>>(E, nf.get(), nt.get());
-    PBGPU_LAUNCHED(c);
-    size_t bytes = 0;
-    PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, bytes, nf.get(), of.get(), nb + 1, c->stream));
-    PBGPU_CUDA(c, ensure_tmp(c, bytes));
-    PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(c->tmp.get(), bytes, nf.get(), of.get(), nb + 1, c->stream));
-    PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(c->tmp.get(), bytes, nt.get(), ot.get(), nb + 1, c->stream));
-    c->launches += 2 * kCubScanLaunches;
-    int64_t nflux = 0, ntri = 0;
-    PBGPU_CUDA(c, cudaMemcpyAsync(&nflux, of.get() + nb, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
-    PBGPU_CUDA(c, cudaMemcpyAsync(&ntri, ot.get() + nb, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
-    PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
-    DBuf<double4> fl, tv, tn;
-    PBGPU_CUDA(c, fl.alloc(nflux > 0 ? nflux : 1));
-    PBGPU_CUDA(c, tv.alloc(ntri > 0 ? ntri : 1));
-    PBGPU_CUDA(c, tn.alloc(ntri > 0 ? ntri : 1));
-    k_energy_fill<<<grid_for(nb, 128), 128, 0, c->stream>>>(E, of.get(), ot.get(), fl.get(), tv.get(), tn.get());
-    PBGPU_LAUNCHED(c);
-    double* P = c->energy_part.get();
-    if (nflux) {
-      k_flux_total<<<nblk, kTile, 0, c->stream>>>(fl.get(), nflux, P);
+    const int64_t nslots = c->rays[0].nc + c->rays[1].nc + c->rays[2].nc;
+    const int64_t ns = nslots > 0 ? nslots : 1;
+    DBuf<double4> acc;
+    DBuf<uint8_t> used;
+    DBuf<int32_t> slot_ray, sel;
+    DBuf<int64_t> nsel;
+    DBuf<unsigned long long> n_extra;
+    // elements whose edge carries no crossing (an epsilon jump seen through a
+    // hanging corner) keep their own point; their list starts at nb entries and
+    // is grown and the pass repeated if it overflows
+    int64_t extra_cap = nb + 1024;
+    DBuf<double4> xp, xd;
+    PBGPU_CUDA(c, acc.alloc(ns));
+    PBGPU_CUDA(c, used.alloc(ns));
+    PBGPU_CUDA(c, slot_ray.alloc(ns));
+    PBGPU_CUDA(c, sel.alloc(ns));
+    PBGPU_CUDA(c, nsel.alloc(1));
+    PBGPU_CUDA(c, n_extra.alloc(1));
+    E.acc = acc.get();
+    E.used = used.get();
+    E.slot_ray = slot_ray.get();
+    E.n_extra = n_extra.get();
+    unsigned long long nx = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      PBGPU_CUDA(c, xp.alloc(extra_cap));
+      PBGPU_CUDA(c, xd.alloc(extra_cap));
+      PBGPU_CUDA(c, cudaMemsetAsync(acc.get(), 0, ns * sizeof(double4), c->stream));
+      PBGPU_CUDA(c, cudaMemsetAsync(used.get(), 0, ns, c->stream));
+      PBGPU_CUDA(c, cudaMemsetAsync(n_extra.get(), 0, sizeof(unsigned long long), c->stream));
+      E.extra_p = xp.get();
+      E.extra_d = xd.get();
+      E.extra_cap = extra_cap;
+      k_energy_accumulate<<<grid_for(nb, 128), 128, 0, c->stream>>>(E);
       PBGPU_LAUNCHED(c);
-      if ((st = sum_partials(c, P, nblk, &charge_pol)) != PBGPU_OK) return st;
-      if (m) {
-        k_nbody_flux<<<nblk, kTile, 0, c->stream>>>(fl.get(), nflux, dq.get(), m, P);
-        PBGPU_LAUNCHED(c);
-        if ((st = sum_partials(c, P, nblk, &first_int)) != PBGPU_OK) return st;
-      }
+      PBGPU_CUDA(c, cudaMemcpyAsync(&nx, n_extra.get(), sizeof(nx), cudaMemcpyDeviceToHost, c->stream));
+      PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+      if ((int64_t)nx <= extra_cap) break;
+      extra_cap = (int64_t)nx;
     }
-    if (ionic && ntri && m) {
-      k_nbody_tri<<<nblk, kTile, 0, c->stream>>>(tv.get(), tn.get(), ntri, dq.get(), m, P);
+    if ((int64_t)nx > extra_cap) return c->fail(PBGPU_ERR_CAPACITY, "energy: surface element list overflow");
+    cub::CountingInputIterator<int32_t> idx(0);
+    size_t bytes = 0;
+    PBGPU_CUDA(c, cub::DeviceSelect::Flagged(nullptr, bytes, idx, used.get(), sel.get(), nsel.get(), ns, c->stream));
+    PBGPU_CUDA(c, ensure_tmp(c, bytes));
+    PBGPU_CUDA(c, cub::DeviceSelect::Flagged(c->tmp.get(), bytes, idx, used.get(), sel.get(), nsel.get(), ns, c->stream));
+    c->launches += kCubSelectLaunches;
+    int64_t np = 0;
+    PBGPU_CUDA(c, cudaMemcpyAsync(&np, nsel.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+    PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    const int64_t npts = np + (int64_t)nx;
+    DBuf<double4> P, D;
+    PBGPU_CUDA(c, P.alloc(npts > 0 ? npts : 1));
+    PBGPU_CUDA(c, D.alloc(npts > 0 ? npts : 1));
+    if (np) {
+      k_energy_points<<<grid_for(np, 256), 256, 0, c->stream>>>(sel.get(), np, E, P.get(), D.get());
       PBGPU_LAUNCHED(c);
-      if ((st = sum_partials(c, P, nblk, &second_int)) != PBGPU_OK) return st;
+    }
+    if (nx) {
+      PBGPU_CUDA(c, cudaMemcpyAsync(P.get() + np, xp.get(), nx * sizeof(double4), cudaMemcpyDeviceToDevice, c->stream));
+      PBGPU_CUDA(c, cudaMemcpyAsync(D.get() + np, xd.get(), nx * sizeof(double4), cudaMemcpyDeviceToDevice, c->stream));
+    }
+    c->energy_points = npts;
+    c->energy_pairs += npts * m;
+    if (npts) {
+      double s[3] = {0, 0, 0};
+      if (ionic)
+        k_energy_pairs<true><<<nblk, kTile, 0, c->stream>>>(P.get(), D.get(), npts, dq.get(), m, c->energy_part.get());
+      else
+        k_energy_pairs<false><<<nblk, kTile, 0, c->stream>>>(P.get(), D.get(), npts, dq.get(), m, c->energy_part.get());
+      PBGPU_LAUNCHED(c);
+      if ((st = sum_partials(c, c->energy_part.get(), nblk, 3, s)) != PBGPU_OK) return st;
+      first_int = s[0];
+      second_int = s[1];
+      charge_pol = s[2];
     }
   }
   if (c->model.calc_coulombic == 1 && m > 1) {
     k_coulomb<<<nblk, kTile, 0, c->stream>>>(dq.get(), m, c->energy_part.get());
     PBGPU_LAUNCHED(c);
-    if ((st = sum_partials(c, c->energy_part.get(), nblk, &coul)) != PBGPU_OK) return st;
+    if ((st = sum_partials(c, c->energy_part.get(), nblk, 1, &coul)) != PBGPU_OK) return st;
     coul *= 1.0 / c->eps_in;
   }
   pbgpu_energy_out e{};

@@ -3,11 +3,13 @@
 // mumps_compute_electric_potential, :2200-2239).
 //
 // Design (B200, HBM-bound):
-//  * SpMV: one thread per row, SELL slices of C rows stored in groups of 4
-//    columns so each thread issues one 16-byte column load and two 16-byte value
-//    loads per 4 nonzeros; a warp reads 1 KiB (values) + 512 B (columns)
-//    contiguous per group.  Matrix streams are loaded with the evict-first hint
-//    (__ldcs) so the gathered vector stays resident in the 126 MB L2.
+//  * SpMV: one thread per row, SELL slices of C rows; each row's columns are
+//    stored in groups of G (1, 2 or 4) lane-interleaved, so a warp's loads of
+//    one group are contiguous (G = 4: one 16-byte column load and two 16-byte
+//    value loads per 4 nonzeros).  Rows are sorted by length inside windows of
+//    sigma rows, which keeps padding near zero on these irregular meshes.
+//    Matrix streams are loaded with the evict-first hint (__ldcs) so the
+//    gathered vector stays resident in the 126 MB L2.
 //  * Every dot product is fused into the kernel that produces its operands;
 //    block partials are reduced by the last block to finish (ticket counter), in
 //    fixed block order, so results are deterministic and the Krylov scalars
@@ -27,6 +29,8 @@
 namespace pbgpu {
 
 constexpr int kBlock = 256;
+// resident blocks per SM the SpMV kernels are compiled for (registers <= 65536 / (256 * 5))
+constexpr int kSpmvMinBlocks = 5;
 
 template <typename T>
 struct SellT {
@@ -36,44 +40,68 @@ struct SellT {
   const T* sval;
   int64_t n_pad;
   int C;
+  int G;  // columns per row stored contiguously: 1, 2 or 4
 };
 
 template <typename T>
-struct Vec2 {};
+struct V2 {};
 template <>
-struct Vec2<double> {
-  using type = double2;
+struct V2<double> {
+  using t = double2;
 };
 template <>
-struct Vec2<float> {
-  using type = float2;
+struct V2<float> {
+  using t = float2;
 };
 
-// y_p = sum_j A(p, j) x_j for SELL row p.
-template <typename T>
+// y_p = sum_j A(p, j) x_j for SELL row p.  Element j of row p sits at
+// slice_ptr[s] + (j / G) G C + lane G + j % G, so for every G a warp's loads
+// of one column group are contiguous.
+template <typename T, int G>
 __device__ __forceinline__ T sell_row(const SellT<T>& A, int64_t p, const T* __restrict__ x) {
   const int64_t s = p / A.C;
   const int lane = (int)(p - s * A.C);
   const int W = A.slice_w[s];
-  const int64_t base = A.slice_ptr[s] + lane * 4;
-  const int64_t stride = 4 * (int64_t)A.C;
   T acc = 0;
-  for (int g = 0; g < (W >> 2); ++g) {
-    const int64_t k = base + g * stride;
-    const int4 c = __ldcs(reinterpret_cast<const int4*>(A.scol + k));
-    if constexpr (sizeof(T) == 8) {
-      const double2 v0 = __ldcs(reinterpret_cast<const double2*>(A.sval + k));
-      const double2 v1 = __ldcs(reinterpret_cast<const double2*>(A.sval + k + 2));
-      acc += v0.x * x[c.x];
-      acc += v0.y * x[c.y];
-      acc += v1.x * x[c.z];
-      acc += v1.y * x[c.w];
-    } else {
-      const float4 v = __ldcs(reinterpret_cast<const float4*>(A.sval + k));
+  if constexpr (G == 1) {
+    const int64_t base = A.slice_ptr[s] + lane;
+    const int64_t stride = A.C;
+#pragma unroll 4
+    for (int j = 0; j < W; ++j) {
+      const int64_t k = base + j * stride;
+      acc += __ldcs(A.sval + k) * x[__ldcs(A.scol + k)];
+    }
+  } else if constexpr (G == 2) {
+    const int64_t base = A.slice_ptr[s] + 2 * lane;
+    const int64_t stride = 2 * (int64_t)A.C;
+#pragma unroll 2
+    for (int g = 0; g < (W >> 1); ++g) {
+      const int64_t k = base + g * stride;
+      const int2 c = __ldcs(reinterpret_cast<const int2*>(A.scol + k));
+      const typename V2<T>::t v = __ldcs(reinterpret_cast<const typename V2<T>::t*>(A.sval + k));
       acc += v.x * x[c.x];
       acc += v.y * x[c.y];
-      acc += v.z * x[c.z];
-      acc += v.w * x[c.w];
+    }
+  } else {
+    const int64_t base = A.slice_ptr[s] + 4 * lane;
+    const int64_t stride = 4 * (int64_t)A.C;
+    for (int g = 0; g < (W >> 2); ++g) {
+      const int64_t k = base + g * stride;
+      const int4 c = __ldcs(reinterpret_cast<const int4*>(A.scol + k));
+      if constexpr (sizeof(T) == 8) {
+        const double2 v0 = __ldcs(reinterpret_cast<const double2*>(A.sval + k));
+        const double2 v1 = __ldcs(reinterpret_cast<const double2*>(A.sval + k + 2));
+        acc += v0.x * x[c.x];
+        acc += v0.y * x[c.y];
+        acc += v1.x * x[c.z];
+        acc += v1.y * x[c.w];
+      } else {
+        const float4 v = __ldcs(reinterpret_cast<const float4*>(A.sval + k));
+        acc += v.x * x[c.x];
+        acc += v.y * x[c.y];
+        acc += v.z * x[c.z];
+        acc += v.w * x[c.w];
+      }
     }
   }
   return acc;
@@ -164,12 +192,12 @@ __global__ void k_cg_init(int64_t n, const T* __restrict__ b, const T* __restric
   }
 }
 
-template <typename T>
-__global__ void k_cg_spmv(SellT<T> A, const T* __restrict__ p, T* __restrict__ q, KrylovScalars* ks, double* partials) {
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock, kSpmvMinBlocks) k_cg_spmv(SellT<T> A, const T* __restrict__ p, T* __restrict__ q, KrylovScalars* ks, double* partials) {
   if (ks->done) return;
   double v[1] = {0.0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x) {
-    const T y = sell_row<T>(A, i, p);
+    const T y = sell_row<T, G>(A, i, p);
     q[i] = y;
     v[0] += (double)p[i] * (double)y;
   }
@@ -272,13 +300,13 @@ __global__ void k_bicg_p(int64_t n, T* __restrict__ p, T* __restrict__ ph, const
 }
 
 // v = A ph;  alpha = rho_new / (rh, v)
-template <typename T>
-__global__ void k_bicg_v(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh,
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock, kSpmvMinBlocks) k_bicg_v(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh,
                          KrylovScalars* ks, double* partials) {
   if (ks->done) return;
   double s[1] = {0.0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x) {
-    const T y = sell_row<T>(A, i, ph);
+    const T y = sell_row<T, G>(A, i, ph);
     v[i] = y;
     s[0] += (double)rh[i] * (double)y;
   }
@@ -311,13 +339,13 @@ __global__ void k_bicg_s(int64_t n, const T* __restrict__ r, const T* __restrict
 }
 
 // t = A sh;  omega = (t, s) / (t, t)
-template <typename T>
-__global__ void k_bicg_t(SellT<T> A, const T* __restrict__ sh, T* __restrict__ t, const T* __restrict__ s,
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock, kSpmvMinBlocks) k_bicg_t(SellT<T> A, const T* __restrict__ sh, T* __restrict__ t, const T* __restrict__ s,
                          KrylovScalars* ks, double* partials) {
   if (ks->done || ks->s_conv) return;
   double a[2] = {0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x) {
-    const T y = sell_row<T>(A, i, sh);
+    const T y = sell_row<T, G>(A, i, sh);
     t[i] = y;
     a[0] += (double)y * (double)s[i];
     a[1] += (double)y * (double)y;
@@ -381,11 +409,12 @@ __global__ void k_bicg_x(int64_t n, T* __restrict__ x, T* __restrict__ r, const 
 
 // ---------------------------------------------------------------------------
 // FP64 residual r = b - A x, its norm, and an fp32 copy (mixed precision).
-__global__ void k_residual(SellT<double> A, int64_t n, const double* __restrict__ b, const double* __restrict__ x,
+template <int G>
+__global__ void __launch_bounds__(kBlock, kSpmvMinBlocks) k_residual(SellT<double> A, int64_t n, const double* __restrict__ b, const double* __restrict__ x,
                            double* __restrict__ r, float* __restrict__ r32, KrylovScalars* ks, double* partials) {
   double a[2] = {0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x) {
-    const double ri = i < n ? b[i] - sell_row<double>(A, i, x) : 0.0;
+    const double ri = i < n ? b[i] - sell_row<double, G>(A, i, x) : 0.0;
     if (r) r[i] = ri;
     if (r32) r32[i] = (float)ri;
     a[0] += ri * ri;
@@ -430,10 +459,11 @@ struct KrylovVecs {
   SellT<T> A;
 };
 
-// Run one Krylov solve on (A, b) to relative tolerance tol; x0 = 0.
-template <typename T>
-static int krylov(Context* c, int method, const KrylovVecs<T>& K, double tol, int max_iter, int check_every,
-                  int* iters, int* status) {
+// Run one Krylov solve on (A, b) to relative tolerance tol; x0 = 0.  GW is the
+// SELL column-group width of A.
+template <typename T, int GW>
+static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, double tol, int max_iter, int check_every,
+                    int* iters, int* status) {
   const int64_t n = K.A.n_pad;
   const int G = grid_blocks(c, n);
   KrylovScalars* ks = c->ks.get();
@@ -456,8 +486,11 @@ static int krylov(Context* c, int method, const KrylovVecs<T>& K, double tol, in
     ev.resize(2 * spmv_per_it * check_every);
     for (cudaEvent_t& e : ev) PBGPU_CUDA(c, cudaEventCreate(&e));
   }
+  // cudaEventRecordExternal makes the record a node of the captured graph
+  // (a plain record inside a capture only orders streams)
   auto mark = [&](int k, int which, int end) {
-    if (c->profiling) cudaEventRecord(ev[2 * (k * spmv_per_it + which) + end], c->stream);
+    if (c->profiling)
+      cudaEventRecordWithFlags(ev[2 * (k * spmv_per_it + which) + end], c->stream, cudaEventRecordExternal);
   };
   // the chunk of iterations is captured once and replayed
   cudaGraph_t graph = nullptr;
@@ -466,18 +499,18 @@ static int krylov(Context* c, int method, const KrylovVecs<T>& K, double tol, in
   for (int k = 0; k < check_every; ++k) {
     if (method == PBGPU_CG) {
       mark(k, 0, 0);
-      k_cg_spmv<T><<<G, kBlock, 0, c->stream>>>(K.A, K.p, K.q, ks, part);
+      k_cg_spmv<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.p, K.q, ks, part);
       mark(k, 0, 1);
       k_cg_update<T><<<G, kBlock, 0, c->stream>>>(n, K.x, K.r, K.p, K.q, K.dinv, ks, part);
       k_cg_pupdate<T><<<G, kBlock, 0, c->stream>>>(n, K.p, K.r, K.dinv, ks);
     } else {
       k_bicg_p<T><<<G, kBlock, 0, c->stream>>>(n, K.p, K.ph, K.r, K.v, K.dinv, ks);
       mark(k, 0, 0);
-      k_bicg_v<T><<<G, kBlock, 0, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
+      k_bicg_v<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
       mark(k, 0, 1);
       k_bicg_s<T><<<G, kBlock, 0, c->stream>>>(n, K.r, K.v, K.s, K.sh, K.dinv, ks, part);
       mark(k, 1, 0);
-      k_bicg_t<T><<<G, kBlock, 0, c->stream>>>(K.A, K.sh, K.t, K.s, ks, part);
+      k_bicg_t<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.sh, K.t, K.s, ks, part);
       mark(k, 1, 1);
       k_bicg_x<T><<<G, kBlock, 0, c->stream>>>(n, K.x, K.r, K.ph, K.sh, K.s, K.t, K.rh, ks, part);
     }
@@ -546,6 +579,26 @@ static int krylov(Context* c, int method, const KrylovVecs<T>& K, double tol, in
   return PBGPU_OK;
 }
 
+template <typename T>
+static int krylov(Context* c, int method, const KrylovVecs<T>& K, double tol, int max_iter, int check_every,
+                  int* iters, int* status) {
+  switch (K.A.G) {
+    case 1: return krylov_g<T, 1>(c, method, K, tol, max_iter, check_every, iters, status);
+    case 2: return krylov_g<T, 2>(c, method, K, tol, max_iter, check_every, iters, status);
+    default: return krylov_g<T, 4>(c, method, K, tol, max_iter, check_every, iters, status);
+  }
+}
+
+// r = b - A x (fp64); optional fp64 / fp32 copies of r; norms into ks
+static void launch_residual(Context* c, const SellT<double>& A, int64_t n, double* r, float* r32) {
+  const int g = grid_blocks(c, A.n_pad);
+  switch (A.G) {
+    case 1: k_residual<1><<<g, kBlock, 0, c->stream>>>(A, n, c->b.get(), c->x.get(), r, r32, c->ks.get(), c->partials.get()); break;
+    case 2: k_residual<2><<<g, kBlock, 0, c->stream>>>(A, n, c->b.get(), c->x.get(), r, r32, c->ks.get(), c->partials.get()); break;
+    default: k_residual<4><<<g, kBlock, 0, c->stream>>>(A, n, c->b.get(), c->x.get(), r, r32, c->ks.get(), c->partials.get()); break;
+  }
+}
+
 static cudaError_t alloc_vectors(Context* c, int64_t n_pad, bool mixed) {
   cudaError_t e;
   DBuf<double>* v64[] = {&c->x, &c->r, &c->p, &c->q, &c->rh, &c->v, &c->s, &c->t, &c->ph, &c->sh};
@@ -576,7 +629,7 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
   PBGPU_CUDA(c, alloc_vectors(c, n_pad, mixed));
   PBGPU_CUDA(c, cudaEventRecord(c->ev0, c->stream));
   int iters = 0, status = PBGPU_OK, outer = 0;
-  SellT<double> A64{c->slice_ptr.get(), c->slice_w.get(), c->scol.get(), c->sval.get(), n_pad, c->C};
+  SellT<double> A64{c->slice_ptr.get(), c->slice_w.get(), c->scol.get(), c->sval.get(), n_pad, c->C, c->G};
   if (!mixed) {
     KrylovVecs<double> K{c->x.get(), c->r.get(), c->p.get(), c->q.get(), c->rh.get(), c->v.get(), c->s.get(),
                          c->t.get(), c->ph.get(), c->sh.get(), c->b.get(), c->dinv.get(), A64};
@@ -589,7 +642,7 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
     k_to_f32<<<grid_blocks(c, n_pad), kBlock, 0, c->stream>>>(n_pad, c->dinv.get(), c->dinv32.get());
     c->launches += 1;
     PBGPU_LAUNCHED(c);
-    SellT<float> A32{c->slice_ptr.get(), c->slice_w.get(), c->scol.get(), c->sval32.get(), n_pad, c->C};
+    SellT<float> A32{c->slice_ptr.get(), c->slice_w.get(), c->scol.get(), c->sval32.get(), n_pad, c->C, c->G};
     PBGPU_CUDA(c, cudaMemsetAsync(c->x.get(), 0, n_pad * sizeof(double), c->stream));
     const int max_outer = opt.max_outer > 0 ? opt.max_outer : 50;
     const double inner = opt.inner_tol > 0 ? opt.inner_tol : 1e-5;
@@ -614,8 +667,7 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
     status = PBGPU_NOT_CONVERGED;
     for (outer = 1; outer <= max_outer; ++outer) {
       // r = b - A x in fp64, handed to the inner solve in fp32
-      k_residual<<<grid_blocks(c, n_pad), kBlock, 0, c->stream>>>(A64, n, c->b.get(), c->x.get(), nullptr,
-                                                                  c->b32.get(), c->ks.get(), c->partials.get());
+      launch_residual(c, A64, n, nullptr, c->b32.get());
       PBGPU_LAUNCHED(c);
       PBGPU_CUDA(c, cudaMemcpyAsync(c->ks_host, c->ks.get(), sizeof(KrylovScalars), cudaMemcpyDeviceToHost, c->stream));
       PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -645,8 +697,7 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
   }
   PBGPU_CUDA(c, cudaEventRecord(c->ev1, c->stream));
   // true residual in fp64
-  k_residual<<<grid_blocks(c, n_pad), kBlock, 0, c->stream>>>(A64, n, c->b.get(), c->x.get(), nullptr, nullptr,
-                                                              c->ks.get(), c->partials.get());
+  launch_residual(c, A64, n, nullptr, nullptr);
   PBGPU_LAUNCHED(c);
   PBGPU_CUDA(c, cudaMemcpyAsync(c->ks_host, c->ks.get(), sizeof(KrylovScalars), cudaMemcpyDeviceToHost, c->stream));
   PBGPU_CUDA(c, c->phi.alloc(n));

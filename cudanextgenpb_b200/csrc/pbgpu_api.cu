@@ -220,9 +220,9 @@ int pbgpu_set_rays(pbgpu_ctx* h, int axis, const pbgpu_rays* r) {
   if ((st = upload(c, R.ptr, r->ptr, nr + 1)) != PBGPU_OK) return st;
   if ((st = upload(c, R.inters, r->inters, nc)) != PBGPU_OK) return st;
   if ((st = upload(c, R.normals, r->normals, 3 * nc)) != PBGPU_OK) return st;
-  DBuf<uint64_t> keys;
-  if ((st = upload(c, keys, r->keys, nr)) != PBGPU_OK) return st;
-  if ((st = build_ray_hash_from(c, axis, keys.get())) != PBGPU_OK) return st;
+  R.nc = nc;
+  if ((st = upload(c, R.keys, r->keys, nr)) != PBGPU_OK) return st;
+  if ((st = build_ray_hash_from(c, axis, R.keys.get())) != PBGPU_OK) return st;
   c->have_rays[axis] = true;
   c->have_markers = c->have_system = c->have_phi = false;
   return PBGPU_OK;
@@ -468,13 +468,15 @@ int pbgpu_get_counters(pbgpu_ctx* h, pbgpu_counters* out) {
   out->spmv_ms = c.spmv_ms;
   out->spmv_bytes = c.spmv_bytes;
   out->krylov_iterations = c.krylov_iters;
+  out->energy_points = c.energy_points;
+  out->energy_pairs = c.energy_pairs;
   return PBGPU_OK;
 }
 
 int pbgpu_reset_counters(pbgpu_ctx* h) {
   CTX_CHECK(h);
   Context& c = h->c;
-  c.launches = c.spmv_launches = c.krylov_iters = 0;
+  c.launches = c.spmv_launches = c.krylov_iters = c.energy_pairs = 0;
   c.spmv_ms = 0.0;
   return PBGPU_OK;
 }

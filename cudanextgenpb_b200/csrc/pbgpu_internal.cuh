@@ -47,8 +47,10 @@ struct DBuf {
 
 struct Rays {
   int64_t n = 0;          // rays with crossings
+  int64_t nc = 0;         // crossings
   int64_t cap = 0;        // hash capacity (power of two)
   int cap_log = 0;
+  DBuf<uint64_t> keys;    // key of each ray (ascending)
   DBuf<uint64_t> hkeys;   // open-addressing table of ray keys
   DBuf<int32_t> hval;     // ray index of each slot
   DBuf<int64_t> ptr;
@@ -119,7 +121,7 @@ struct Context {
   bool have_density = false;
 
   // ---- system in SELL-C-sigma (rows permuted; vectors live in SELL order)
-  int C = 32, sigma = 32;
+  int C = 32, sigma = 2048, G = 1;
   int64_t n_slices = 0, nnz = 0, sell_len = 0;
   DBuf<int64_t> slice_ptr;   // element offset of each slice
   DBuf<int32_t> slice_w;     // width (multiple of 4) of each slice
@@ -161,6 +163,8 @@ struct Context {
   double spmv_ms = 0.0;
   double spmv_bytes = 0.0;
   int64_t krylov_iters = 0;
+  int64_t energy_points = 0;  // surface points of the last energy call
+  int64_t energy_pairs = 0;   // point x charged-atom pairs evaluated
 
   int fail(int code, const std::string& msg) {
     err = msg;
@@ -229,12 +233,14 @@ struct RayView {
   const int64_t* ptr;
   const double* inters;
   const double* normals;
+  const uint64_t* keys;
   int64_t cap;
   int cap_log;
 };
 
 inline RayView ray_view(const Rays& r) {
-  return RayView{r.hkeys.get(), r.hval.get(), r.ptr.get(), r.inters.get(), r.normals.get(), r.cap, r.cap_log};
+  return RayView{r.hkeys.get(), r.hval.get(), r.ptr.get(), r.inters.get(), r.normals.get(), r.keys.get(),
+                 r.cap, r.cap_log};
 }
 
 // Which axis edge e runs along, and its two corners (reference edge table,

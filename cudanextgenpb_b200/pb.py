@@ -218,8 +218,10 @@ class GpuPath:
     def create_density_map(self):
         self._check(self._lib.pbgpu_create_density_map(self._ctx))
 
-    def assemble(self, chunk=32, sigma=None):
-        o = N.PbgpuSellOpts(chunk, sigma if sigma is not None else chunk)
+    def assemble(self, chunk=32, sigma=2048, group=1):
+        """SELL-C-sigma layout: slice height `chunk`, length-sorting window
+        `sigma` rows, `group` columns stored contiguously per row."""
+        o = N.PbgpuSellOpts(chunk, sigma, group)
         self._check(self._lib.pbgpu_assemble(self._ctx, C.byref(o)))
 
     def solve(self, opts: N.PbgpuSolverOpts | None = None, allow_not_converged=False):
@@ -299,10 +301,10 @@ class GpuPath:
     def reset_counters(self):
         self._check(self._lib.pbgpu_reset_counters(self._ctx))
 
-    def run(self, opts=None, fast=False, chunk=32, sigma=None):
+    def run(self, opts=None, fast=False, chunk=32, sigma=2048, group=1):
         """create_markers .. energy in the driver's order; returns (energy dict, solve stats)."""
         self.create_markers()
         self.create_density_map()
-        self.assemble(chunk, sigma)
+        self.assemble(chunk, sigma, group)
         st = self.solve(opts)
         return self.energy(fast), st

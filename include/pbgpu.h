@@ -99,7 +99,9 @@ typedef struct {
 
 typedef struct {
   int chunk;                 /* SELL slice height C (multiple of 32; 0 = default 32) */
-  int sigma;                 /* sorting window in rows (multiple of chunk; 0 = default) */
+  int sigma;                 /* sorting window in rows (1 or a multiple of chunk; 0 = default 2048) */
+  int group;                 /* columns stored contiguously per row: 1, 2 or 4 (0 = default 1);
+                                a thread loads `group` values with one load instruction */
 } pbgpu_sell_opts;
 
 typedef struct {
@@ -203,6 +205,8 @@ typedef struct {
   double spmv_ms;
   double spmv_bytes;
   int64_t krylov_iterations;
+  int64_t energy_points;     /* distinct surface points of the last energy call */
+  int64_t energy_pairs;      /* surface point x charged atom pairs evaluated */
 } pbgpu_counters;
 int pbgpu_set_profiling(pbgpu_ctx* ctx, int on);
 int pbgpu_get_counters(pbgpu_ctx* ctx, pbgpu_counters* out);
