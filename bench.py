@@ -328,7 +328,7 @@ def run_ours(args, rank, world, local):
                 "workload": workload_desc(args.workload, info),
                 "n_dof": info["n_nodes"], "n_octants": info["n_oct"], "n_hanging": info["n_hang"],
                 "n_atoms": info["n_atoms"], "nnz": info_nnz(g), "cg_iterations": int(np.median(iters)),
-                "tol": args.tol, "sell": {"C": args.chunk, "sigma": args.sigma},
+                "tol": args.tol, "sell": {"C": args.chunk, "sigma": args.sigma, "group": args.group},
                 "energy_kT": energies[-1],
                 "dof_iterations_per_s": world * info["n_nodes"] * float(np.median(iters)) / (ms / 1e3 / args.steps),
                 "stage_ms": stage,

@@ -102,74 +102,140 @@ struct RowAcc {
   }
 };
 
-// Gather row i of A and its right-hand side entry (before Dirichlet handling).
-__device__ void gather_row(int64_t i, const AsmView& A, RowAcc& R, double& rhs) {
+// Local box-method coefficients of every octant, computed once per octant
+// with the expressions (and accumulation order) of the local matrix: the 12
+// edge conductances wha(eps_i1, eps_i2, f) * area_h, the 8 diagonal entries
+// (sum of the corner's 3 conductances in edge order, then the lumped reaction
+// kappa_c * V/8 * w_c, w_c the product of the corner's half-edge shares), and
+// the 8 right-hand-side terms V/8 * rho_c.
+__global__ void k_octant_local(AsmView A, int64_t n_oct, double* __restrict__ cond, double* __restrict__ kd,
+                               double* __restrict__ fr) {
+  const int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (o >= n_oct) return;
+  const int4 q = A.oct[o];
+  const int32_t s = 1 << (kRootLog - q.w);
+  const int32_t qc[3] = {q.x, q.y, q.z};
+  double h[3];
+  for (int d = 0; d < 3; ++d) h[d] = coord(A.lo[d], A.len[d], qc[d] + s) - coord(A.lo[d], A.len[d], qc[d]);
+  const double area_h[3] = {h[1] * h[2] / h[0] * 0.25, h[0] * h[2] / h[1] * 0.25, h[0] * h[1] / h[2] * 0.25};
+  const double v8 = h[0] * h[1] * h[2] * 0.125;
+  const int32_t bp = A.border_pos[o];
+  const int4 na = reinterpret_cast<const int4*>(A.oct_nodes)[2 * o];
+  const int4 nb = reinterpret_cast<const int4*>(A.oct_nodes)[2 * o + 1];
+  const int32_t nd[8] = {na.x, na.y, na.z, na.w, nb.x, nb.y, nb.z, nb.w};
+  double ec[8], w[8], k[8];
+  for (int c = 0; c < 8; ++c) {
+    ec[c] = corner_val(A.eps, nd[c], A);
+    w[c] = 1.0;
+    k[c] = 0.0;
+  }
+  double* co = cond + 12 * o;
+  for (int e = 0; e < 12; ++e) {
+    const int i1 = d_edge_nodes[2 * e], i2 = d_edge_nodes[2 * e + 1];
+    const double f = bp >= 0 ? A.frac[12 * (int64_t)bp + e] : 0.5;
+    const double c = wha(ec[i1], ec[i2], f) * area_h[d_edge_axis[e]];
+    co[e] = c;
+    k[i1] += c;
+    k[i2] += c;
+    w[i1] *= fmin(1.0, 2.0 * f);
+    w[i2] *= fmin(1.0, 2.0 * (1.0 - f));
+  }
+  for (int c = 0; c < 8; ++c) {
+    if (A.stern)
+      k[c] += A.react_cell[o] * v8;
+    else
+      k[c] += corner_val(A.react, nd[c], A) * v8 * w[c];
+    kd[8 * o + c] = k[c];
+    fr[8 * o + c] = v8 * corner_val(A.rho, nd[c], A);
+  }
+}
+
+struct LocalView {
+  const double* cond;
+  const double* kd;
+  const double* fr;
+};
+
+// The 3 edges at corner a in ascending edge id, with their axes.
+__device__ __forceinline__ void corner_edges(int a, int ed[3], int ax[3]) {
+  for (int d = 0; d < 3; ++d) {
+    ed[d] = edge_of(a, d);
+    ax[d] = d;
+  }
+  for (int u = 0; u < 3; ++u)
+    for (int v = u + 1; v < 3; ++v)
+      if (ed[v] < ed[u]) {
+        int tmp = ed[u];
+        ed[u] = ed[v];
+        ed[v] = tmp;
+        tmp = ax[u];
+        ax[u] = ax[v];
+        ax[v] = tmp;
+      }
+}
+
+// Gather row i of A and its right-hand side entry (before Dirichlet handling)
+// from the octants' local coefficients: A = P^T K P over the node's incidences.
+__device__ void gather_row(int64_t i, const AsmView& A, const LocalView& L, RowAcc& R, double& rhs) {
   rhs = 0.0;
   for (int64_t e = A.inc_ptr[i]; e < A.inc_ptr[i + 1]; ++e) {
     const uint32_t t = A.inc[e];
     const int64_t o = t >> 3;
     const int a = (int)(t & 7);
-    const int4 q = A.oct[o];
-    const int32_t s = 1 << (kRootLog - q.w);
-    const int32_t qc[3] = {q.x, q.y, q.z};
-    double h[3];
-    for (int d = 0; d < 3; ++d) h[d] = coord(A.lo[d], A.len[d], qc[d] + s) - coord(A.lo[d], A.len[d], qc[d]);
-    const double area_h[3] = {h[1] * h[2] / h[0] * 0.25, h[0] * h[2] / h[1] * 0.25, h[0] * h[1] / h[2] * 0.25};
-    const double v8 = h[0] * h[1] * h[2] * 0.125;
-    const int32_t bp = A.border_pos[o];
     const int32_t nda = A.oct_nodes[t];
     const double wa = nda < A.n ? 1.0 : 1.0 / A.hang_np[nda - A.n];
-    const double ea = corner_val(A.eps, nda, A);
-    // the 3 edges at corner a, in ascending edge id (the order the local
-    // matrix accumulates them in)
+    const double kaa = L.kd[t];
     int ed[3], ax[3];
-    for (int d = 0; d < 3; ++d) {
-      ed[d] = edge_of(a, d);
-      ax[d] = d;
-    }
-    for (int u = 0; u < 3; ++u)
-      for (int v = u + 1; v < 3; ++v)
-        if (ed[v] < ed[u]) {
-          int tmp = ed[u];
-          ed[u] = ed[v];
-          ed[v] = tmp;
-          tmp = ax[u];
-          ax[u] = ax[v];
-          ax[v] = tmp;
-        }
-    double cond[3], kaa = 0.0, wr = 1.0;
-    int32_t ndb[3];
-    for (int u = 0; u < 3; ++u) {
-      const int d = ax[u];
-      const int b = a ^ (1 << d);
-      ndb[u] = A.oct_nodes[8 * o + b];
-      const double eb = corner_val(A.eps, ndb[u], A);
-      const double f = bp >= 0 ? A.frac[12 * (int64_t)bp + ed[u]] : 0.5;
-      const bool first = ((a >> d) & 1) == 0;  // a is the edge's first node
-      const double c = first ? wha(ea, eb, f) * area_h[d] : wha(eb, ea, f) * area_h[d];
-      cond[u] = c;
-      kaa += c;
-      wr *= first ? fmin(1.0, 2.0 * f) : fmin(1.0, 2.0 * (1.0 - f));
-    }
-    if (A.stern)
-      kaa += A.react_cell[o] * v8;
-    else
-      kaa += corner_val(A.react, nda, A) * v8 * wr;
+    corner_edges(a, ed, ax);
     int32_t g[4];
     double w[4];
     int ng = expand(nda, A, g, w);
     for (int j = 0; j < ng; ++j) R.add(g[j], wa * kaa * w[j]);
     for (int u = 0; u < 3; ++u) {
-      ng = expand(ndb[u], A, g, w);
-      const double kab = 0.0 - cond[u];
+      const int32_t ndb = A.oct_nodes[8 * o + (a ^ (1 << ax[u]))];
+      const double kab = 0.0 - L.cond[12 * o + ed[u]];
+      ng = expand(ndb, A, g, w);
       for (int j = 0; j < ng; ++j) R.add(g[j], wa * kab * w[j]);
     }
-    const double fc = v8 * corner_val(A.rho, nda, A);
-    rhs += wa * fc;
+    rhs += wa * L.fr[t];
   }
 }
 
-// Pass 1: number of stored columns of each row.
+// Sorted set of column ids held by one thread (pass 1 needs no values).
+struct ColSet {
+  int32_t col[kMaxRow];
+  int m = 0;
+  bool overflow = false;
+  __device__ __forceinline__ void add(int32_t c) {
+    int j = m - 1;
+    while (j >= 0 && col[j] > c) --j;
+    if (j >= 0 && col[j] == c) return;
+    if (m == kMaxRow) {
+      overflow = true;
+      return;
+    }
+    for (int k = m - 1; k > j; --k) col[k + 1] = col[k];
+    col[j + 1] = c;
+    ++m;
+  }
+};
+
+__device__ __forceinline__ void add_expanded(int32_t nd, const AsmView& A, ColSet& S) {
+  if (nd < A.n) {
+    S.add(nd);
+    return;
+  }
+  const int64_t h = nd - A.n;
+  const int4 p = A.hang_par[h];
+  S.add(p.x);
+  S.add(p.y);
+  if (A.hang_np[h] == 4) {
+    S.add(p.z);
+    S.add(p.w);
+  }
+}
+
+// Pass 1: number of stored columns of each row (topology only).
 __global__ void k_row_len(AsmView A, int32_t* __restrict__ rowlen, int* __restrict__ overflow) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= A.n) return;
@@ -177,12 +243,17 @@ __global__ void k_row_len(AsmView A, int32_t* __restrict__ rowlen, int* __restri
     rowlen[i] = 1;
     return;
   }
-  RowAcc R;
-  double rhs;
-  gather_row(i, A, R, rhs);
-  if (R.overflow) atomicExch(overflow, 1);
+  ColSet S;
+  for (int64_t e = A.inc_ptr[i]; e < A.inc_ptr[i + 1]; ++e) {
+    const uint32_t t = A.inc[e];
+    const int64_t o = t >> 3;
+    const int a = (int)(t & 7);
+    add_expanded(A.oct_nodes[t], A, S);
+    for (int d = 0; d < 3; ++d) add_expanded(A.oct_nodes[8 * o + (a ^ (1 << d))], A, S);
+  }
+  if (S.overflow) atomicExch(overflow, 1);
   int m = 0;
-  for (int j = 0; j < R.m; ++j) m += A.dirichlet[R.col[j]] ? 0 : 1;
+  for (int j = 0; j < S.m; ++j) m += A.dirichlet[S.col[j]] ? 0 : 1;
   rowlen[i] = m;
 }
 
@@ -206,7 +277,7 @@ __device__ __forceinline__ int64_t sell_index(const SellOut& S, int64_t p, int j
 }
 
 // Pass 2: values, columns (SELL numbering), right-hand side, 1/diagonal.
-__global__ void k_row_fill(AsmView A, SellOut S) {
+__global__ void k_row_fill(AsmView A, LocalView L, SellOut S) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= A.n) return;
   const int64_t p = S.iperm[i];
@@ -221,7 +292,7 @@ __global__ void k_row_fill(AsmView A, SellOut S) {
   } else {
     RowAcc R;
     double rhs;
-    gather_row(i, A, R, rhs);
+    gather_row(i, A, L, R, rhs);
     double diag = 1.0;
     for (int u = 0; u < R.m; ++u) {
       const int32_t cn = R.col[u];
@@ -444,7 +515,15 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   PBGPU_CUDA(c, c->dinv.alloc(n_pad));
   SellOut S{c->slice_ptr.get(), c->slice_w.get(), c->iperm.get(), c->scol.get(), c->sval.get(), c->b.get(),
             c->dinv.get(), C, G};
-  k_row_fill<<<grid_for(n, 128), 128, 0, c->stream>>>(A, S);
+  // local coefficients of every octant, once
+  DBuf<double> ocond, okd, ofr;
+  PBGPU_CUDA(c, ocond.alloc(12 * c->n_oct));
+  PBGPU_CUDA(c, okd.alloc(8 * c->n_oct));
+  PBGPU_CUDA(c, ofr.alloc(8 * c->n_oct));
+  k_octant_local<<<grid_for(c->n_oct, 128), 128, 0, c->stream>>>(A, c->n_oct, ocond.get(), okd.get(), ofr.get());
+  PBGPU_LAUNCHED(c);
+  const LocalView L{ocond.get(), okd.get(), ofr.get()};
+  k_row_fill<<<grid_for(n, 128), 128, 0, c->stream>>>(A, L, S);
   PBGPU_LAUNCHED(c);
   if (n_pad > n) {
     k_pad_rows<<<grid_for(n_pad - n, 128), 128, 0, c->stream>>>(S, n, n_pad);
