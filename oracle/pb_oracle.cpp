@@ -386,99 +386,117 @@ struct Trip {
   double v;
 };
 
-// assemple_system_matrix (src/pb_class.cpp:2053-2159) with the bimpp operators
-// restated as described at the top of this file.
-int oracle_assemble(oracle_state* s) {
-  if (!s->have_markers || !s->have_density) return PBGPU_ERR_STATE;
+// The local box-method matrix K (8x8), right-hand side f and corner expansion
+// of octant o (bimpp operators restated as at the top of this file).
+struct Local {
+  double K[8][8];
+  double f[8];
+  int32_t g[8][4];
+  double gw[8][4];
+  int ng[8];
+};
+
+static void local_octant(const oracle_state* s, int64_t o, Local& L) {
+  const int64_t n = s->n;
+  const bool stern = s->model.stern_layer_surf == 1;
+  double h[3];
+  octant_h(s, o, h);
+  const double area_h[3] = {h[1] * h[2] / h[0] * 0.25, h[0] * h[2] / h[1] * 0.25, h[0] * h[1] / h[2] * 0.25};
+  const double v8 = h[0] * h[1] * h[2] * 0.125;
+  double f[12];
+  const int64_t bp = s->border_pos[o];
+  for (int e = 0; e < 12; ++e) f[e] = bp >= 0 ? s->frac[12 * bp + e] : 0.5;
+  double ec[8], kc[8], rc[8], w[8];
+  for (int c = 0; c < 8; ++c) {
+    const int32_t nd = s->oct_nodes[8 * o + c];
+    ec[c] = s->corner_val(s->eps, nd);
+    kc[c] = s->corner_val(s->react, nd);
+    rc[c] = s->corner_val(s->rho, nd);
+    w[c] = 1.0;
+  }
+  std::memset(L.K, 0, sizeof(L.K));
+  for (int e = 0; e < 12; ++e) {
+    const int i1 = E2N[2 * e], i2 = E2N[2 * e + 1];
+    const double c = wha(ec[i1], ec[i2], f[e]) * area_h[EAX[e]];
+    L.K[i1][i1] += c;
+    L.K[i2][i2] += c;
+    L.K[i1][i2] -= c;
+    L.K[i2][i1] -= c;
+    w[i1] *= std::min(1.0, 2.0 * f[e]);
+    w[i2] *= std::min(1.0, 2.0 * (1.0 - f[e]));
+  }
+  for (int c = 0; c < 8; ++c) {
+    if (stern)
+      L.K[c][c] += s->react_cell[o] * v8;
+    else
+      L.K[c][c] += kc[c] * v8 * w[c];
+    L.f[c] = v8 * rc[c];
+  }
+  for (int c = 0; c < 8; ++c) {
+    const int32_t nd = s->oct_nodes[8 * o + c];
+    if (nd < n) {
+      L.ng[c] = 1;
+      L.g[c][0] = nd;
+      L.gw[c][0] = 1.0;
+    } else {
+      const int64_t hh = nd - n;
+      L.ng[c] = s->hang_np[hh];
+      for (int j = 0; j < L.ng[c]; ++j) {
+        L.g[c][j] = s->hang_par[4 * hh + j];
+        L.gw[c][j] = 1.0 / L.ng[c];
+      }
+    }
+  }
+}
+
+// Dirichlet nodes: any coordinate on the root boundary; bc_type 0 = none.
+static void dirichlet_nodes(const oracle_state* s, std::vector<int8_t>& dir, std::vector<double>& gval) {
+  const int64_t n = s->n;
+  dir.assign(n, 0);
+  gval.assign(n, 0.0);
+  if (s->model.bc_type == 0) return;
+  for (int64_t i = 0; i < n; ++i) {
+    const int32_t* p = &s->node_xyz[3 * i];
+    bool onb = false;
+    for (int a = 0; a < 3; ++a) onb = onb || p[a] == 0 || p[a] == kRoot;
+    if (onb) {
+      dir[i] = 1;
+      gval[i] = dirichlet_value(s, s->coord(0, p[0]), s->coord(1, p[1]), s->coord(2, p[2]));
+    }
+  }
+}
+
+// Triplet assembly: every octant emits its P^T K P entries in a fixed order
+// (diagonal blocks of corners 0..7, then the 12 edges in both directions),
+// a stable sort by (row, column) groups them, and equal entries are summed in
+// emission order.
+static int assemble_triplets(oracle_state* s) {
   const int64_t n = s->n;
   std::vector<Trip> trips;
   trips.reserve(s->n_oct * 40);
   std::vector<double> b(n, 0.0);
-  const bool stern = s->model.stern_layer_surf == 1;
+  Local L;
   for (int64_t o = 0; o < s->n_oct; ++o) {
-    double h[3];
-    octant_h(s, o, h);
-    const double area_h[3] = {h[1] * h[2] / h[0] * 0.25, h[0] * h[2] / h[1] * 0.25, h[0] * h[1] / h[2] * 0.25};
-    const double v8 = h[0] * h[1] * h[2] * 0.125;
-    double f[12];
-    const int64_t bp = s->border_pos[o];
-    for (int e = 0; e < 12; ++e) f[e] = bp >= 0 ? s->frac[12 * bp + e] : 0.5;
-    double ec[8], kc[8], rc[8], w[8];
-    for (int c = 0; c < 8; ++c) {
-      const int32_t nd = s->oct_nodes[8 * o + c];
-      ec[c] = s->corner_val(s->eps, nd);
-      kc[c] = s->corner_val(s->react, nd);
-      rc[c] = s->corner_val(s->rho, nd);
-      w[c] = 1.0;
-    }
-    double K[8][8];
-    std::memset(K, 0, sizeof(K));
-    for (int e = 0; e < 12; ++e) {
-      const int i1 = E2N[2 * e], i2 = E2N[2 * e + 1];
-      const double c = wha(ec[i1], ec[i2], f[e]) * area_h[EAX[e]];
-      K[i1][i1] += c;
-      K[i2][i2] += c;
-      K[i1][i2] -= c;
-      K[i2][i1] -= c;
-      w[i1] *= std::min(1.0, 2.0 * f[e]);
-      w[i2] *= std::min(1.0, 2.0 * (1.0 - f[e]));
-    }
-    for (int c = 0; c < 8; ++c) {
-      if (stern)
-        K[c][c] += s->react_cell[o] * v8;
-      else
-        K[c][c] += kc[c] * v8 * w[c];
-    }
-    // expansion of each corner onto independent nodes
-    int32_t g[8][4];
-    double gw[8][4];
-    int ng[8];
-    for (int c = 0; c < 8; ++c) {
-      const int32_t nd = s->oct_nodes[8 * o + c];
-      if (nd < n) {
-        ng[c] = 1;
-        g[c][0] = nd;
-        gw[c][0] = 1.0;
-      } else {
-        const int64_t hh = nd - n;
-        ng[c] = s->hang_np[hh];
-        for (int j = 0; j < ng[c]; ++j) {
-          g[c][j] = s->hang_par[4 * hh + j];
-          gw[c][j] = 1.0 / ng[c];
-        }
-      }
-    }
+    local_octant(s, o, L);
     auto put = [&](int a, int bb) {
-      for (int i = 0; i < ng[a]; ++i)
-        for (int j = 0; j < ng[bb]; ++j) trips.push_back({g[a][i], g[bb][j], gw[a][i] * K[a][bb] * gw[bb][j]});
+      for (int i = 0; i < L.ng[a]; ++i)
+        for (int j = 0; j < L.ng[bb]; ++j)
+          trips.push_back({L.g[a][i], L.g[bb][j], L.gw[a][i] * L.K[a][bb] * L.gw[bb][j]});
     };
     for (int c = 0; c < 8; ++c) put(c, c);
     for (int e = 0; e < 12; ++e) {
       put(E2N[2 * e], E2N[2 * e + 1]);
       put(E2N[2 * e + 1], E2N[2 * e]);
     }
-    for (int c = 0; c < 8; ++c) {
-      const double fc = v8 * rc[c];
-      for (int i = 0; i < ng[c]; ++i) b[g[c][i]] += gw[c][i] * fc;
-    }
+    for (int c = 0; c < 8; ++c)
+      for (int i = 0; i < L.ng[c]; ++i) b[L.g[c][i]] += L.gw[c][i] * L.f[c];
   }
   __gnu_parallel::stable_sort(trips.begin(), trips.end(), [](const Trip& x, const Trip& y) {
     return x.row < y.row || (x.row == y.row && x.col < y.col);
   });
-  // Dirichlet nodes: any coordinate on the root boundary; bc_type 0 = none
-  std::vector<int8_t> dir(n, 0);
-  std::vector<double> gval(n, 0.0);
-  if (s->model.bc_type != 0) {
-    for (int64_t i = 0; i < n; ++i) {
-      const int32_t* p = &s->node_xyz[3 * i];
-      bool onb = false;
-      for (int a = 0; a < 3; ++a) onb = onb || p[a] == 0 || p[a] == kRoot;
-      if (onb) {
-        dir[i] = 1;
-        gval[i] = dirichlet_value(s, s->coord(0, p[0]), s->coord(1, p[1]), s->coord(2, p[2]));
-      }
-    }
-  }
+  std::vector<int8_t> dir;
+  std::vector<double> gval;
+  dirichlet_nodes(s, dir, gval);
   s->row_ptr.assign(n + 1, 0);
   s->col.clear();
   s->val.clear();
@@ -507,6 +525,134 @@ int oracle_assemble(oracle_state* s) {
   }
   s->have_system = true;
   return PBGPU_OK;
+}
+
+// Row assembly for large meshes (memory O(nnz)): each row walks its node's
+// octant incidences in ascending order and, inside an octant, the same
+// emission order as the triplet assembly, so both give identical sums.
+static int assemble_rows(oracle_state* s) {
+  const int64_t n = s->n, no = s->n_oct;
+  // node -> octant incidence lists
+  std::vector<int64_t> ptr(n + 1, 0);
+  for (int64_t t = 0; t < 8 * no; ++t) {
+    const int32_t nd = s->oct_nodes[t];
+    if (nd < n)
+      ++ptr[nd + 1];
+    else
+      for (int j = 0; j < s->hang_np[nd - n]; ++j) ++ptr[s->hang_par[4 * (nd - n) + j] + 1];
+  }
+  for (int64_t i = 0; i < n; ++i) ptr[i + 1] += ptr[i];
+  std::vector<int64_t> octs(ptr[n]);
+  {
+    std::vector<int64_t> cur(ptr.begin(), ptr.end() - 1);
+    for (int64_t t = 0; t < 8 * no; ++t) {
+      const int32_t nd = s->oct_nodes[t];
+      if (nd < n)
+        octs[cur[nd]++] = t >> 3;
+      else
+        for (int j = 0; j < s->hang_np[nd - n]; ++j) octs[cur[s->hang_par[4 * (nd - n) + j]]++] = t >> 3;
+    }
+  }
+  std::vector<int8_t> dir;
+  std::vector<double> gval;
+  dirichlet_nodes(s, dir, gval);
+  const int nt = omp_get_max_threads();
+  std::vector<std::vector<int32_t>> tcol(nt);
+  std::vector<std::vector<double>> tval(nt);
+  std::vector<int64_t> rowlen(n, 0);
+  std::vector<double> rhs(n, 0.0);
+  const int64_t chunk = (n + nt - 1) / nt;
+#pragma omp parallel num_threads(nt)
+  {
+    const int tid = omp_get_thread_num();
+    const int64_t r0 = std::min(n, tid * chunk), r1 = std::min(n, r0 + chunk);
+    std::vector<std::pair<int32_t, double>> row;
+    Local L;
+    for (int64_t r = r0; r < r1; ++r) {
+      if (dir[r]) {
+        tcol[tid].push_back((int32_t)r);
+        tval[tid].push_back(1.0);
+        rowlen[r] = 1;
+        rhs[r] = gval[r];
+        continue;
+      }
+      row.clear();
+      double b = 0.0;
+      auto add = [&](int32_t c, double v) {
+        auto it = std::lower_bound(row.begin(), row.end(), std::make_pair(c, -1e308),
+                                   [](const std::pair<int32_t, double>& x, const std::pair<int32_t, double>& y) {
+                                     return x.first < y.first;
+                                   });
+        if (it != row.end() && it->first == c)
+          it->second += v;
+        else
+          row.insert(it, {c, v});
+      };
+      // distinct octants of this row, ascending
+      int64_t k = ptr[r];
+      while (k < ptr[r + 1]) {
+        const int64_t o = octs[k];
+        while (k < ptr[r + 1] && octs[k] == o) ++k;
+        local_octant(s, o, L);
+        // row r's weight in each local corner (0 when r is not behind it)
+        double wr[8];
+        for (int c = 0; c < 8; ++c) {
+          wr[c] = 0.0;
+          for (int i = 0; i < L.ng[c]; ++i)
+            if (L.g[c][i] == r) wr[c] = L.gw[c][i];
+        }
+        auto put = [&](int a, int bb) {
+          if (wr[a] == 0.0) return;
+          for (int j = 0; j < L.ng[bb]; ++j) add(L.g[bb][j], wr[a] * L.K[a][bb] * L.gw[bb][j]);
+        };
+        for (int c = 0; c < 8; ++c) put(c, c);
+        for (int e = 0; e < 12; ++e) {
+          put(E2N[2 * e], E2N[2 * e + 1]);
+          put(E2N[2 * e + 1], E2N[2 * e]);
+        }
+        for (int c = 0; c < 8; ++c)
+          if (wr[c] != 0.0) b += wr[c] * L.f[c];
+      }
+      int64_t m = 0;
+      for (const auto& e : row) {
+        if (dir[e.first]) {
+          b -= e.second * gval[e.first];
+          continue;
+        }
+        tcol[tid].push_back(e.first);
+        tval[tid].push_back(e.second);
+        ++m;
+      }
+      rowlen[r] = m;
+      rhs[r] = b;
+    }
+  }
+  s->row_ptr.assign(n + 1, 0);
+  for (int64_t r = 0; r < n; ++r) s->row_ptr[r + 1] = s->row_ptr[r] + rowlen[r];
+  s->col.clear();
+  s->val.clear();
+  s->col.reserve(s->row_ptr[n]);
+  s->val.reserve(s->row_ptr[n]);
+  for (int t = 0; t < nt; ++t) {
+    s->col.insert(s->col.end(), tcol[t].begin(), tcol[t].end());
+    s->val.insert(s->val.end(), tval[t].begin(), tval[t].end());
+  }
+  s->rhs = rhs;
+  s->have_system = true;
+  return PBGPU_OK;
+}
+
+// assemple_system_matrix (src/pb_class.cpp:2053-2159) with the bimpp operators
+// restated as described at the top of this file.  Meshes above 2M octants use
+// the row assembly (same sums, O(nnz) memory).
+int oracle_assemble(oracle_state* s) {
+  if (!s->have_markers || !s->have_density) return PBGPU_ERR_STATE;
+  return s->n_oct > 2000000 ? assemble_rows(s) : assemble_triplets(s);
+}
+
+int oracle_assemble_mode(oracle_state* s, int rows) {
+  if (!s->have_markers || !s->have_density) return PBGPU_ERR_STATE;
+  return rows ? assemble_rows(s) : assemble_triplets(s);
 }
 
 static void spmv(const oracle_state* s, const double* x, double* y) {

@@ -43,6 +43,10 @@ void oracle_destroy(oracle_state* s);
 int oracle_markers(oracle_state* s);
 int oracle_density(oracle_state* s);
 int oracle_assemble(oracle_state* s);
+/* rows = 0: triplet assembly (emit, stable sort, sum); rows = 1: per-row
+ * gather over node incidences (O(nnz) memory).  Both give identical sums;
+ * oracle_assemble picks the row assembly above 2M octants. */
+int oracle_assemble_mode(oracle_state* s, int rows);
 /* method PBGPU_CG / PBGPU_BICGSTAB, Jacobi preconditioner, x0 = 0, stop on
  * ||b - A x||_2 <= tol ||b||_2 (recursive residual, checked against the true
  * residual at exit).  threads <= 0: all cores.  Returns iterations (<0 error). */

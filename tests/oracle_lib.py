@@ -31,6 +31,7 @@ def load():
         L.oracle_destroy.argtypes = [sp]
         for f in ("oracle_markers", "oracle_density", "oracle_assemble"):
             getattr(L, f).argtypes = [sp]
+        L.oracle_assemble_mode.argtypes = [sp, C.c_int]
         L.oracle_solve.argtypes = [sp, C.c_int, C.c_double, C.c_int, C.c_int, P(C.c_double)]
         L.oracle_phi_on_atoms.argtypes = [sp, P(C.c_double)]
         L.oracle_energy.argtypes = [sp, C.c_int, P(N.PbgpuEnergyOut)]
@@ -108,8 +109,12 @@ class Oracle:
         self._ok(self.L.oracle_get_density(self.s, _d(rho), _d(vp)))
         return rho, vp
 
-    def assemble(self):
-        self._ok(self.L.oracle_assemble(self.s))
+    def assemble(self, mode=None):
+        """mode None: automatic; "triplets" or "rows" forces one assembly."""
+        if mode is None:
+            self._ok(self.L.oracle_assemble(self.s))
+        else:
+            self._ok(self.L.oracle_assemble_mode(self.s, 1 if mode == "rows" else 0))
         return self.system()
 
     def system(self):
