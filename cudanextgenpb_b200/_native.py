@@ -105,6 +105,7 @@ PBGPU_FUNCS = {
     "pbgpu_set_profiling": (C.c_int, [ctx_p, C.c_int]),
     "pbgpu_get_counters": (C.c_int, [ctx_p, P(PbgpuCounters)]),
     "pbgpu_reset_counters": (C.c_int, [ctx_p]),
+    "pbgpu_coulomb_energy_static": (C.c_int, [C.c_void_p, i64, dbl, dbl, C.c_void_p, C.c_void_p]),
 }
 
 host_p = C.c_void_p

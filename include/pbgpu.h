@@ -212,6 +212,28 @@ int pbgpu_set_profiling(pbgpu_ctx* ctx, int on);
 int pbgpu_get_counters(pbgpu_ctx* ctx, pbgpu_counters* out);
 int pbgpu_reset_counters(pbgpu_ctx* ctx);
 
+/* Coulomb energy sum_{i<j} q_i q_j / r_ij / eps_in [kT] that allocates no
+ * device memory.  It has no counterpart in the reference; it is the Coulomb
+ * term of pbgpu_energy (energy_coul) for callers that cannot call cudaMalloc:
+ * code running inside another library's enqueue or plugin callback, where
+ * allocating is not permitted, or a process whose device memory is owned by a
+ * pool allocator.  Needs no context.
+ *   atoms       device pointer, n_atoms x 4 doubles (x, y, z, q); charges with
+ *               |q| <= 1e-5 are left out, as in the reference
+ *   e_in, T     molecular dielectric constant and temperature (eps_in is
+ *               formed in the reference's units)
+ *   out_energy  device pointer to one double, written on `cuda_stream`
+ *               (NULL: the legacy default stream); read it after the stream
+ *               has reached the call
+ * Scratch lives in fixed device arrays of this library (4 MiB, held by every
+ * GPU that loads it until the process exits): at most 131072 atoms
+ * (PBGPU_ERR_CAPACITY beyond).  The first call on a device looks up the
+ * arrays' device addresses (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  All calls share the arrays:
+ * calls whose work overlaps on the GPU race and must be serialised. */
+int pbgpu_coulomb_energy_static(const double* atoms, int64_t n_atoms, double e_in, double T, double* out_energy,
+                                void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
