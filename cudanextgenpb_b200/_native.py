@@ -38,7 +38,8 @@ class PbgpuSellOpts(C.Structure):
 
 class PbgpuSolverOpts(C.Structure):
     _fields_ = [("method", C.c_int), ("precond", C.c_int), ("precision", C.c_int), ("tol", dbl),
-                ("max_iter", C.c_int), ("inner_tol", dbl), ("max_outer", C.c_int), ("check_every", C.c_int)]
+                ("max_iter", C.c_int), ("inner_tol", dbl), ("max_outer", C.c_int), ("check_every", C.c_int),
+                ("conv_cond", C.c_int), ("tol_w", dbl)]
 
 
 class PbgpuSolveStats(C.Structure):
@@ -70,7 +71,7 @@ class PbhostInfo(C.Structure):
 PBGPU_OK = 0
 PBGPU_ERR_ARG, PBGPU_ERR_CUDA, PBGPU_ERR_OOM, PBGPU_ERR_STATE, PBGPU_ERR_CAPACITY = 1, 2, 3, 4, 5
 PBGPU_NOT_CONVERGED, PBGPU_BREAKDOWN, PBGPU_TIMEOUT = 10, 11, 12
-PBGPU_CG, PBGPU_BICGSTAB = 0, 1
+PBGPU_CG, PBGPU_BICGSTAB, PBGPU_CGS = 0, 1, 2
 PBGPU_PRECOND_NONE, PBGPU_PRECOND_JACOBI, PBGPU_PRECOND_BLOCK_JACOBI = 0, 1, 2
 PBGPU_FP64, PBGPU_MIXED = 0, 1
 

@@ -261,6 +261,7 @@ struct SellOut {
   const int64_t* slice_ptr;
   const int32_t* slice_w;
   const int32_t* iperm;
+  const int32_t* perm;
   int32_t* scol;
   double* sval;
   double* b;
@@ -269,22 +270,23 @@ struct SellOut {
   int G;  // columns per row stored contiguously (1, 2 or 4)
 };
 
-// Element j of SELL row p: groups of G consecutive columns, lane-interleaved.
-__device__ __forceinline__ int64_t sell_index(const SellOut& S, int64_t p, int j) {
+// Element j of SELL row p (slice width W).
+__device__ __forceinline__ int64_t sell_index(const SellOut& S, int64_t p, int W, int j) {
   const int64_t sl = p / S.C;
-  const int lane = (int)(p % S.C);
-  return S.slice_ptr[sl] + (int64_t)(j / S.G) * S.G * S.C + lane * S.G + (j % S.G);
+  return sell_elem(S.slice_ptr[sl], W, S.C, S.G, (int)(p - sl * S.C), j);
 }
 
 // Pass 2: values, columns (SELL numbering), right-hand side, 1/diagonal.
+// One thread per SELL position p < n (row perm[p]), so the 32 lanes of a warp
+// fill one slice and every store of element j is one contiguous warp store.
 __global__ void k_row_fill(AsmView A, LocalView L, SellOut S) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
-  const int64_t p = S.iperm[i];
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= A.n) return;
+  const int64_t i = S.perm[p];
   const int W = S.slice_w[p / S.C];
   int j = 0;
   if (A.dirichlet[i]) {
-    const int64_t k = sell_index(S, p, j++);
+    const int64_t k = sell_index(S, p, W, j++);
     S.scol[k] = (int32_t)p;
     S.sval[k] = 1.0;
     S.b[p] = A.gval[i];
@@ -301,7 +303,7 @@ __global__ void k_row_fill(AsmView A, LocalView L, SellOut S) {
         continue;
       }
       if (cn == i) diag = R.val[u];
-      const int64_t k = sell_index(S, p, j++);
+      const int64_t k = sell_index(S, p, W, j++);
       S.scol[k] = S.iperm[cn];
       S.sval[k] = R.val[u];
     }
@@ -309,7 +311,7 @@ __global__ void k_row_fill(AsmView A, LocalView L, SellOut S) {
     S.dinv[p] = 1.0 / diag;
   }
   for (; j < W; ++j) {
-    const int64_t k = sell_index(S, p, j);
+    const int64_t k = sell_index(S, p, W, j);
     S.scol[k] = (int32_t)p;
     S.sval[k] = 0.0;
   }
@@ -321,7 +323,7 @@ __global__ void k_pad_rows(SellOut S, int64_t n, int64_t n_pad) {
   if (p >= n_pad) return;
   const int W = S.slice_w[p / S.C];
   for (int j = 0; j < W; ++j) {
-    const int64_t k = sell_index(S, p, j);
+    const int64_t k = sell_index(S, p, W, j);
     S.scol[k] = (int32_t)p;
     S.sval[k] = 0.0;
   }
@@ -394,7 +396,6 @@ __global__ void k_slice_width(const int32_t* __restrict__ perm, const int32_t* _
     const int64_t p = s * C + l;
     if (p < n) mx = max(mx, rowlen[perm[p]]);
   }
-  mx = (mx + G - 1) / G * G;
   w[s] = mx;
   elems[s] = (int64_t)mx * C;
 }
@@ -444,7 +445,7 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   }
 
   PBGPU_CUDA(c, c->rowlen.alloc(n));
-  DBuf<int> ovf;
+  Scratch<int> ovf(c, kScAsmOvf);
   PBGPU_CUDA(c, ovf.alloc(1));
   PBGPU_CUDA(c, cudaMemsetAsync(ovf.get(), 0, sizeof(int), c->stream));
   k_row_len<<<grid_for(n, 128), 128, 0, c->stream>>>(A, c->rowlen.get(), ovf.get());
@@ -459,8 +460,8 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   PBGPU_CUDA(c, c->perm.alloc(n_pad));
   PBGPU_CUDA(c, c->iperm.alloc(n_pad));
   if (sigma > 1) {
-    DBuf<uint64_t> k0, k1;
-    DBuf<int32_t> id0;
+    Scratch<uint64_t> k0(c, kScAsmK0), k1(c, kScAsmK1);
+    Scratch<int32_t> id0(c, kScAsmId0);
     PBGPU_CUDA(c, k0.alloc(n));
     PBGPU_CUDA(c, k1.alloc(n));
     PBGPU_CUDA(c, id0.alloc(n));
@@ -482,7 +483,7 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   PBGPU_LAUNCHED(c);
   PBGPU_CUDA(c, c->slice_w.alloc(n_slices));
   PBGPU_CUDA(c, c->slice_ptr.alloc(n_slices + 1));
-  DBuf<int64_t> elems;
+  Scratch<int64_t> elems(c, kScAsmElems);
   PBGPU_CUDA(c, elems.alloc(n_slices + 1));
   PBGPU_CUDA(c, cudaMemsetAsync(elems.get(), 0, (n_slices + 1) * sizeof(int64_t), c->stream));
   k_slice_width<<<grid_for(n_slices, 128), 128, 0, c->stream>>>(c->perm.get(), c->rowlen.get(), n, n_slices, C, G,
@@ -498,7 +499,7 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   PBGPU_CUDA(c, cudaMemcpyAsync(&total, c->slice_ptr.get() + n_slices, sizeof(int64_t), cudaMemcpyDeviceToHost,
                                 c->stream));
   // nnz = sum of row lengths
-  DBuf<unsigned long long> nnz_d;
+  Scratch<unsigned long long> nnz_d(c, kScAsmNnz);
   PBGPU_CUDA(c, nnz_d.alloc(1));
   PBGPU_CUDA(c, cudaMemsetAsync(nnz_d.get(), 0, sizeof(unsigned long long), c->stream));
   k_sum_rowlen<<<grid_for(n, 256), 256, 0, c->stream>>>(c->rowlen.get(), n, nnz_d.get());
@@ -513,10 +514,10 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   PBGPU_CUDA(c, c->sval.alloc(total));
   PBGPU_CUDA(c, c->b.alloc(n_pad));
   PBGPU_CUDA(c, c->dinv.alloc(n_pad));
-  SellOut S{c->slice_ptr.get(), c->slice_w.get(), c->iperm.get(), c->scol.get(), c->sval.get(), c->b.get(),
-            c->dinv.get(), C, G};
+  SellOut S{c->slice_ptr.get(), c->slice_w.get(), c->iperm.get(), c->perm.get(), c->scol.get(), c->sval.get(),
+            c->b.get(), c->dinv.get(), C, G};
   // local coefficients of every octant, once
-  DBuf<double> ocond, okd, ofr;
+  Scratch<double> ocond(c, kScAsmCond), okd(c, kScAsmKd), ofr(c, kScAsmFr);
   PBGPU_CUDA(c, ocond.alloc(12 * c->n_oct));
   PBGPU_CUDA(c, okd.alloc(8 * c->n_oct));
   PBGPU_CUDA(c, ofr.alloc(8 * c->n_oct));
@@ -531,6 +532,7 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   }
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   c->have_system = true;
+  c->bj_ready = false;
   c->have_phi = false;
   return PBGPU_OK;
 }
@@ -563,8 +565,7 @@ int export_system(Context* c, int64_t* nnz_out, int64_t* row_ptr, int32_t* col, 
     const int lane = (int)(p % C);
     row.clear();
     for (int j = 0; j < rl[i]; ++j) {
-      const int G = c->G;
-      const int64_t k = sp[s] + (int64_t)(j / G) * G * C + lane * G + (j % G);
+      const int64_t k = sell_elem(sp[s], sw[s], C, c->G, lane, j);
       row.push_back({perm[sc[k]], sv[k]});
     }
     std::sort(row.begin(), row.end());

@@ -99,7 +99,7 @@ int build_incidence(Context* c) {
   if (c->have_incidence) return PBGPU_OK;
   const int64_t n = c->n, n8 = 8 * c->n_oct;
   if (n8 >= (int64_t(1) << 32)) return c->fail(PBGPU_ERR_CAPACITY, "too many octants for 32-bit incidence entries");
-  DBuf<int32_t> cnt;
+  Scratch<int32_t> cnt(c, kScDenCnt);
   PBGPU_CUDA(c, cnt.alloc(n + 1));
   PBGPU_CUDA(c, cudaMemsetAsync(cnt.get(), 0, (n + 1) * sizeof(int32_t), c->stream));
   k_inc_count<<<grid_for(n8, 256), 256, 0, c->stream>>>(c->oct_nodes.get(), n8, n, c->hang_par.get(),
@@ -298,8 +298,8 @@ int run_density(Context* c) {
                                                               c->n_oct, g, c->tol, c->atom_oct.get());
     PBGPU_LAUNCHED(c);
     const int64_t m = 32 * na;
-    DBuf<uint64_t> k0, k1;
-    DBuf<double> v0, v1;
+    Scratch<uint64_t> k0(c, kScDenK0), k1(c, kScDenK1);
+    Scratch<double> v0(c, kScDenV0), v1(c, kScDenV1);
     PBGPU_CUDA(c, k0.alloc(m));
     PBGPU_CUDA(c, k1.alloc(m));
     PBGPU_CUDA(c, v0.alloc(m));

@@ -393,7 +393,7 @@ int run_phi_atoms(Context* c, double* out) {
   if (!c->have_phi) return c->fail(PBGPU_ERR_STATE, "phi_on_atoms: solve has not run");
   if (!c->have_density) return c->fail(PBGPU_ERR_STATE, "phi_on_atoms: create_density_map has not run");
   if (c->na == 0) return PBGPU_OK;
-  DBuf<double> d;
+  Scratch<double> d(c, kScEnPhi);
   PBGPU_CUDA(c, d.alloc(c->na));
   EnergyView E = energy_view(c, 0);
   k_phi_atoms<<<grid_for(c->na, 128), 128, 0, c->stream>>>(c->atoms.get(), c->na, c->atom_oct.get(), E, d.get());
@@ -455,7 +455,7 @@ int run_energy(Context* c, int fast, pbgpu_energy_out* out) {
     if (std::fabs(a.w) > 1.e-5) qa.push_back(a);
   }
   const int64_t m = (int64_t)qa.size();
-  DBuf<double4> dq;
+  Scratch<double4> dq(c, kScEnQ);
   PBGPU_CUDA(c, dq.alloc(m > 0 ? m : 1));
   if (m) PBGPU_CUDA(c, cudaMemcpyAsync(dq.get(), qa.data(), m * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
   const int nblk = c->sm_count * 4;
@@ -464,16 +464,16 @@ int run_energy(Context* c, int fast, pbgpu_energy_out* out) {
   if ((polar || ionic) && nb > 0) {
     const int64_t nslots = c->rays[0].nc + c->rays[1].nc + c->rays[2].nc;
     const int64_t ns = nslots > 0 ? nslots : 1;
-    DBuf<double4> acc;
-    DBuf<uint8_t> used;
-    DBuf<int32_t> slot_ray, sel;
-    DBuf<int64_t> nsel;
-    DBuf<unsigned long long> n_extra;
+    Scratch<double4> acc(c, kScEnAcc);
+    Scratch<uint8_t> used(c, kScEnUsed);
+    Scratch<int32_t> slot_ray(c, kScEnSlotRay), sel(c, kScEnSel);
+    Scratch<int64_t> nsel(c, kScEnNsel);
+    Scratch<unsigned long long> n_extra(c, kScEnNextra);
     // elements whose edge carries no crossing (an epsilon jump seen through a
     // hanging corner) keep their own point; their list starts at nb entries and
     // is grown and the pass repeated if it overflows
     int64_t extra_cap = nb + 1024;
-    DBuf<double4> xp, xd;
+    Scratch<double4> xp(c, kScEnXp), xd(c, kScEnXd);
     PBGPU_CUDA(c, acc.alloc(ns));
     PBGPU_CUDA(c, used.alloc(ns));
     PBGPU_CUDA(c, slot_ray.alloc(ns));
@@ -512,7 +512,7 @@ int run_energy(Context* c, int fast, pbgpu_energy_out* out) {
     PBGPU_CUDA(c, cudaMemcpyAsync(&np, nsel.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
     PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     const int64_t npts = np + (int64_t)nx;
-    DBuf<double4> P, D;
+    Scratch<double4> P(c, kScEnP), D(c, kScEnD);
     PBGPU_CUDA(c, P.alloc(npts > 0 ? npts : 1));
     PBGPU_CUDA(c, D.alloc(npts > 0 ? npts : 1));
     if (np) {

@@ -10,6 +10,10 @@
 //    sigma rows, which keeps padding near zero on these irregular meshes.
 //    Matrix streams are loaded with the evict-first hint (__ldcs) so the
 //    gathered vector stays resident in the 126 MB L2.
+//  * For the C = 32, G = 1 layout the SpMV instead stages each warp's slices
+//    through shared memory with bulk async copies (cp.async.bulk, mbarrier
+//    completion, double-buffered), so the matrix stream never stalls a warp
+//    and only the vector gathers remain on the critical path.
 //  * Every dot product is fused into the kernel that produces its operands;
 //    block partials are reduced by the last block to finish (ticket counter), in
 //    fixed block order, so results are deterministic and the Krylov scalars
@@ -22,15 +26,22 @@
 //    final residual are FP64.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <type_traits>
 
 #include "pbgpu_internal.cuh"
+#include "tma.cuh"
 
 namespace pbgpu {
 
 constexpr int kBlock = 256;
-// resident blocks per SM the SpMV kernels are compiled for (registers <= 65536 / (256 * 5))
+// resident blocks per SM the SpMV kernels are compiled for (registers <= 65536 / (256 * 5));
+// kernels with three or more fused reductions get 4 (64 registers, no spills)
 constexpr int kSpmvMinBlocks = 5;
+constexpr int kSpmvMinBlocksWide = 4;
 
 template <typename T>
 struct SellT {
@@ -54,25 +65,27 @@ struct V2<float> {
   using t = float2;
 };
 
-// y_p = sum_j A(p, j) x_j for SELL row p.  Element j of row p sits at
-// slice_ptr[s] + (j / G) G C + lane G + j % G, so for every G a warp's loads
-// of one column group are contiguous.
+// y_p = sum_j A(p, j) x_j for SELL row p, element j at sell_elem(): the
+// first W - W % G columns in groups of G (one vector load per group, a warp's
+// loads of one group contiguous), the remaining W % G columns one per lane.
 template <typename T, int G>
 __device__ __forceinline__ T sell_row(const SellT<T>& A, int64_t p, const T* __restrict__ x) {
   const int64_t s = p / A.C;
   const int lane = (int)(p - s * A.C);
   const int W = A.slice_w[s];
+  const int64_t sb = A.slice_ptr[s];
   T acc = 0;
   if constexpr (G == 1) {
-    const int64_t base = A.slice_ptr[s] + lane;
+    const int64_t base = sb + lane;
     const int64_t stride = A.C;
 #pragma unroll 4
     for (int j = 0; j < W; ++j) {
       const int64_t k = base + j * stride;
       acc += __ldcs(A.sval + k) * x[__ldcs(A.scol + k)];
     }
+    return acc;
   } else if constexpr (G == 2) {
-    const int64_t base = A.slice_ptr[s] + 2 * lane;
+    const int64_t base = sb + 2 * lane;
     const int64_t stride = 2 * (int64_t)A.C;
 #pragma unroll 2
     for (int g = 0; g < (W >> 1); ++g) {
@@ -83,8 +96,9 @@ __device__ __forceinline__ T sell_row(const SellT<T>& A, int64_t p, const T* __r
       acc += v.y * x[c.y];
     }
   } else {
-    const int64_t base = A.slice_ptr[s] + 4 * lane;
+    const int64_t base = sb + 4 * lane;
     const int64_t stride = 4 * (int64_t)A.C;
+#pragma unroll 2
     for (int g = 0; g < (W >> 2); ++g) {
       const int64_t k = base + g * stride;
       const int4 c = __ldcs(reinterpret_cast<const int4*>(A.scol + k));
@@ -104,7 +118,130 @@ __device__ __forceinline__ T sell_row(const SellT<T>& A, int64_t p, const T* __r
       }
     }
   }
+  // tail columns, one per lane
+  const int Wg = W - W % G;
+  const int64_t tb = sb + (int64_t)Wg * A.C + lane;
+  for (int j = Wg; j < W; ++j) {
+    const int64_t k = tb + (int64_t)(j - Wg) * A.C;
+    acc += __ldcs(A.sval + k) * x[__ldcs(A.scol + k)];
+  }
   return acc;
+}
+
+// ---------------------------------------------------------------------------
+// SpMV with the matrix staged through shared memory by bulk async copies
+// (G = 1, C = 32 layout).  Each warp owns a sequence of slices (grid stride);
+// a slice is copied in chunks of up to NC columns (values and column ids,
+// contiguous in the G = 1 layout), one chunk ahead of the one being multiplied,
+// into two per-warp buffers completed through mbarriers.  The matrix stream is
+// then fully asynchronous and each lane's x gathers (column ids read from
+// shared memory) are all independent.  Copies carry an L2 evict-first hint so
+// the gathered vector stays resident in L2.
+constexpr int kTmaWarps = kBlock / 32;
+
+template <typename T, int NC>
+__host__ __device__ constexpr size_t tma_buf_bytes() {
+  return (size_t)NC * 32 * (sizeof(T) + sizeof(int32_t));
+}
+template <typename T, int NC>
+__host__ __device__ constexpr size_t tma_smem_bytes() {
+  return (size_t)kTmaWarps * 2 * tma_buf_bytes<T, NC>() + (size_t)kTmaWarps * 2 * sizeof(uint64_t);
+}
+
+// Calls fn(row, y) for every row of every slice of this warp; false when a
+// bounded wait gave up (the warp's outstanding copies are waited for first).
+template <typename T, int NC, typename Fn>
+__device__ __forceinline__ bool spmv_tma_rows(const SellT<T>& A, const T* __restrict__ x, Fn&& fn) {
+  extern __shared__ __align__(128) unsigned char tma_smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t nwarps = (int64_t)gridDim.x * kTmaWarps;
+  const int64_t n_slices = A.n_pad / 32;
+  unsigned char* base = tma_smem + (size_t)wib * 2 * tma_buf_bytes<T, NC>();
+  // buffer b: values at base + b * buf, column ids right after them
+  auto vbuf = [&](int b) { return reinterpret_cast<T*>(base + b * tma_buf_bytes<T, NC>()); };
+  auto cbuf = [&](int b) {
+    return reinterpret_cast<int32_t*>(base + b * tma_buf_bytes<T, NC>() + (size_t)NC * 32 * sizeof(T));
+  };
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tma_smem + (size_t)kTmaWarps * 2 * tma_buf_bytes<T, NC>()) + 2 * wib;
+  if (lane == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  const uint64_t pol = l2_evict_first_policy();
+  // copy columns [jj, jj + 16) of the slice at element offset ptr (width ww) into buffer b
+  auto issue = [&](int64_t ptr, int jj, int ww, int b) {
+    if (lane == 0) {
+      const int nc = min(NC, ww - jj);
+      const int64_t off = ptr + (int64_t)jj * 32;
+      const uint32_t bv = (uint32_t)(nc * 32 * sizeof(T)), bc = (uint32_t)(nc * 32 * sizeof(int32_t));
+      mbar_arrive_expect_tx(&bars[b], nc > 0 ? bv + bc : 0u);
+      if (nc > 0) {
+        bulk_g2s(vbuf(b), A.sval + off, bv, &bars[b], pol);
+        bulk_g2s(cbuf(b), A.scol + off, bc, &bars[b], pol);
+      }
+    }
+  };
+  // current slice (s, W, P) and the warp's next slice (sn, Wn, Pn): the next
+  // slice's width and offset are loaded one slice ahead, so issuing its copy
+  // never waits on a global load
+  int64_t s = (int64_t)blockIdx.x * kTmaWarps + wib;
+  if (s >= n_slices) return true;
+  int W = A.slice_w[s];
+  int64_t P = A.slice_ptr[s];
+  int64_t sn = s + nwarps;
+  int Wn = sn < n_slices ? A.slice_w[sn] : 0;
+  int64_t Pn = sn < n_slices ? A.slice_ptr[sn] : 0;
+  int j0 = 0;
+  uint32_t phases = 0;  // bit b: parity of buffer b's next completion
+  int b = 0;
+  issue(P, 0, W, 0);
+  T acc = 0;
+  while (true) {
+    const bool more_cols = j0 + NC < W;
+    const bool next = more_cols || sn < n_slices;
+    if (more_cols)
+      issue(P, j0 + NC, W, b ^ 1);
+    else if (next)
+      issue(Pn, 0, Wn, b ^ 1);
+    // every lane observes the phase itself (acquiring the copied bytes); the
+    // vote keeps the warp together should any lane reach the limit
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bars[b], (phases >> b) & 1u))) {
+      // give up: let this warp's copies land before the block can exit
+      mbar_wait_bounded(&bars[b], (phases >> b) & 1u);
+      if (next) mbar_wait_bounded(&bars[b ^ 1], (phases >> (b ^ 1)) & 1u);
+      return false;
+    }
+    phases ^= 1u << b;
+    const int nc = min(NC, W - j0);
+    const T* vs = vbuf(b);
+    const int32_t* cs = cbuf(b);
+    // all gathers of the chunk are issued before the first use
+    T xv[NC];
+#pragma unroll
+    for (int j = 0; j < NC; ++j) xv[j] = j < nc ? x[cs[j * 32 + lane]] : (T)0;
+#pragma unroll
+    for (int j = 0; j < NC; ++j)
+      if (j < nc) acc += vs[j * 32 + lane] * xv[j];
+    __syncwarp();
+    b ^= 1;
+    if (more_cols) {
+      j0 += NC;
+      continue;
+    }
+    fn(s * 32 + lane, acc);
+    acc = 0;
+    if (!next) break;
+    s = sn;
+    W = Wn;
+    P = Pn;
+    j0 = 0;
+    sn = s + nwarps;
+    Wn = sn < n_slices ? A.slice_w[sn] : 0;
+    Pn = sn < n_slices ? A.slice_ptr[sn] : 0;
+  }
+  return true;
 }
 
 // Block-wide sum of K values; result valid in thread 0.
@@ -163,25 +300,45 @@ __device__ __forceinline__ bool grid_sum(double (&v)[K], double* partials, unsig
 
 __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 
+// Stopping rule (LIS -conv_cond): 0 / 1: ||r||_2 <= tol ||b||_2 (x0 = 0);
+// 2: ||r||_1 <= tol_w ||b||_1 + tol.
+struct ConvRule {
+  int mode;
+  double tol, tol_w;
+};
+
+__device__ __forceinline__ void set_conv(KrylovScalars* ks, const ConvRule& cr, double bb, double b1) {
+  ks->conv = cr.mode;
+  ks->bb = bb;
+  ks->b1 = b1;
+  ks->tol2 = cr.tol * cr.tol * bb;
+  ks->tol1 = cr.tol_w * b1 + cr.tol;
+}
+
+// convergence on rr = ||r||_2^2 and r1 = ||r||_1
+__device__ __forceinline__ bool conv_met(const KrylovScalars* ks, double rr, double r1) {
+  return ks->conv == 2 ? r1 <= ks->tol1 : rr <= ks->tol2;
+}
+
 // ---------------------------------------------------------------------------
 // CG (Jacobi preconditioner), templated on the storage precision.
 template <typename T>
 __global__ void k_cg_init(int64_t n, const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ x,
-                          T* __restrict__ r, T* __restrict__ p, KrylovScalars* ks, double* partials, double tol) {
-  double v[2] = {0.0, 0.0};
+                          T* __restrict__ r, T* __restrict__ p, KrylovScalars* ks, double* partials, ConvRule cr) {
+  double v[3] = {0.0, 0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const T bi = b[i];
-    const T zi = dinv[i] * bi;
+    const T zi = dinv ? dinv[i] * bi : (T)0;
     x[i] = 0;
     r[i] = bi;
     p[i] = zi;
     v[0] += (double)bi * (double)zi;
     v[1] += (double)bi * (double)bi;
+    v[2] += fabs((double)bi);
   }
-  if (grid_sum<2>(v, partials, &ks->ticket[0]) && threadIdx.x == 0) {
+  if (grid_sum<3>(v, partials, &ks->ticket[0]) && threadIdx.x == 0) {
     ks->rz = v[0];
-    ks->bb = v[1];
-    ks->tol2 = tol * tol * v[1];
+    set_conv(ks, cr, v[1], v[2]);
     ks->iter = 0;
     ks->status = PBGPU_OK;
     ks->done = (v[1] == 0.0);
@@ -193,7 +350,7 @@ __global__ void k_cg_init(int64_t n, const T* __restrict__ b, const T* __restric
 }
 
 template <typename T, int G>
-__global__ void __launch_bounds__(kBlock, kSpmvMinBlocks) k_cg_spmv(SellT<T> A, const T* __restrict__ p, T* __restrict__ q, KrylovScalars* ks, double* partials) {
+__global__ void __launch_bounds__(kBlock, G == 1 ? kSpmvMinBlocks : kSpmvMinBlocksWide) k_cg_spmv(SellT<T> A, const T* __restrict__ p, T* __restrict__ q, KrylovScalars* ks, double* partials) {
   if (ks->done) return;
   double v[1] = {0.0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x) {
@@ -216,39 +373,153 @@ __global__ void k_cg_update(int64_t n, T* __restrict__ x, T* __restrict__ r, con
                             const T* __restrict__ q, const T* __restrict__ dinv, KrylovScalars* ks, double* partials) {
   if (ks->done) return;
   const T alpha = (T)ks->alpha;
-  double v[2] = {0.0, 0.0};
+  double v[3] = {0.0, 0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     x[i] += alpha * p[i];
     const T ri = r[i] - alpha * q[i];
     r[i] = ri;
-    v[0] += (double)ri * (double)(dinv[i] * ri);
+    if (dinv) v[0] += (double)ri * (double)(dinv[i] * ri);
     v[1] += (double)ri * (double)ri;
+    v[2] += fabs((double)ri);
   }
-  if (grid_sum<2>(v, partials, &ks->ticket[2]) && threadIdx.x == 0) {
+  if (grid_sum<3>(v, partials, &ks->ticket[2]) && threadIdx.x == 0) {
     ks->iter += 1;
     ks->rr = v[1];
+    ks->r1 = v[2];
     if (!finite(v[0]) || !finite(v[1])) {
       ks->status = PBGPU_BREAKDOWN;
       ks->done = 1;
-    } else if (v[1] <= ks->tol2) {
+    } else if (conv_met(ks, v[1], v[2])) {
       ks->done = 1;
     } else if (ks->iter >= ks->max_iter) {
       ks->status = PBGPU_NOT_CONVERGED;
       ks->done = 1;
-    } else {
+    } else if (dinv) {  // block Jacobi: beta comes from k_bj_apply
       ks->beta = v[0] / ks->rz;
       ks->rz = v[0];
     }
   }
 }
 
+// p = z + beta p with z = Dinv r (Jacobi) or z given (block Jacobi)
 template <typename T>
 __global__ void k_cg_pupdate(int64_t n, T* __restrict__ p, const T* __restrict__ r, const T* __restrict__ dinv,
-                             const KrylovScalars* ks) {
+                             const T* __restrict__ z, const KrylovScalars* ks) {
   if (ks->done) return;
   const T beta = (T)ks->beta;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    p[i] = dinv[i] * r[i] + beta * p[i];
+    p[i] = (z ? z[i] : dinv[i] * r[i]) + beta * p[i];
+}
+
+// ---------------------------------------------------------------------------
+// Block-Jacobi preconditioner: M = blockdiag(A_kk) over blocks of kBjBlock
+// consecutive nodes in node (Morton) order, i.e. small spatially compact node
+// groups (2 x 2 x 2 nodes in uniform regions).  The inverse blocks are built
+// once per assembled system in FP64 and stored symmetrised in FP32 (a fixed
+// SPD operator either way, so CG's theory holds); the apply runs in the
+// vectors' precision.  Vectors live in SELL order, the blocks in node order:
+// iperm maps one to the other.
+constexpr int kBjBlock = 8;
+
+// one thread per block: gather A_kk from the SELL rows, invert (Gauss-Jordan,
+// SPD so no pivoting), write the symmetrised inverse row-major
+template <typename T, int BS>
+__global__ void k_bj_setup(SellT<double> A, int64_t n, const int32_t* __restrict__ perm,
+                           const int32_t* __restrict__ iperm, float* __restrict__ binv, int* __restrict__ bad) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t n_blk = (n + BS - 1) / BS;
+  if (k >= n_blk) return;
+  double D[BS][BS], I[BS][BS];
+#pragma unroll
+  for (int a = 0; a < BS; ++a)
+#pragma unroll
+    for (int b = 0; b < BS; ++b) {
+      D[a][b] = 0.0;
+      I[a][b] = a == b ? 1.0 : 0.0;
+    }
+  const int64_t k0 = k * BS;
+#pragma unroll
+  for (int li = 0; li < BS; ++li) {
+    const int64_t i = k0 + li;
+    if (i >= n) {
+      D[li][li] = 1.0;
+      continue;
+    }
+    const int64_t p = iperm[i];
+    const int64_t s = p / A.C;
+    const int lane = (int)(p - s * A.C);
+    const int W = A.slice_w[s];
+    for (int j = 0; j < W; ++j) {
+      const int64_t idx = sell_elem(A.slice_ptr[s], W, A.C, A.G, lane, j);
+      const int64_t node = perm[A.scol[idx]];
+      const int64_t d = node - k0;
+#pragma unroll
+      for (int b = 0; b < BS; ++b)
+        if (d == b) D[li][b] += A.sval[idx];
+    }
+  }
+  bool ok = true;
+#pragma unroll
+  for (int c = 0; c < BS; ++c) {
+    const double piv = D[c][c];
+    ok = ok && piv > 0.0 && isfinite(piv);
+    const double ip = 1.0 / piv;
+#pragma unroll
+    for (int b = 0; b < BS; ++b) {
+      D[c][b] *= ip;
+      I[c][b] *= ip;
+    }
+#pragma unroll
+    for (int a = 0; a < BS; ++a) {
+      if (a == c) continue;
+      const double f = D[a][c];
+#pragma unroll
+      for (int b = 0; b < BS; ++b) {
+        D[a][b] -= f * D[c][b];
+        I[a][b] -= f * I[c][b];
+      }
+    }
+  }
+  if (!ok) atomicExch(bad, 1);
+  float* out = binv + k * BS * BS;
+#pragma unroll
+  for (int a = 0; a < BS; ++a)
+#pragma unroll
+    for (int b = 0; b < BS; ++b) out[a * BS + b] = (float)(0.5 * (I[a][b] + I[b][a]));
+}
+
+// z = M^-1 r; with DOT also (r, z) and beta = (r, z)_new / (r, z)_old
+template <typename T, int BS, bool DOT>
+__global__ void k_bj_apply(int64_t n, const int32_t* __restrict__ iperm, const float* __restrict__ binv,
+                           const T* __restrict__ r, T* __restrict__ z, KrylovScalars* ks, double* partials) {
+  if (ks->done) return;
+  double v[1] = {0.0};
+  const int64_t n_rows = (n + BS - 1) / BS * BS;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_rows;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k0 = i - i % BS;
+    const float* row = binv + i * BS;
+    T acc = 0;
+#pragma unroll
+    for (int j = 0; j < BS; ++j)
+      if (k0 + j < n) acc += (T)row[j] * r[iperm[k0 + j]];
+    if (i < n) {
+      const int32_t pi = iperm[i];
+      z[pi] = acc;
+      if (DOT) v[0] += (double)r[pi] * (double)acc;
+    }
+  }
+  if constexpr (DOT) {
+    if (grid_sum<1>(v, partials, &ks->ticket[6]) && threadIdx.x == 0) {
+      // the first apply (iteration 0) starts the recurrence with beta = 0
+      ks->beta = ks->iter == 0 ? 0.0 : v[0] / ks->rz;
+      ks->rz = v[0];
+      if (!finite(v[0]) || (ks->iter > 0 && !finite(ks->beta))) {
+        ks->status = PBGPU_BREAKDOWN;
+        ks->done = 1;
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -256,8 +527,8 @@ __global__ void k_cg_pupdate(int64_t n, T* __restrict__ p, const T* __restrict__
 template <typename T>
 __global__ void k_bicg_init(int64_t n, const T* __restrict__ b, T* __restrict__ x, T* __restrict__ r,
                             T* __restrict__ rh, T* __restrict__ p, T* __restrict__ v, KrylovScalars* ks,
-                            double* partials, double tol) {
-  double s[1] = {0.0};
+                            double* partials, ConvRule cr) {
+  double s[2] = {0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const T bi = b[i];
     x[i] = 0;
@@ -266,10 +537,10 @@ __global__ void k_bicg_init(int64_t n, const T* __restrict__ b, T* __restrict__ 
     p[i] = 0;
     v[i] = 0;
     s[0] += (double)bi * (double)bi;
+    s[1] += fabs((double)bi);
   }
-  if (grid_sum<1>(s, partials, &ks->ticket[0]) && threadIdx.x == 0) {
-    ks->bb = s[0];
-    ks->tol2 = tol * tol * s[0];
+  if (grid_sum<2>(s, partials, &ks->ticket[0]) && threadIdx.x == 0) {
+    set_conv(ks, cr, s[0], s[1]);
     ks->rho = 1.0;
     ks->alpha = 1.0;
     ks->omega = 1.0;
@@ -295,13 +566,13 @@ __global__ void k_bicg_p(int64_t n, T* __restrict__ p, T* __restrict__ ph, const
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const T pi = r[i] + beta * (p[i] - omega * v[i]);
     p[i] = pi;
-    ph[i] = dinv[i] * pi;
+    if (dinv) ph[i] = dinv[i] * pi;
   }
 }
 
 // v = A ph;  alpha = rho_new / (rh, v)
 template <typename T, int G>
-__global__ void __launch_bounds__(kBlock, kSpmvMinBlocks) k_bicg_v(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh,
+__global__ void __launch_bounds__(kBlock, G == 1 ? kSpmvMinBlocks : kSpmvMinBlocksWide) k_bicg_v(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh,
                          KrylovScalars* ks, double* partials) {
   if (ks->done) return;
   double s[1] = {0.0};
@@ -325,22 +596,24 @@ __global__ void k_bicg_s(int64_t n, const T* __restrict__ r, const T* __restrict
                          T* __restrict__ sh, const T* __restrict__ dinv, KrylovScalars* ks, double* partials) {
   if (ks->done) return;
   const T alpha = (T)ks->alpha;
-  double a[1] = {0.0};
+  double a[2] = {0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const T si = r[i] - alpha * v[i];
     s[i] = si;
-    sh[i] = dinv[i] * si;
+    if (dinv) sh[i] = dinv[i] * si;
     a[0] += (double)si * (double)si;
+    a[1] += fabs((double)si);
   }
-  if (grid_sum<1>(a, partials, &ks->ticket[2]) && threadIdx.x == 0) {
+  if (grid_sum<2>(a, partials, &ks->ticket[2]) && threadIdx.x == 0) {
     ks->ss = a[0];
-    ks->s_conv = a[0] <= ks->tol2;
+    ks->r1 = a[1];
+    ks->s_conv = conv_met(ks, a[0], a[1]);
   }
 }
 
 // t = A sh;  omega = (t, s) / (t, t)
 template <typename T, int G>
-__global__ void __launch_bounds__(kBlock, kSpmvMinBlocks) k_bicg_t(SellT<T> A, const T* __restrict__ sh, T* __restrict__ t, const T* __restrict__ s,
+__global__ void __launch_bounds__(kBlock, kSpmvMinBlocksWide) k_bicg_t(SellT<T> A, const T* __restrict__ sh, T* __restrict__ t, const T* __restrict__ s,
                          KrylovScalars* ks, double* partials) {
   if (ks->done || ks->s_conv) return;
   double a[2] = {0.0, 0.0};
@@ -376,22 +649,24 @@ __global__ void k_bicg_x(int64_t n, T* __restrict__ x, T* __restrict__ r, const 
     return;
   }
   const T omega = (T)ks->omega;
-  double a[2] = {0.0, 0.0};
+  double a[3] = {0.0, 0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     x[i] += alpha * ph[i] + omega * sh[i];
     const T ri = s[i] - omega * t[i];
     r[i] = ri;
     a[0] += (double)ri * (double)ri;
     a[1] += (double)rh[i] * (double)ri;
+    a[2] += fabs((double)ri);
   }
-  if (grid_sum<2>(a, partials, &ks->ticket[4]) && threadIdx.x == 0) {
+  if (grid_sum<3>(a, partials, &ks->ticket[4]) && threadIdx.x == 0) {
     ks->iter += 1;
     ks->rr = a[0];
+    ks->r1 = a[2];
     const double rho_new = a[1];
     if (!finite(a[0]) || !finite(a[1])) {
       ks->status = PBGPU_BREAKDOWN;
       ks->done = 1;
-    } else if (a[0] <= ks->tol2) {
+    } else if (conv_met(ks, a[0], a[2])) {
       ks->done = 1;
     } else if (ks->iter >= ks->max_iter) {
       ks->status = PBGPU_NOT_CONVERGED;
@@ -410,19 +685,277 @@ __global__ void k_bicg_x(int64_t n, T* __restrict__ x, T* __restrict__ r, const 
 // ---------------------------------------------------------------------------
 // FP64 residual r = b - A x, its norm, and an fp32 copy (mixed precision).
 template <int G>
-__global__ void __launch_bounds__(kBlock, kSpmvMinBlocks) k_residual(SellT<double> A, int64_t n, const double* __restrict__ b, const double* __restrict__ x,
+__global__ void __launch_bounds__(kBlock, kSpmvMinBlocksWide) k_residual(SellT<double> A, int64_t n, const double* __restrict__ b, const double* __restrict__ x,
                            double* __restrict__ r, float* __restrict__ r32, KrylovScalars* ks, double* partials) {
-  double a[2] = {0.0, 0.0};
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x) {
     const double ri = i < n ? b[i] - sell_row<double, G>(A, i, x) : 0.0;
     if (r) r[i] = ri;
     if (r32) r32[i] = (float)ri;
     a[0] += ri * ri;
     a[1] += i < n ? b[i] * b[i] : 0.0;
+    a[2] += fabs(ri);
+    a[3] += i < n ? fabs(b[i]) : 0.0;
   }
-  if (grid_sum<2>(a, partials, &ks->ticket[5]) && threadIdx.x == 0) {
+  if (grid_sum<4>(a, partials, &ks->ticket[5]) && threadIdx.x == 0) {
     ks->rr = a[0];
     ks->bb = a[1];
+    ks->r1 = a[2];
+    ks->b1 = a[3];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The SpMV kernels again with the matrix staged by bulk async copies (C = 32,
+// G = 1).  A bounded wait that gives up ends the solve with PBGPU_TIMEOUT.
+constexpr int kTmaMinBlocks = 2;
+
+__device__ __forceinline__ void tma_timeout(KrylovScalars* ks) {
+  if ((threadIdx.x & 31) == 0) {
+    atomicExch(&ks->status, (int)PBGPU_TIMEOUT);
+    atomicExch(&ks->done, 1);
+  }
+}
+// Block-uniform early exit: a staged kernel that timed out sets `done` while
+// other blocks of the same launch may still be starting, so one thread reads
+// the flags for the whole block (the warps must stay complete for the votes).
+__device__ __forceinline__ bool block_skip(const KrylovScalars* ks, bool with_s_conv) {
+  __shared__ int skip;
+  if (threadIdx.x == 0) {
+    const volatile int* f = reinterpret_cast<const volatile int*>(&ks->done);
+    skip = *f != 0 || (with_s_conv && *reinterpret_cast<const volatile int*>(&ks->s_conv) != 0);
+  }
+  __syncthreads();
+  return skip != 0;
+}
+__device__ __forceinline__ bool timed_out(const KrylovScalars* ks) {
+  return *reinterpret_cast<const volatile int*>(&ks->status) == PBGPU_TIMEOUT;
+}
+
+template <typename T, int NC>
+__global__ void __launch_bounds__(kBlock, kTmaMinBlocks)
+    k_cg_spmv_tma(SellT<T> A, const T* __restrict__ p, T* __restrict__ q, KrylovScalars* ks, double* partials) {
+  if (block_skip(ks, false)) return;
+  double v[1] = {0.0};
+  if (!spmv_tma_rows<T, NC>(A, p, [&](int64_t i, T y) {
+        q[i] = y;
+        v[0] += (double)p[i] * (double)y;
+      }))
+    tma_timeout(ks);
+  if (grid_sum<1>(v, partials, &ks->ticket[1]) && threadIdx.x == 0 && !timed_out(ks)) {
+    ks->pq = v[0];
+    ks->alpha = ks->rz / v[0];
+    if (!(v[0] > 0.0) || !finite(ks->alpha)) {
+      ks->status = PBGPU_BREAKDOWN;
+      ks->done = 1;
+    }
+  }
+}
+
+template <typename T, int NC>
+__global__ void __launch_bounds__(kBlock, kTmaMinBlocks)
+    k_bicg_v_tma(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh,
+                 KrylovScalars* ks, double* partials) {
+  if (block_skip(ks, false)) return;
+  double s[1] = {0.0};
+  if (!spmv_tma_rows<T, NC>(A, ph, [&](int64_t i, T y) {
+        v[i] = y;
+        s[0] += (double)rh[i] * (double)y;
+      }))
+    tma_timeout(ks);
+  if (grid_sum<1>(s, partials, &ks->ticket[1]) && threadIdx.x == 0 && !timed_out(ks)) {
+    ks->alpha = ks->rv / s[0];
+    if (s[0] == 0.0 || !finite(ks->alpha)) {
+      ks->status = PBGPU_BREAKDOWN;
+      ks->done = 1;
+    }
+  }
+}
+
+template <typename T, int NC>
+__global__ void __launch_bounds__(kBlock, kTmaMinBlocks)
+    k_bicg_t_tma(SellT<T> A, const T* __restrict__ sh, T* __restrict__ t, const T* __restrict__ s,
+                 KrylovScalars* ks, double* partials) {
+  if (block_skip(ks, true)) return;
+  double a[2] = {0.0, 0.0};
+  if (!spmv_tma_rows<T, NC>(A, sh, [&](int64_t i, T y) {
+        t[i] = y;
+        a[0] += (double)y * (double)s[i];
+        a[1] += (double)y * (double)y;
+      }))
+    tma_timeout(ks);
+  if (grid_sum<2>(a, partials, &ks->ticket[3]) && threadIdx.x == 0 && !timed_out(ks)) {
+    ks->ts = a[0];
+    ks->tt = a[1];
+    ks->omega = a[1] > 0.0 ? a[0] / a[1] : 0.0;
+  }
+}
+
+template <int NC>
+__global__ void __launch_bounds__(kBlock, kTmaMinBlocks)
+    k_residual_tma(SellT<double> A, int64_t n, const double* __restrict__ b, const double* __restrict__ x,
+                   double* __restrict__ r, float* __restrict__ r32, KrylovScalars* ks, double* partials) {
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
+  if (!spmv_tma_rows<double, NC>(A, x, [&](int64_t i, double y) {
+        const double ri = i < n ? b[i] - y : 0.0;
+        if (r) r[i] = ri;
+        if (r32) r32[i] = (float)ri;
+        a[0] += ri * ri;
+        a[1] += i < n ? b[i] * b[i] : 0.0;
+        a[2] += fabs(ri);
+        a[3] += i < n ? fabs(b[i]) : 0.0;
+      }))
+    tma_timeout(ks);
+  if (grid_sum<4>(a, partials, &ks->ticket[5]) && threadIdx.x == 0) {
+    ks->rr = a[0];
+    ks->bb = a[1];
+    ks->r1 = a[2];
+    ks->b1 = a[3];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CGS (conjugate gradient squared, right preconditioning M), templated on the
+// storage precision; LIS's default solver in the reference's options
+// (src/pb_class.cpp:970).  Per iteration, with rho = (rh, r):
+//   u = r + beta q;  p = u + beta (q + beta p);  ph = M^-1 p;  v = A ph
+//   alpha = rho / (rh, v);  q = u - alpha v;  uh = M^-1 (u + q)
+//   x += alpha uh;  r -= alpha A uh;  beta = rho_new / rho
+// The last SpMV is fused with the x / r updates and the three reductions.
+// Buffers: u in `s`, uh in `sh`, and u + q in `v` once v is consumed.
+
+template <typename T>
+__global__ void k_cgs_init(int64_t n, const T* __restrict__ b, T* __restrict__ x, T* __restrict__ r,
+                           T* __restrict__ rh, T* __restrict__ p, T* __restrict__ q, KrylovScalars* ks,
+                           double* partials, ConvRule cr) {
+  double s[2] = {0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T bi = b[i];
+    x[i] = 0;
+    r[i] = bi;
+    rh[i] = bi;
+    p[i] = 0;
+    q[i] = 0;
+    s[0] += (double)bi * (double)bi;
+    s[1] += fabs((double)bi);
+  }
+  if (grid_sum<2>(s, partials, &ks->ticket[0]) && threadIdx.x == 0) {
+    set_conv(ks, cr, s[0], s[1]);
+    ks->rv = s[0];  // rho = (rh, r)
+    ks->beta = 0.0;
+    ks->iter = 0;
+    ks->status = PBGPU_OK;
+    ks->done = (s[0] == 0.0);
+    if (!finite(s[0])) {
+      ks->status = PBGPU_BREAKDOWN;
+      ks->done = 1;
+    }
+  }
+}
+
+// u = r + beta q;  p = u + beta (q + beta p);  ph = Dinv p (Jacobi)
+template <typename T>
+__global__ void k_cgs_p(int64_t n, const T* __restrict__ r, const T* __restrict__ q, T* __restrict__ u,
+                        T* __restrict__ p, T* __restrict__ ph, const T* __restrict__ dinv, const KrylovScalars* ks) {
+  if (ks->done) return;
+  const T beta = (T)ks->beta;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T qi = q[i];
+    const T ui = r[i] + beta * qi;
+    const T pi = ui + beta * (qi + beta * p[i]);
+    u[i] = ui;
+    p[i] = pi;
+    if (dinv) ph[i] = dinv[i] * pi;
+  }
+}
+
+// q = u - alpha v;  w = u + q;  uh = Dinv w (Jacobi), else w is left in v for
+// the block-Jacobi apply
+template <typename T>
+__global__ void k_cgs_q(int64_t n, const T* __restrict__ u, T* __restrict__ v, T* __restrict__ q,
+                        T* __restrict__ uh, const T* __restrict__ dinv, const KrylovScalars* ks) {
+  if (ks->done) return;
+  const T alpha = (T)ks->alpha;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T ui = u[i];
+    const T qi = ui - alpha * v[i];
+    q[i] = qi;
+    if (dinv)
+      uh[i] = dinv[i] * (ui + qi);
+    else
+      v[i] = ui + qi;
+  }
+}
+
+// The rows of y = A x for this kernel: staged (NC > 0) or direct.
+template <typename T, int G, int NC, typename Fn>
+__device__ __forceinline__ bool spmv_rows(const SellT<T>& A, const T* __restrict__ x, Fn&& fn) {
+  if constexpr (NC > 0) {
+    return spmv_tma_rows<T, NC>(A, x, fn);
+  } else {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x)
+      fn(i, sell_row<T, G>(A, i, x));
+    return true;
+  }
+}
+
+// v = A ph;  alpha = rho / (rh, v)
+template <typename T, int G, int NC>
+__global__ void __launch_bounds__(kBlock, NC > 0 ? kTmaMinBlocks : G == 1 ? kSpmvMinBlocks : kSpmvMinBlocksWide)
+    k_cgs_v(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh, KrylovScalars* ks,
+            double* partials) {
+  if (block_skip(ks, false)) return;
+  double a[1] = {0.0};
+  if (!spmv_rows<T, G, NC>(A, ph, [&](int64_t i, T y) {
+        v[i] = y;
+        a[0] += (double)rh[i] * (double)y;
+      }))
+    tma_timeout(ks);
+  if (grid_sum<1>(a, partials, &ks->ticket[1]) && threadIdx.x == 0 && !timed_out(ks)) {
+    ks->alpha = ks->rv / a[0];
+    if (a[0] == 0.0 || !finite(ks->alpha)) {
+      ks->status = PBGPU_BREAKDOWN;
+      ks->done = 1;
+    }
+  }
+}
+
+// r -= alpha A uh;  x += alpha uh;  (r, r), (rh, r), ||r||_1; convergence; beta
+template <typename T, int G, int NC>
+__global__ void __launch_bounds__(kBlock, NC > 0 ? kTmaMinBlocks : kSpmvMinBlocksWide)
+    k_cgs_r(SellT<T> A, const T* __restrict__ uh, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ rh,
+            KrylovScalars* ks, double* partials) {
+  if (block_skip(ks, false)) return;
+  const T alpha = (T)ks->alpha;
+  double a[3] = {0.0, 0.0, 0.0};
+  if (!spmv_rows<T, G, NC>(A, uh, [&](int64_t i, T y) {
+        x[i] += alpha * uh[i];
+        const T ri = r[i] - alpha * y;
+        r[i] = ri;
+        a[0] += (double)ri * (double)ri;
+        a[1] += (double)rh[i] * (double)ri;
+        a[2] += fabs((double)ri);
+      }))
+    tma_timeout(ks);
+  if (grid_sum<3>(a, partials, &ks->ticket[3]) && threadIdx.x == 0 && !timed_out(ks)) {
+    ks->iter += 1;
+    ks->rr = a[0];
+    ks->r1 = a[2];
+    if (!finite(a[0]) || !finite(a[1])) {
+      ks->status = PBGPU_BREAKDOWN;
+      ks->done = 1;
+    } else if (conv_met(ks, a[0], a[2])) {
+      ks->done = 1;
+    } else if (ks->iter >= ks->max_iter) {
+      ks->status = PBGPU_NOT_CONVERGED;
+      ks->done = 1;
+    } else if (a[1] == 0.0) {
+      ks->status = PBGPU_BREAKDOWN;
+      ks->done = 1;
+    } else {
+      ks->beta = a[1] / ks->rv;
+      ks->rv = a[1];
+    }
   }
 }
 
@@ -434,6 +967,12 @@ __global__ void k_axpy_f32(int64_t n, double* __restrict__ x, const float* __res
 __global__ void k_to_f32(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     b[i] = (float)a[i];
+}
+
+template <typename T>
+__global__ void k_fill(int64_t n, T* __restrict__ a, T v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = v;
 }
 
 __global__ void k_gather_phi(int64_t n, const int32_t* __restrict__ iperm, const double* __restrict__ x,
@@ -452,17 +991,62 @@ static int grid_blocks(const Context* c, int64_t n) {
   return (int)(g < 1 ? 1 : g);
 }
 
+// Chunk width (columns per bulk copy) of the staged SpMV for this context:
+// 0 when the staged path does not apply (layouts other than C = 32, G = 1) or
+// is switched off with PBGPU_SPMV=direct; PBGPU_SPMV_COLS=8|12|16 overrides
+// the context's choice.
+static int staged_cols(const Context* c, int C, int G) {
+  if (C != 32 || G != 1) return 0;
+  const char* env = std::getenv("PBGPU_SPMV");
+  if (env && std::strcmp(env, "direct") == 0) return 0;
+  int nc = c->spmv_cols;
+  if (const char* e2 = std::getenv("PBGPU_SPMV_COLS")) nc = std::atoi(e2);
+  return (nc == 8 || nc == 12 || nc == 16) ? nc : 16;
+}
+
+// Grid of the staged SpMV kernels for storage type T and chunk width NC:
+// resident blocks per SM at their dynamic shared memory; 0 if they cannot run.
+template <typename T, int NC>
+static int tma_grid(Context* c) {
+  const int smem = (int)tma_smem_bytes<T, NC>();
+  int occ = 0;
+  auto setup = [&](const void* f) -> cudaError_t {
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    int o = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, f, kBlock, smem);
+    occ = occ == 0 ? o : std::min(occ, o);
+    return e;
+  };
+  cudaError_t e = setup((const void*)k_cg_spmv_tma<T, NC>);
+  if (e == cudaSuccess) e = setup((const void*)k_bicg_v_tma<T, NC>);
+  if (e == cudaSuccess) e = setup((const void*)k_bicg_t_tma<T, NC>);
+  if (e == cudaSuccess) e = setup((const void*)k_cgs_v<T, 1, NC>);
+  if (e == cudaSuccess) e = setup((const void*)k_cgs_r<T, 1, NC>);
+  if (e == cudaSuccess && sizeof(T) == sizeof(double)) e = setup((const void*)k_residual_tma<NC>);
+  if (e != cudaSuccess || occ <= 0) {
+    cudaGetLastError();
+    return 0;  // the direct kernels serve the layout as well
+  }
+  return c->sm_count * std::min(occ, 8);
+}
+
 template <typename T>
 struct KrylovVecs {
   T *x, *r, *p, *q, *rh, *v, *s, *t, *ph, *sh;
-  const T *b, *dinv;
+  const T *b, *dinv;  // dinv: 1 / diag (Jacobi), ones (no preconditioner), null (block Jacobi)
   SellT<T> A;
+  T* z = nullptr;                   // block Jacobi: preconditioned residual (CG)
+  const float* bj = nullptr;        // block Jacobi: inverse blocks, node order
+  const int32_t* iperm = nullptr;   // node -> SELL position
+  int64_t n_nodes = 0;
 };
 
-// Run one Krylov solve on (A, b) to relative tolerance tol; x0 = 0.  GW is the
-// SELL column-group width of A.
-template <typename T, int GW>
-static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, double tol, int max_iter, int check_every,
+// Run one Krylov solve on (A, b) with stopping rule cr; x0 = 0.  GW is the
+// SELL column-group width of A; NC > 0 selects the staged SpMV with chunks of
+// NC columns (GW = 1).
+template <typename T, int GW, int NC>
+static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr, int max_iter, int check_every,
                     int* iters, int* status) {
   const int64_t n = K.A.n_pad;
   const int G = grid_blocks(c, n);
@@ -471,15 +1055,36 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, double tol, 
   PBGPU_CUDA(c, cudaMemsetAsync(ks, 0, sizeof(KrylovScalars), c->stream));
   int mi = max_iter;
   PBGPU_CUDA(c, cudaMemcpyAsync(&ks->max_iter, &mi, sizeof(int), cudaMemcpyHostToDevice, c->stream));
-  if (method == PBGPU_CG)
-    k_cg_init<T><<<G, kBlock, 0, c->stream>>>(n, K.b, K.dinv, K.x, K.r, K.p, ks, part, tol);
-  else
-    k_bicg_init<T><<<G, kBlock, 0, c->stream>>>(n, K.b, K.x, K.r, K.rh, K.p, K.v, ks, part, tol);
+  const bool bj = K.dinv == nullptr;
+  const int Gb = grid_blocks(c, (K.n_nodes + kBjBlock - 1) / kBjBlock * kBjBlock);
+  // z = M^-1 r (with (r, z) and beta when `dot`)
+  auto bj_apply = [&](const T* in, T* out, bool dot) {
+    if (dot)
+      k_bj_apply<T, kBjBlock, true><<<Gb, kBlock, 0, c->stream>>>(K.n_nodes, K.iperm, K.bj, in, out, ks, part);
+    else
+      k_bj_apply<T, kBjBlock, false><<<Gb, kBlock, 0, c->stream>>>(K.n_nodes, K.iperm, K.bj, in, out, ks, part);
+  };
+  if (method == PBGPU_CG) {
+    k_cg_init<T><<<G, kBlock, 0, c->stream>>>(n, K.b, K.dinv, K.x, K.r, K.p, ks, part, cr);
+    c->launches += 1;
+    if (bj) {  // p = z = M^-1 b
+      bj_apply(K.r, K.z, true);
+      k_cg_pupdate<T><<<G, kBlock, 0, c->stream>>>(n, K.p, K.r, K.dinv, K.z, ks);
+      c->launches += 2;
+    }
+  } else if (method == PBGPU_CGS) {
+    k_cgs_init<T><<<G, kBlock, 0, c->stream>>>(n, K.b, K.x, K.r, K.rh, K.p, K.q, ks, part, cr);
+    c->launches += 1;
+  } else {
+    k_bicg_init<T><<<G, kBlock, 0, c->stream>>>(n, K.b, K.x, K.r, K.rh, K.p, K.v, ks, part, cr);
+    c->launches += 1;
+  }
   PBGPU_CUDA(c, cudaGetLastError());
-  c->launches += 1;
   // With profiling on, events recorded around every SpMV launch become event
   // nodes of the graph; the elapsed times of the launches that did work are
   // summed after each chunk.
+  const int tg = NC > 0 ? tma_grid<T, (NC > 0 ? NC : 16)>(c) : 0;
+  const size_t smem = tma_smem_bytes<T, (NC > 0 ? NC : 16)>();
   const int spmv_per_it = method == PBGPU_CG ? 1 : 2;
   std::vector<cudaEvent_t> ev;
   if (c->profiling) {
@@ -496,21 +1101,52 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, double tol, 
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   PBGPU_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int kernels_per_chunk = 0;
   for (int k = 0; k < check_every; ++k) {
+    kernels_per_chunk += (method == PBGPU_CG ? 3 : method == PBGPU_CGS ? 4 : 5) + (bj ? (method == PBGPU_CG ? 1 : 2) : 0);
     if (method == PBGPU_CG) {
       mark(k, 0, 0);
-      k_cg_spmv<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.p, K.q, ks, part);
+      if (tg)
+        k_cg_spmv_tma<T, (NC > 0 ? NC : 16)><<<tg, kBlock, smem, c->stream>>>(K.A, K.p, K.q, ks, part);
+      else
+        k_cg_spmv<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.p, K.q, ks, part);
       mark(k, 0, 1);
       k_cg_update<T><<<G, kBlock, 0, c->stream>>>(n, K.x, K.r, K.p, K.q, K.dinv, ks, part);
-      k_cg_pupdate<T><<<G, kBlock, 0, c->stream>>>(n, K.p, K.r, K.dinv, ks);
+      if (bj) bj_apply(K.r, K.z, true);
+      k_cg_pupdate<T><<<G, kBlock, 0, c->stream>>>(n, K.p, K.r, K.dinv, K.z, ks);
+    } else if (method == PBGPU_CGS) {
+      k_cgs_p<T><<<G, kBlock, 0, c->stream>>>(n, K.r, K.q, K.s, K.p, K.ph, K.dinv, ks);
+      if (bj) bj_apply(K.p, K.ph, false);
+      mark(k, 0, 0);
+      if (tg)
+        k_cgs_v<T, 1, (NC > 0 ? NC : 16)><<<tg, kBlock, smem, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
+      else
+        k_cgs_v<T, GW, 0><<<G, kBlock, 0, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
+      mark(k, 0, 1);
+      k_cgs_q<T><<<G, kBlock, 0, c->stream>>>(n, K.s, K.v, K.q, K.sh, K.dinv, ks);
+      if (bj) bj_apply(K.v, K.sh, false);
+      mark(k, 1, 0);
+      if (tg)
+        k_cgs_r<T, 1, (NC > 0 ? NC : 16)><<<tg, kBlock, smem, c->stream>>>(K.A, K.sh, K.x, K.r, K.rh, ks, part);
+      else
+        k_cgs_r<T, GW, 0><<<G, kBlock, 0, c->stream>>>(K.A, K.sh, K.x, K.r, K.rh, ks, part);
+      mark(k, 1, 1);
     } else {
       k_bicg_p<T><<<G, kBlock, 0, c->stream>>>(n, K.p, K.ph, K.r, K.v, K.dinv, ks);
+      if (bj) bj_apply(K.p, K.ph, false);
       mark(k, 0, 0);
-      k_bicg_v<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
+      if (tg)
+        k_bicg_v_tma<T, (NC > 0 ? NC : 16)><<<tg, kBlock, smem, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
+      else
+        k_bicg_v<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
       mark(k, 0, 1);
       k_bicg_s<T><<<G, kBlock, 0, c->stream>>>(n, K.r, K.v, K.s, K.sh, K.dinv, ks, part);
+      if (bj) bj_apply(K.s, K.sh, false);
       mark(k, 1, 0);
-      k_bicg_t<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.sh, K.t, K.s, ks, part);
+      if (tg)
+        k_bicg_t_tma<T, (NC > 0 ? NC : 16)><<<tg, kBlock, smem, c->stream>>>(K.A, K.sh, K.t, K.s, ks, part);
+      else
+        k_bicg_t<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.sh, K.t, K.s, ks, part);
       mark(k, 1, 1);
       k_bicg_x<T><<<G, kBlock, 0, c->stream>>>(n, K.x, K.r, K.ph, K.sh, K.s, K.t, K.rh, ks, part);
     }
@@ -526,7 +1162,6 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, double tol, 
     for (cudaEvent_t e : ev) cudaEventDestroy(e);
     return cuda_fail(c, ce, "cudaGraphInstantiate");
   }
-  const int kernels_per_chunk = (method == PBGPU_CG ? 3 : 5) * check_every;
   int rc = PBGPU_OK;
   const int max_chunks = max_iter / check_every + 2;
   int prev_iter = 0;
@@ -580,18 +1215,38 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, double tol, 
 }
 
 template <typename T>
-static int krylov(Context* c, int method, const KrylovVecs<T>& K, double tol, int max_iter, int check_every,
+static int krylov(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr, int max_iter, int check_every,
                   int* iters, int* status) {
+  switch (staged_cols(c, K.A.C, K.A.G)) {
+    case 8: return krylov_g<T, 1, 8>(c, method, K, cr, max_iter, check_every, iters, status);
+    case 12: return krylov_g<T, 1, 12>(c, method, K, cr, max_iter, check_every, iters, status);
+    case 16: return krylov_g<T, 1, 16>(c, method, K, cr, max_iter, check_every, iters, status);
+    default: break;
+  }
   switch (K.A.G) {
-    case 1: return krylov_g<T, 1>(c, method, K, tol, max_iter, check_every, iters, status);
-    case 2: return krylov_g<T, 2>(c, method, K, tol, max_iter, check_every, iters, status);
-    default: return krylov_g<T, 4>(c, method, K, tol, max_iter, check_every, iters, status);
+    case 1: return krylov_g<T, 1, 0>(c, method, K, cr, max_iter, check_every, iters, status);
+    case 2: return krylov_g<T, 2, 0>(c, method, K, cr, max_iter, check_every, iters, status);
+    default: return krylov_g<T, 4, 0>(c, method, K, cr, max_iter, check_every, iters, status);
   }
 }
 
 // r = b - A x (fp64); optional fp64 / fp32 copies of r; norms into ks
 static void launch_residual(Context* c, const SellT<double>& A, int64_t n, double* r, float* r32) {
   const int g = grid_blocks(c, A.n_pad);
+  auto staged = [&](auto nc_tag) -> bool {
+    constexpr int NC = decltype(nc_tag)::value;
+    const int tg = tma_grid<double, NC>(c);
+    if (!tg) return false;
+    k_residual_tma<NC><<<tg, kBlock, tma_smem_bytes<double, NC>(), c->stream>>>(A, n, c->b.get(), c->x.get(), r,
+                                                                              r32, c->ks.get(), c->partials.get());
+    return true;
+  };
+  switch (staged_cols(c, A.C, A.G)) {
+    case 8: if (staged(std::integral_constant<int, 8>{})) return; break;
+    case 12: if (staged(std::integral_constant<int, 12>{})) return; break;
+    case 16: if (staged(std::integral_constant<int, 16>{})) return; break;
+    default: break;
+  }
   switch (A.G) {
     case 1: k_residual<1><<<g, kBlock, 0, c->stream>>>(A, n, c->b.get(), c->x.get(), r, r32, c->ks.get(), c->partials.get()); break;
     case 2: k_residual<2><<<g, kBlock, 0, c->stream>>>(A, n, c->b.get(), c->x.get(), r, r32, c->ks.get(), c->partials.get()); break;
@@ -614,6 +1269,26 @@ static cudaError_t alloc_vectors(Context* c, int64_t n_pad, bool mixed) {
   return c->ks.alloc(1);
 }
 
+// Builds the block-Jacobi inverse blocks of the current system (once per
+// assembly); PBGPU_BREAKDOWN when a diagonal block is not positive definite.
+static int build_block_jacobi(Context* c, const SellT<double>& A) {
+  if (c->bj_ready) return PBGPU_OK;
+  const int64_t n_blk = (c->n + kBjBlock - 1) / kBjBlock;
+  PBGPU_CUDA(c, c->bjinv.alloc((size_t)n_blk * kBjBlock * kBjBlock));
+  int* bad = reinterpret_cast<int*>(&c->ks_host->status);  // scratch flag in pinned memory
+  Scratch<int> dbad(c, kScKrBad);
+  PBGPU_CUDA(c, dbad.alloc(1));
+  PBGPU_CUDA(c, cudaMemsetAsync(dbad.get(), 0, sizeof(int), c->stream));
+  k_bj_setup<double, kBjBlock><<<grid_for(n_blk, 128), 128, 0, c->stream>>>(A, c->n, c->perm.get(), c->iperm.get(),
+                                                                            c->bjinv.get(), dbad.get());
+  PBGPU_LAUNCHED(c);
+  PBGPU_CUDA(c, cudaMemcpyAsync(bad, dbad.get(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (*bad) return c->fail(PBGPU_BREAKDOWN, "solve: a block-Jacobi diagonal block is not positive definite");
+  c->bj_ready = true;
+  return PBGPU_OK;
+}
+
 int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
   if (!c->have_system) return c->fail(PBGPU_ERR_STATE, "solve: assemble has not run");
   pbgpu_solver_opts opt;
@@ -621,7 +1296,14 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
     opt = *o;
   else
     pbgpu_default_solver_opts(&opt);
-  if (opt.method != PBGPU_CG && opt.method != PBGPU_BICGSTAB) return c->fail(PBGPU_ERR_ARG, "solve: unknown method");
+  if (opt.method != PBGPU_CG && opt.method != PBGPU_BICGSTAB && opt.method != PBGPU_CGS)
+    return c->fail(PBGPU_ERR_ARG, "solve: unknown method");
+  if (opt.conv_cond < 0 || opt.conv_cond > 2 || !(opt.tol_w >= 0))
+    return c->fail(PBGPU_ERR_ARG, "solve: conv_cond must be 0, 1 or 2 and tol_w non-negative");
+  const ConvRule rule{opt.conv_cond, opt.tol, opt.tol_w};
+  if (opt.precond != PBGPU_PRECOND_NONE && opt.precond != PBGPU_PRECOND_JACOBI &&
+      opt.precond != PBGPU_PRECOND_BLOCK_JACOBI)
+    return c->fail(PBGPU_ERR_ARG, "solve: unknown preconditioner");
   if (!(opt.tol > 0) || opt.max_iter <= 0) return c->fail(PBGPU_ERR_ARG, "solve: tol and max_iter must be positive");
   if (opt.check_every <= 0) opt.check_every = 16;
   const bool mixed = opt.precision == PBGPU_MIXED;
@@ -630,11 +1312,34 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
   PBGPU_CUDA(c, cudaEventRecord(c->ev0, c->stream));
   int iters = 0, status = PBGPU_OK, outer = 0;
   SellT<double> A64{c->slice_ptr.get(), c->slice_w.get(), c->scol.get(), c->sval.get(), n_pad, c->C, c->G};
+  const bool bj = opt.precond == PBGPU_PRECOND_BLOCK_JACOBI;
+  if (bj) {
+    const int rc = build_block_jacobi(c, A64);
+    if (rc != PBGPU_OK) return rc;
+  }
+  const double* diag64 = c->dinv.get();
+  if (opt.precond == PBGPU_PRECOND_NONE) {
+    PBGPU_CUDA(c, c->ones.alloc(n_pad));
+    k_fill<double><<<grid_blocks(c, n_pad), kBlock, 0, c->stream>>>(n_pad, c->ones.get(), 1.0);
+    PBGPU_LAUNCHED(c);
+    diag64 = c->ones.get();
+  } else if (bj) {
+    diag64 = nullptr;
+  }
   if (!mixed) {
     KrylovVecs<double> K{c->x.get(), c->r.get(), c->p.get(), c->q.get(), c->rh.get(), c->v.get(), c->s.get(),
-                         c->t.get(), c->ph.get(), c->sh.get(), c->b.get(), c->dinv.get(), A64};
-    int rc = krylov<double>(c, opt.method, K, opt.tol, opt.max_iter, opt.check_every, &iters, &status);
+                         c->t.get(), c->ph.get(), c->sh.get(), c->b.get(), diag64, A64};
+    if (bj) {
+      PBGPU_CUDA(c, c->z.alloc(n_pad));
+      PBGPU_CUDA(c, cudaMemsetAsync(c->z.get(), 0, n_pad * sizeof(double), c->stream));
+      K.z = c->z.get();
+      K.bj = c->bjinv.get();
+      K.iperm = c->iperm.get();
+      K.n_nodes = n;
+    }
+    int rc = krylov<double>(c, opt.method, K, rule, opt.max_iter, opt.check_every, &iters, &status);
     if (rc != PBGPU_OK) return rc;
+    if (status == PBGPU_TIMEOUT) return c->fail(PBGPU_TIMEOUT, "solve: SpMV copy wait timed out");
   } else {
     // FP32 copies of the matrix values and of 1/diag
     const int G = grid_blocks(c, c->sell_len);
@@ -647,10 +1352,28 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
     const int max_outer = opt.max_outer > 0 ? opt.max_outer : 50;
     const double inner = opt.inner_tol > 0 ? opt.inner_tol : 1e-5;
     // the fp32 inner solve keeps its own x (the correction d), r, p, q
+    const float* diag32 = c->dinv32.get();
+    if (opt.precond == PBGPU_PRECOND_NONE) {
+      PBGPU_CUDA(c, c->ones32.alloc(n_pad));
+      k_fill<float><<<grid_blocks(c, n_pad), kBlock, 0, c->stream>>>(n_pad, c->ones32.get(), 1.0f);
+      PBGPU_LAUNCHED(c);
+      diag32 = c->ones32.get();
+    } else if (bj) {
+      diag32 = nullptr;
+    }
     KrylovVecs<float> K{c->x32.get(), c->r32.get(), c->p32.get(), c->q32.get(), nullptr, nullptr, nullptr,
-                        nullptr, nullptr, nullptr, c->b32.get(), c->dinv32.get(), A32};
-    DBuf<float> rh32, v32, s32, t32, ph32, sh32;
-    if (opt.method == PBGPU_BICGSTAB) {
+                        nullptr, nullptr, nullptr, c->b32.get(), diag32, A32};
+    if (bj) {
+      PBGPU_CUDA(c, c->z32.alloc(n_pad));
+      PBGPU_CUDA(c, cudaMemsetAsync(c->z32.get(), 0, n_pad * sizeof(float), c->stream));
+      K.z = c->z32.get();
+      K.bj = c->bjinv.get();
+      K.iperm = c->iperm.get();
+      K.n_nodes = n;
+    }
+    Scratch<float> rh32(c, kScKrRh32), v32(c, kScKrV32), s32(c, kScKrS32), t32(c, kScKrT32),
+        ph32(c, kScKrPh32), sh32(c, kScKrSh32);
+    if (opt.method != PBGPU_CG) {
       PBGPU_CUDA(c, rh32.alloc(n_pad));
       PBGPU_CUDA(c, v32.alloc(n_pad));
       PBGPU_CUDA(c, s32.alloc(n_pad));
@@ -671,21 +1394,27 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
       PBGPU_LAUNCHED(c);
       PBGPU_CUDA(c, cudaMemcpyAsync(c->ks_host, c->ks.get(), sizeof(KrylovScalars), cudaMemcpyDeviceToHost, c->stream));
       PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+      if (c->ks_host->status == PBGPU_TIMEOUT) return c->fail(PBGPU_TIMEOUT, "solve: SpMV copy wait timed out");
       const double rr = c->ks_host->rr, bb = c->ks_host->bb;
       if (!std::isfinite(rr)) {
         status = PBGPU_BREAKDOWN;
         break;
       }
-      if (rr <= opt.tol * opt.tol * bb) {
+      const bool met = rule.mode == 2 ? c->ks_host->r1 <= rule.tol_w * c->ks_host->b1 + rule.tol
+                                      : rr <= opt.tol * opt.tol * bb;
+      if (met) {
         status = PBGPU_OK;
         break;
       }
-      // inner tolerance: reduce the residual by `inner`, never below what fp32 can resolve
+      // inner tolerance: reduce the residual by `inner`, never below what fp32 can resolve;
+      // an inner solve that stagnates in fp32 (CGS, BiCGStab) is cut off and its
+      // correction used all the same, the fp64 residual decides
       int it = 0, ist = 0;
-      const int left = opt.max_iter - iters;
+      const int left = std::min(opt.max_iter - iters, std::max(256, opt.max_iter / 8));
       if (left <= 0) break;
-      int rc = krylov<float>(c, opt.method, K, inner, left, opt.check_every, &it, &ist);
+      int rc = krylov<float>(c, opt.method, K, ConvRule{0, inner, 1.0}, left, opt.check_every, &it, &ist);
       if (rc != PBGPU_OK) return rc;
+      if (ist == PBGPU_TIMEOUT) return c->fail(PBGPU_TIMEOUT, "solve: SpMV copy wait timed out");
       iters += it;
       if (ist == PBGPU_BREAKDOWN && it == 0) {
         status = PBGPU_BREAKDOWN;
@@ -706,6 +1435,7 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   float ms = 0;
   PBGPU_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  if (c->ks_host->status == PBGPU_TIMEOUT) return c->fail(PBGPU_TIMEOUT, "solve: SpMV copy wait timed out");
   const double rel = c->ks_host->bb > 0 ? std::sqrt(c->ks_host->rr / c->ks_host->bb) : 0.0;
   if (st) {
     st->status = status;

@@ -46,7 +46,7 @@ int build_ray_hash_from(Context* c, int axis, const uint64_t* d_keys) {
   PBGPU_CUDA(c, R.hkeys.alloc(R.cap));
   PBGPU_CUDA(c, R.hval.alloc(R.cap));
   PBGPU_CUDA(c, cudaMemsetAsync(R.hkeys.get(), 0xff, R.cap * sizeof(uint64_t), c->stream));
-  DBuf<int> ovf;
+  Scratch<int> ovf(c, kScMkOvf);
   PBGPU_CUDA(c, ovf.alloc(1));
   PBGPU_CUDA(c, cudaMemsetAsync(ovf.get(), 0, sizeof(int), c->stream));
   k_hash_insert<<<grid_for(R.n, 256), 256, 0, c->stream>>>(d_keys, R.n, R.hkeys.get(), R.hval.get(), R.cap, R.cap_log,
@@ -174,15 +174,15 @@ int run_markers(Context* c) {
       c->node_xyz.get(), n, ray_view(c->rays[2]), c->lo[2], c->len[2], c->eps_in, c->eps_out, react_out, stern,
       c->model.stern_layer, c->inside.get(), c->eps.get(), c->react.get());
   PBGPU_LAUNCHED(c);
-  DBuf<uint8_t> flags;
+  Scratch<uint8_t> flags(c, kScMkFlags);
   PBGPU_CUDA(c, flags.alloc(no));
   k_octant_markers<<<grid_for(no, 256), 256, 0, c->stream>>>(c->oct_nodes.get(), no, n, c->inside.get(), stern,
                                                               react_out, c->marker.get(), flags.get(),
                                                               stern ? c->react_cell.get() : nullptr);
   PBGPU_LAUNCHED(c);
   // border list in ascending octant order
-  DBuf<int32_t> sel;
-  DBuf<int64_t> nsel;
+  Scratch<int32_t> sel(c, kScMkSel);
+  Scratch<int64_t> nsel(c, kScMkNsel);
   PBGPU_CUDA(c, sel.alloc(no));
   PBGPU_CUDA(c, nsel.alloc(1));
   cub::CountingInputIterator<int32_t> idx(0);

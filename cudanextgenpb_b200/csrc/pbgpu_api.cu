@@ -133,6 +133,75 @@ const char* pbgpu_last_error(const pbgpu_ctx* h) { return h ? h->c.err.c_str() :
 
 void* pbgpu_ctx_stream(const pbgpu_ctx* h) { return h ? static_cast<void*>(h->c.stream) : nullptr; }
 
+// ---- input packing and checks on the device (the host only copies)
+enum { kErrLevel, kErrNodeId, kErrNodeXyz, kErrHangNp, kErrHangPar, kErrRayPtr, kErrRayKey, kNumInputErr };
+
+__global__ void k_pack_octants(int64_t no, const int32_t* __restrict__ xyz, const int8_t* __restrict__ lvl,
+                               int4* __restrict__ oct, int* __restrict__ err) {
+  const int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (o >= no) return;
+  const int lv = lvl[o];
+  if (lv < 0 || lv > 18) err[kErrLevel] = 1;
+  oct[o] = make_int4(xyz[3 * o], xyz[3 * o + 1], xyz[3 * o + 2], lv);
+}
+
+__global__ void k_check_ids(int64_t m, const int32_t* __restrict__ ids, int64_t lim, int* __restrict__ err) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < m && (ids[t] < 0 || ids[t] >= lim)) err[kErrNodeId] = 1;
+}
+
+__global__ void k_pack_nodes(int64_t n, const int32_t* __restrict__ xyz, int4* __restrict__ nodes,
+                             int* __restrict__ err) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int p[3], flag = 0;
+  for (int a = 0; a < 3; ++a) {
+    p[a] = xyz[3 * i + a];
+    if (p[a] < 0 || p[a] > kRoot) err[kErrNodeXyz] = 1;
+    if (p[a] == 0 || p[a] == kRoot) flag = 1;
+  }
+  nodes[i] = make_int4(p[0], p[1], p[2], flag);
+}
+
+__global__ void k_pack_hanging(int64_t nh, const int8_t* __restrict__ np_in, const int32_t* __restrict__ par_in,
+                               int64_t n, int4* __restrict__ par, int8_t* __restrict__ np_out,
+                               int* __restrict__ err) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= nh) return;
+  const int np = np_in[j];
+  if (np != 2 && np != 4) err[kErrHangNp] = 1;
+  int32_t q[4];
+  for (int k = 0; k < 4; ++k) {
+    q[k] = k < np ? par_in[4 * j + k] : par_in[4 * j];
+    if (q[k] < 0 || q[k] >= n) err[kErrHangPar] = 1;
+  }
+  par[j] = make_int4(q[0], q[1], q[2], q[3]);
+  np_out[j] = (int8_t)np;
+}
+
+__global__ void k_check_rays(int64_t nr, const uint64_t* __restrict__ keys, const int64_t* __restrict__ ptr,
+                             int* __restrict__ err) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= nr) return;
+  if (ptr[j + 1] < ptr[j]) err[kErrRayPtr] = 1;
+  if (j && keys[j] <= keys[j - 1]) err[kErrRayKey] = 1;
+}
+
+static const char* kInputErrMsg[kNumInputErr] = {
+    "set_mesh: octant level out of range", "set_mesh: bad node id", "set_mesh: node coordinate out of range",
+    "set_mesh: hanging node needs 2 or 4 parents", "set_mesh: hanging parent is not an independent node",
+    "set_rays: ptr not ascending", "set_rays: keys not strictly ascending"};
+
+// Waits for the stream and reports the first input check that failed.
+static int input_errors(Context* c, const int* d_err) {
+  int h[kNumInputErr];
+  PBGPU_CUDA(c, cudaMemcpyAsync(h, d_err, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < kNumInputErr; ++k)
+    if (h[k]) return c->fail(PBGPU_ERR_ARG, kInputErrMsg[k]);
+  return PBGPU_OK;
+}
+
 int pbgpu_set_mesh(pbgpu_ctx* h, const pbgpu_mesh* m) {
   CTX_CHECK(h);
   Context* c = &h->c;
@@ -144,35 +213,10 @@ int pbgpu_set_mesh(pbgpu_ctx* h, const pbgpu_mesh* m) {
     if (!(m->hi[a] > m->lo[a])) return c->fail(PBGPU_ERR_ARG, "set_mesh: empty domain box");
   SET_DEVICE(c);
   const int64_t no = m->n_oct, n = m->n_nodes, nh = m->n_hang;
-  // validate node ids and pack octants / nodes as int4
-  std::vector<int4> oct(no), nodes(n), hp(nh > 0 ? nh : 1);
-  for (int64_t o = 0; o < no; ++o) {
-    const int lv = m->oct_level[o];
-    if (lv < 0 || lv > 18) return c->fail(PBGPU_ERR_ARG, "set_mesh: octant level out of range");
-    oct[o] = make_int4(m->oct_xyz[3 * o], m->oct_xyz[3 * o + 1], m->oct_xyz[3 * o + 2], lv);
-  }
-  for (int64_t t = 0; t < 8 * no; ++t)
-    if (m->oct_nodes[t] < 0 || m->oct_nodes[t] >= n + nh) return c->fail(PBGPU_ERR_ARG, "set_mesh: bad node id");
-  for (int64_t i = 0; i < n; ++i) {
-    const int32_t* p = m->node_xyz + 3 * i;
-    int flag = 0;
-    for (int a = 0; a < 3; ++a) {
-      if (p[a] < 0 || p[a] > kRoot) return c->fail(PBGPU_ERR_ARG, "set_mesh: node coordinate out of range");
-      if (p[a] == 0 || p[a] == kRoot) flag = 1;
-    }
-    nodes[i] = make_int4(p[0], p[1], p[2], flag);
-  }
-  for (int64_t j = 0; j < nh; ++j) {
-    const int np = m->hang_np[j];
-    if (np != 2 && np != 4) return c->fail(PBGPU_ERR_ARG, "set_mesh: hanging node needs 2 or 4 parents");
-    int32_t par[4];
-    for (int k = 0; k < 4; ++k) {
-      par[k] = k < np ? m->hang_par[4 * j + k] : m->hang_par[4 * j];
-      if (par[k] < 0 || par[k] >= n) return c->fail(PBGPU_ERR_ARG, "set_mesh: hanging parent is not an independent node");
-    }
-    hp[j] = make_int4(par[0], par[1], par[2], par[3]);
-  }
+  // the host copies the caller's arrays as they are; packing to int4 and the
+  // range checks run on the device, and the mesh is dropped if a check fails
   invalidate_from_mesh(c);
+  c->have_mesh = false;
   c->n_oct = no;
   c->n = n;
   c->nh = nh;
@@ -181,18 +225,46 @@ int pbgpu_set_mesh(pbgpu_ctx* h, const pbgpu_mesh* m) {
     c->len[a] = m->hi[a] - m->lo[a];
   }
   c->tol = m->locate_tol;
-  int st;
-  if ((st = upload(c, c->oct, oct.data(), no)) != PBGPU_OK) return st;
-  if ((st = upload(c, c->oct_nodes, m->oct_nodes, 8 * no)) != PBGPU_OK) return st;
-  if ((st = upload(c, c->node_xyz, nodes.data(), n)) != PBGPU_OK) return st;
-  if ((st = upload(c, c->hang_par, hp.data(), nh > 0 ? nh : 1)) != PBGPU_OK) return st;
-  std::vector<int8_t> np(nh > 0 ? nh : 1, 2);
-  if (nh) std::memcpy(np.data(), m->hang_np, nh);
-  if ((st = upload(c, c->hang_np, np.data(), np.size())) != PBGPU_OK) return st;
+  Scratch<int32_t> oxyz(c, kScInOctXyz), nxyz(c, kScInNodeXyz), hpar(c, kScInHangPar);
+  Scratch<int8_t> olvl(c, kScInOctLvl), hnp(c, kScInHangNp);
+  Scratch<int> err(c, kScInErr);
+  PBGPU_CUDA(c, err.alloc(kNumInputErr));
+  PBGPU_CUDA(c, cudaMemsetAsync(err.get(), 0, kNumInputErr * sizeof(int), c->stream));
+  PBGPU_CUDA(c, oxyz.alloc(3 * no));
+  PBGPU_CUDA(c, olvl.alloc(no));
+  PBGPU_CUDA(c, nxyz.alloc(3 * n));
+  PBGPU_CUDA(c, c->oct.alloc(no));
+  PBGPU_CUDA(c, c->oct_nodes.alloc(8 * no));
+  PBGPU_CUDA(c, c->node_xyz.alloc(n));
+  PBGPU_CUDA(c, c->hang_par.alloc(nh > 0 ? nh : 1));
+  PBGPU_CUDA(c, c->hang_np.alloc(nh > 0 ? nh : 1));
+  auto h2d = [&](void* d, const void* src, size_t bytes) {
+    return cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, c->stream);
+  };
+  PBGPU_CUDA(c, h2d(oxyz.get(), m->oct_xyz, 3 * no * sizeof(int32_t)));
+  PBGPU_CUDA(c, h2d(olvl.get(), m->oct_level, no));
+  PBGPU_CUDA(c, h2d(c->oct_nodes.get(), m->oct_nodes, 8 * no * sizeof(int32_t)));
+  PBGPU_CUDA(c, h2d(nxyz.get(), m->node_xyz, 3 * n * sizeof(int32_t)));
+  k_pack_octants<<<grid_for(no, 256), 256, 0, c->stream>>>(no, oxyz.get(), olvl.get(), c->oct.get(), err.get());
+  PBGPU_LAUNCHED(c);
+  k_check_ids<<<grid_for(8 * no, 256), 256, 0, c->stream>>>(8 * no, c->oct_nodes.get(), n + nh, err.get());
+  PBGPU_LAUNCHED(c);
+  k_pack_nodes<<<grid_for(n, 256), 256, 0, c->stream>>>(n, nxyz.get(), c->node_xyz.get(), err.get());
+  PBGPU_LAUNCHED(c);
+  if (nh > 0) {
+    PBGPU_CUDA(c, hpar.alloc(4 * nh));
+    PBGPU_CUDA(c, hnp.alloc(nh));
+    PBGPU_CUDA(c, h2d(hpar.get(), m->hang_par, 4 * nh * sizeof(int32_t)));
+    PBGPU_CUDA(c, h2d(hnp.get(), m->hang_np, nh));
+    k_pack_hanging<<<grid_for(nh, 256), 256, 0, c->stream>>>(nh, hnp.get(), hpar.get(), n, c->hang_par.get(),
+                                                             c->hang_np.get(), err.get());
+    PBGPU_LAUNCHED(c);
+  }
   PBGPU_CUDA(c, c->oct_key.alloc(no));
   launch_oct_keys(c->oct.get(), no, c->oct_key.get(), c->stream);
   PBGPU_LAUNCHED(c);
-  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int st = input_errors(c, err.get());
+  if (st != PBGPU_OK) return st;
   c->have_mesh = true;
   return PBGPU_OK;
 }
@@ -207,14 +279,9 @@ int pbgpu_set_rays(pbgpu_ctx* h, int axis, const pbgpu_rays* r) {
   SET_DEVICE(c);
   const int64_t nr = r->n_rays;
   const int64_t nc = nr > 0 ? r->ptr[nr] : 0;
-  if (nr > 0) {
-    if (r->ptr[0] != 0) return c->fail(PBGPU_ERR_ARG, "set_rays: ptr[0] must be 0");
-    for (int64_t j = 0; j < nr; ++j) {
-      if (r->ptr[j + 1] < r->ptr[j]) return c->fail(PBGPU_ERR_ARG, "set_rays: ptr not ascending");
-      if (j && r->keys[j] <= r->keys[j - 1]) return c->fail(PBGPU_ERR_ARG, "set_rays: keys not strictly ascending");
-    }
-  }
+  if (nr > 0 && (r->ptr[0] != 0 || nc < 0)) return c->fail(PBGPU_ERR_ARG, "set_rays: ptr[0] must be 0");
   Rays& R = c->rays[axis];
+  c->have_rays[axis] = false;
   R.n = nr;
   int st;
   if ((st = upload(c, R.ptr, r->ptr, nr + 1)) != PBGPU_OK) return st;
@@ -222,6 +289,15 @@ int pbgpu_set_rays(pbgpu_ctx* h, int axis, const pbgpu_rays* r) {
   if ((st = upload(c, R.normals, r->normals, 3 * nc)) != PBGPU_OK) return st;
   R.nc = nc;
   if ((st = upload(c, R.keys, r->keys, nr)) != PBGPU_OK) return st;
+  if (nr > 0) {
+    // ascending offsets and strictly ascending keys, checked on the device
+    Scratch<int> err(c, kScInErr);
+    PBGPU_CUDA(c, err.alloc(kNumInputErr));
+    PBGPU_CUDA(c, cudaMemsetAsync(err.get(), 0, kNumInputErr * sizeof(int), c->stream));
+    k_check_rays<<<grid_for(nr, 256), 256, 0, c->stream>>>(nr, R.keys.get(), R.ptr.get(), err.get());
+    PBGPU_LAUNCHED(c);
+    if ((st = input_errors(c, err.get())) != PBGPU_OK) return st;
+  }
   if ((st = build_ray_hash_from(c, axis, R.keys.get())) != PBGPU_OK) return st;
   c->have_rays[axis] = true;
   c->have_markers = c->have_system = c->have_phi = false;
@@ -332,6 +408,8 @@ void pbgpu_default_solver_opts(pbgpu_solver_opts* o) {
   o->inner_tol = 1e-5;
   o->max_outer = 50;
   o->check_every = 16;
+  o->conv_cond = 0;
+  o->tol_w = 1.0;
 }
 
 int pbgpu_parse_lis_options(const char* options, pbgpu_solver_opts* out) {
@@ -349,8 +427,10 @@ int pbgpu_parse_lis_options(const char* options, pbgpu_solver_opts* out) {
       const std::string v = tok[++i];
       if (v == "cg" || v == "1" || v == "cr" || v == "5")
         out->method = PBGPU_CG;
+      else if (v == "cgs" || v == "3")
+        out->method = PBGPU_CGS;
       else
-        out->method = PBGPU_BICGSTAB;  // bicg, cgs, bicgstab, bicgsafe, gmres, ...
+        out->method = PBGPU_BICGSTAB;  // bicg, bicgstab, bicgsafe, gmres, ...
     } else if ((k == "-p" || k == "-precon") && has) {
       const std::string v = tok[++i];
       if (v == "none" || v == "0")
@@ -363,6 +443,14 @@ int pbgpu_parse_lis_options(const char* options, pbgpu_solver_opts* out) {
       const double t = std::strtod(tok[++i].c_str(), nullptr);
       if (!(t > 0)) return PBGPU_ERR_ARG;
       out->tol = t;
+    } else if (k == "-conv_cond" && has) {
+      const long m = std::strtol(tok[++i].c_str(), nullptr, 10);
+      if (m < 0 || m > 2) return PBGPU_ERR_ARG;
+      out->conv_cond = (int)m;
+    } else if (k == "-tol_w" && has) {
+      const double t = std::strtod(tok[++i].c_str(), nullptr);
+      if (!(t >= 0)) return PBGPU_ERR_ARG;
+      out->tol_w = t;
     } else if (k == "-maxiter" && has) {
       const long m = std::strtol(tok[++i].c_str(), nullptr, 10);
       if (m <= 0) return PBGPU_ERR_ARG;

@@ -63,8 +63,50 @@ struct Rays {
 struct KrylovScalars {
   double rz, rz_new, pq, alpha, beta, omega, rho, rr, bb, ss, ts, tt, rv;
   double tol2;            // tol^2 * ||b||^2
+  double r1, b1, tol1;    // ||r||_1, ||b||_1, tol_w ||b||_1 + tol (LIS conv_cond 2)
+  int conv;               // 2: stop on the 1-norm rule, else on the 2-norm rule
   int iter, max_iter, done, status, s_conv;
   unsigned int ticket[8]; // last-block tickets, one per reducing kernel
+};
+
+// Element j of the SELL row in lane `lane` of a slice that starts at element
+// `base` and has width W (columns), height C and column-group width G: the
+// first W - W % G columns are stored in groups of G lane-interleaved (a
+// thread loads a group with one vector load, a warp's loads of one group are
+// contiguous), the last W % G columns one per lane, so slice widths need no
+// padding to a multiple of G.
+__host__ __device__ __forceinline__ int64_t sell_elem(int64_t base, int W, int C, int G, int lane, int j) {
+  const int Wg = W - W % G;
+  if (j < Wg) return base + (int64_t)(j / G) * G * C + (int64_t)lane * G + j % G;
+  return base + (int64_t)Wg * C + (int64_t)(j - Wg) * C + lane;
+}
+
+// Scratch slots of a context: one per stage-local buffer.
+enum ScratchSlot {
+  kScMkOvf, kScMkFlags, kScMkSel, kScMkNsel,
+  kScDenCnt, kScDenK0, kScDenK1, kScDenV0, kScDenV1,
+  kScAsmOvf, kScAsmK0, kScAsmK1, kScAsmId0, kScAsmElems, kScAsmNnz, kScAsmCond, kScAsmKd, kScAsmFr,
+  kScKrBad, kScKrRh32, kScKrV32, kScKrS32, kScKrT32, kScKrPh32, kScKrSh32,
+  kScEnPhi, kScEnQ, kScEnAcc, kScEnUsed, kScEnSlotRay, kScEnSel, kScEnNsel, kScEnNextra, kScEnXp, kScEnXd,
+  kScEnP, kScEnD,
+  kScInOctXyz, kScInOctLvl, kScInNodeXyz, kScInHangNp, kScInHangPar, kScInErr,
+  kScratchSlots
+};
+
+struct Context;
+
+// A typed view of one scratch slot with DBuf's alloc() / get() interface.
+template <typename T>
+struct Scratch {
+  DBuf<uint8_t>* slot;
+  T* p = nullptr;
+  Scratch(Context* c, int which);
+  cudaError_t alloc(size_t count) {
+    const cudaError_t e = slot->alloc(count * sizeof(T) > 0 ? count * sizeof(T) : 1);
+    p = reinterpret_cast<T*>(slot->get());
+    return e;
+  }
+  T* get() const { return p; }
 };
 
 struct Context {
@@ -122,6 +164,7 @@ struct Context {
 
   // ---- system in SELL-C-sigma (rows permuted; vectors live in SELL order)
   int C = 32, sigma = 2048, G = 1;
+  int spmv_cols = 16;        // staged SpMV chunk width (8, 12 or 16 columns)
   int64_t n_slices = 0, nnz = 0, sell_len = 0;
   DBuf<int64_t> slice_ptr;   // element offset of each slice
   DBuf<int32_t> slice_w;     // width (multiple of 4) of each slice
@@ -139,7 +182,11 @@ struct Context {
 
   // ---- solve
   DBuf<double> x, r, p, q, z, rh, v, s, t, ph, sh;   // fp64 work vectors (SELL order)
-  DBuf<float> x32, r32, p32, q32, b32, dinv32;       // fp32 inner vectors
+  DBuf<float> x32, r32, p32, q32, b32, dinv32, z32; // fp32 inner vectors
+  DBuf<double> ones;         // the "no preconditioner" diagonal
+  DBuf<float> ones32;
+  DBuf<float> bjinv;         // block-Jacobi inverse blocks (node order)
+  bool bj_ready = false;     // bjinv belongs to the current system
   DBuf<double> partials;     // block partial sums
   DBuf<KrylovScalars> ks;
   KrylovScalars* ks_host = nullptr;   // pinned mirror
@@ -156,6 +203,11 @@ struct Context {
   // ---- scratch for CUB
   DBuf<uint8_t> tmp;
 
+  // ---- per-stage scratch, kept between calls (grow-only) so a repeated
+  // stage neither allocates nor frees device memory (cudaFree synchronises
+  // the device and large cudaMalloc calls take milliseconds)
+  DBuf<uint8_t> scratch[kScratchSlots];
+
   // ---- measurement
   bool profiling = false;
   int64_t launches = 0;       // kernels launched (CUB device algorithms count their kernels)
@@ -171,6 +223,9 @@ struct Context {
     return code;
   }
 };
+
+template <typename T>
+Scratch<T>::Scratch(Context* c, int which) : slot(&c->scratch[which]) {}
 
 int cuda_fail(Context* c, cudaError_t e, const char* what);
 

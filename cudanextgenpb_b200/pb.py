@@ -144,12 +144,15 @@ class Problem:
 
 
 def solver_opts(method="cg", tol=1e-8, max_iter=20000, precision="fp64", inner_tol=1e-5, check_every=16,
-                max_outer=50) -> N.PbgpuSolverOpts:
+                max_outer=50, precond="jacobi", conv_cond=0, tol_w=1.0) -> N.PbgpuSolverOpts:
     o = N.PbgpuSolverOpts()
     N.load_gpu().pbgpu_default_solver_opts(C.byref(o))
-    o.method = {"cg": N.PBGPU_CG, "bicgstab": N.PBGPU_BICGSTAB}[method]
+    o.method = {"cg": N.PBGPU_CG, "bicgstab": N.PBGPU_BICGSTAB, "cgs": N.PBGPU_CGS}[method]
+    o.precond = {"none": N.PBGPU_PRECOND_NONE, "jacobi": N.PBGPU_PRECOND_JACOBI,
+                 "block_jacobi": N.PBGPU_PRECOND_BLOCK_JACOBI}[precond]
     o.precision = {"fp64": N.PBGPU_FP64, "mixed": N.PBGPU_MIXED}[precision]
     o.tol, o.max_iter, o.inner_tol, o.check_every, o.max_outer = tol, max_iter, inner_tol, check_every, max_outer
+    o.conv_cond, o.tol_w = conv_cond, tol_w
     return o
 
 

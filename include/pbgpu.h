@@ -52,7 +52,7 @@ enum {
   PBGPU_TIMEOUT = 12          /* a bounded device-side wait gave up */
 };
 
-enum { PBGPU_CG = 0, PBGPU_BICGSTAB = 1 };
+enum { PBGPU_CG = 0, PBGPU_BICGSTAB = 1, PBGPU_CGS = 2 };
 enum { PBGPU_PRECOND_NONE = 0, PBGPU_PRECOND_JACOBI = 1, PBGPU_PRECOND_BLOCK_JACOBI = 2 };
 enum { PBGPU_FP64 = 0, PBGPU_MIXED = 1 };
 
@@ -105,14 +105,17 @@ typedef struct {
 } pbgpu_sell_opts;
 
 typedef struct {
-  int method;                /* PBGPU_CG or PBGPU_BICGSTAB */
+  int method;                /* PBGPU_CG, PBGPU_BICGSTAB or PBGPU_CGS */
   int precond;               /* PBGPU_PRECOND_* */
   int precision;             /* PBGPU_FP64 or PBGPU_MIXED */
-  double tol;                /* stop when ||b - A x||_2 <= tol * ||b||_2 */
+  double tol;                /* stopping tolerance, see conv_cond */
   int max_iter;              /* inner iteration cap */
   double inner_tol;          /* PBGPU_MIXED: residual reduction per fp32 inner solve */
   int max_outer;             /* PBGPU_MIXED: refinement steps cap */
   int check_every;           /* iterations between host polls of the device convergence flag */
+  int conv_cond;             /* LIS -conv_cond: 0 or 1 stop when ||r||_2 <= tol ||b||_2 (x0 = 0, so
+                                r0 = b); 2 stop when ||r||_1 <= tol_w ||b||_1 + tol */
+  double tol_w;              /* LIS -tol_w (conv_cond 2) */
 } pbgpu_solver_opts;
 
 typedef struct {

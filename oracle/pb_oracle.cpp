@@ -688,14 +688,106 @@ static std::vector<double> jacobi_inverse(const oracle_state* s) {
   return d;
 }
 
+// The preconditioners of lis_compute_electric_potential's "-p" option as the
+// GPU path defines them: none, Jacobi (1 / diag), and block Jacobi over blocks
+// of 8 consecutive nodes (node order), each inverted in FP64 by Gauss-Jordan
+// elimination and stored symmetrised in FP32.
+struct Precond {
+  static constexpr int kBlock = 8;
+  int kind = PBGPU_PRECOND_JACOBI;
+  int64_t n = 0;
+  std::vector<double> di;
+  std::vector<float> bj;
+
+  Precond(const oracle_state* s, int k) : kind(k), n(s->n) {
+    if (kind == PBGPU_PRECOND_NONE) {
+      di.assign(n, 1.0);
+    } else if (kind == PBGPU_PRECOND_JACOBI) {
+      di = jacobi_inverse(s);
+    } else {
+      const int64_t nb = (n + kBlock - 1) / kBlock;
+      bj.assign(nb * kBlock * kBlock, 0.f);
+      for (int64_t k0 = 0; k0 < nb * kBlock; k0 += kBlock) {
+        double D[kBlock][kBlock] = {}, I[kBlock][kBlock] = {};
+        for (int a = 0; a < kBlock; ++a) {
+          I[a][a] = 1.0;
+          const int64_t r = k0 + a;
+          if (r >= n) {
+            D[a][a] = 1.0;
+            continue;
+          }
+          for (int64_t q = s->row_ptr[r]; q < s->row_ptr[r + 1]; ++q) {
+            const int64_t d = s->col[q] - k0;
+            if (d >= 0 && d < kBlock) D[a][d] += s->val[q];
+          }
+        }
+        for (int c = 0; c < kBlock; ++c) {
+          const double ip = 1.0 / D[c][c];
+          for (int b = 0; b < kBlock; ++b) {
+            D[c][b] *= ip;
+            I[c][b] *= ip;
+          }
+          for (int a = 0; a < kBlock; ++a) {
+            if (a == c) continue;
+            const double f = D[a][c];
+            for (int b = 0; b < kBlock; ++b) {
+              D[a][b] -= f * D[c][b];
+              I[a][b] -= f * I[c][b];
+            }
+          }
+        }
+        for (int a = 0; a < kBlock; ++a)
+          for (int b = 0; b < kBlock; ++b) bj[(k0 + a) * kBlock + b] = (float)(0.5 * (I[a][b] + I[b][a]));
+      }
+    }
+  }
+
+  // out = M^-1 in
+  void apply(const double* in, double* out) const {
+    if (kind != PBGPU_PRECOND_BLOCK_JACOBI) {
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < n; ++i) out[i] = di[i] * in[i];
+      return;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+      const int64_t k0 = i - i % kBlock;
+      double acc = 0.0;
+      for (int j = 0; j < kBlock && k0 + j < n; ++j) acc += (double)bj[i * kBlock + j] * in[k0 + j];
+      out[i] = acc;
+    }
+  }
+};
+
+static double norm1(const double* a, int64_t n) {
+  double t = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : t)
+  for (int64_t i = 0; i < n; ++i) t += std::fabs(a[i]);
+  return t;
+}
+
 int oracle_solve(oracle_state* s, int method, double tol, int max_iter, int threads, double* rel_residual) {
+  return oracle_solve_ex(s, method, PBGPU_PRECOND_JACOBI, 0, tol, 1.0, max_iter, threads, rel_residual);
+}
+
+int oracle_solve_ex(oracle_state* s, int method, int precond, int conv_cond, double tol, double tol_w, int max_iter,
+                    int threads, double* rel_residual) {
   if (!s->have_system) return -PBGPU_ERR_STATE;
+  if (precond != PBGPU_PRECOND_NONE && precond != PBGPU_PRECOND_JACOBI && precond != PBGPU_PRECOND_BLOCK_JACOBI)
+    return -PBGPU_ERR_ARG;
+  if (method != PBGPU_CG && method != PBGPU_BICGSTAB && method != PBGPU_CGS) return -PBGPU_ERR_ARG;
+  if (conv_cond < 0 || conv_cond > 2) return -PBGPU_ERR_ARG;
   const int prev = omp_get_max_threads();
   if (threads > 0) omp_set_num_threads(threads);
   const int64_t n = s->n;
-  const std::vector<double> Di = jacobi_inverse(s);
+  const Precond M(s, precond);
   std::vector<double> x(n, 0.0), r(s->rhs), z(n), p(n), q(n);
   const double bnorm = std::sqrt(dot(s->rhs.data(), s->rhs.data(), n));
+  // LIS conv_cond: 0 / 1 ||r||_2 <= tol ||b||_2 (x0 = 0); 2 ||r||_1 <= tol_w ||b||_1 + tol
+  const double lim1 = tol_w * norm1(s->rhs.data(), n) + tol;
+  auto converged = [&](const std::vector<double>& res, double rr) {
+    return conv_cond == 2 ? norm1(res.data(), n) <= lim1 : std::sqrt(rr) <= tol * bnorm;
+  };
   int it = 0;
   if (bnorm == 0.0) {
     s->phi = x;
@@ -705,8 +797,8 @@ int oracle_solve(oracle_state* s, int method, double tol, int max_iter, int thre
     return 0;
   }
   if (method == PBGPU_CG) {
-#pragma omp parallel for
-    for (int64_t i = 0; i < n; ++i) p[i] = z[i] = Di[i] * r[i];
+    M.apply(r.data(), z.data());
+    p = z;
     double rz = dot(r.data(), z.data(), n);
     for (it = 1; it <= max_iter; ++it) {
       spmv(s, p.data(), q.data());
@@ -718,19 +810,15 @@ int oracle_solve(oracle_state* s, int method, double tol, int max_iter, int thre
         r[i] -= alpha * q[i];
         rr += r[i] * r[i];
       }
-      if (std::sqrt(rr) <= tol * bnorm) break;
-      double rzn = 0.0;
-#pragma omp parallel for reduction(+ : rzn)
-      for (int64_t i = 0; i < n; ++i) {
-        z[i] = Di[i] * r[i];
-        rzn += r[i] * z[i];
-      }
+      if (converged(r, rr)) break;
+      M.apply(r.data(), z.data());
+      const double rzn = dot(r.data(), z.data(), n);
       const double beta = rzn / rz;
       rz = rzn;
 #pragma omp parallel for
       for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
     }
-  } else {
+  } else if (method == PBGPU_BICGSTAB) {
     std::vector<double> rh(r), v(n, 0.0), ph(n), sv(n), sh(n), t(n);
     std::fill(p.begin(), p.end(), 0.0);
     double rho = 1.0, alpha = 1.0, omega = 1.0;
@@ -739,10 +827,8 @@ int oracle_solve(oracle_state* s, int method, double tol, int max_iter, int thre
       if (rho_n == 0.0 || !std::isfinite(rho_n)) break;
       const double beta = (rho_n / rho) * (alpha / omega);
 #pragma omp parallel for
-      for (int64_t i = 0; i < n; ++i) {
-        p[i] = r[i] + beta * (p[i] - omega * v[i]);
-        ph[i] = Di[i] * p[i];
-      }
+      for (int64_t i = 0; i < n; ++i) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+      M.apply(p.data(), ph.data());
       spmv(s, ph.data(), v.data());
       alpha = rho_n / dot(rh.data(), v.data(), n);
       double ss = 0.0;
@@ -751,13 +837,12 @@ int oracle_solve(oracle_state* s, int method, double tol, int max_iter, int thre
         sv[i] = r[i] - alpha * v[i];
         ss += sv[i] * sv[i];
       }
-      if (std::sqrt(ss) <= tol * bnorm) {
+      if (converged(sv, ss)) {
 #pragma omp parallel for
         for (int64_t i = 0; i < n; ++i) x[i] += alpha * ph[i];
         break;
       }
-#pragma omp parallel for
-      for (int64_t i = 0; i < n; ++i) sh[i] = Di[i] * sv[i];
+      M.apply(sv.data(), sh.data());
       spmv(s, sh.data(), t.data());
       double ts = 0.0, tt = 0.0;
 #pragma omp parallel for reduction(+ : ts, tt)
@@ -774,8 +859,44 @@ int oracle_solve(oracle_state* s, int method, double tol, int max_iter, int thre
         rr += r[i] * r[i];
       }
       rho = rho_n;
-      if (std::sqrt(rr) <= tol * bnorm) break;
+      if (converged(r, rr)) break;
       if (omega == 0.0) break;
+    }
+  } else {
+    // CGS with right preconditioning (the GPU path's k_cgs_* sequence)
+    std::vector<double> rh(r), u(n), qc(n, 0.0), v(n), ph(n), w(n), uh(n), t(n);
+    std::fill(p.begin(), p.end(), 0.0);
+    double rho = dot(rh.data(), r.data(), n), beta = 0.0;
+    for (it = 1; it <= max_iter; ++it) {
+#pragma omp parallel for
+      for (int64_t i = 0; i < n; ++i) {
+        u[i] = r[i] + beta * qc[i];
+        p[i] = u[i] + beta * (qc[i] + beta * p[i]);
+      }
+      M.apply(p.data(), ph.data());
+      spmv(s, ph.data(), v.data());
+      const double sigma = dot(rh.data(), v.data(), n);
+      if (sigma == 0.0 || !std::isfinite(sigma)) break;
+      const double alpha = rho / sigma;
+#pragma omp parallel for
+      for (int64_t i = 0; i < n; ++i) {
+        qc[i] = u[i] - alpha * v[i];
+        w[i] = u[i] + qc[i];
+      }
+      M.apply(w.data(), uh.data());
+      spmv(s, uh.data(), t.data());
+      double rr = 0.0;
+#pragma omp parallel for reduction(+ : rr)
+      for (int64_t i = 0; i < n; ++i) {
+        x[i] += alpha * uh[i];
+        r[i] -= alpha * t[i];
+        rr += r[i] * r[i];
+      }
+      if (converged(r, rr)) break;
+      const double rho_n = dot(rh.data(), r.data(), n);
+      if (rho_n == 0.0 || !std::isfinite(rho_n)) break;
+      beta = rho_n / rho;
+      rho = rho_n;
     }
   }
   // true residual

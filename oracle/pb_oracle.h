@@ -14,7 +14,8 @@
  *                      it calls are restated from their use in this file, see
  *                      pb_oracle.cpp), BCs :3531-3571
  *   Krylov solve       lis_compute_electric_potential :2244-2329 (CG and
- *                      BiCGStab with Jacobi), solved tight as MUMPS stand-in
+ *                      BiCGStab with none / Jacobi / block-Jacobi
+ *                      preconditioning), solved tight as MUMPS stand-in
  *   potential at atoms write_potential_on_atoms_fast :2333-2417
  *   energy             energy :2791-3063, energy_fast :3066-3338
  *
@@ -51,6 +52,12 @@ int oracle_assemble_mode(oracle_state* s, int rows);
  * ||b - A x||_2 <= tol ||b||_2 (recursive residual, checked against the true
  * residual at exit).  threads <= 0: all cores.  Returns iterations (<0 error). */
 int oracle_solve(oracle_state* s, int method, double tol, int max_iter, int threads, double* rel_residual);
+/* the same for method PBGPU_CG / _BICGSTAB / _CGS, preconditioner
+ * PBGPU_PRECOND_NONE / _JACOBI / _BLOCK_JACOBI (blocks of 8 consecutive nodes,
+ * inverses stored symmetrised in FP32) and LIS's conv_cond: 0 or 1 stop on
+ * ||r||_2 <= tol ||b||_2, 2 on ||r||_1 <= tol_w ||b||_1 + tol */
+int oracle_solve_ex(oracle_state* s, int method, int precond, int conv_cond, double tol, double tol_w, int max_iter,
+                    int threads, double* rel_residual);
 int oracle_phi_on_atoms(oracle_state* s, double* out);
 int oracle_energy(oracle_state* s, int fast, pbgpu_energy_out* out);
 

@@ -33,6 +33,8 @@ def load():
             getattr(L, f).argtypes = [sp]
         L.oracle_assemble_mode.argtypes = [sp, C.c_int]
         L.oracle_solve.argtypes = [sp, C.c_int, C.c_double, C.c_int, C.c_int, P(C.c_double)]
+        L.oracle_solve_ex.argtypes = [sp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
+                                      P(C.c_double)]
         L.oracle_phi_on_atoms.argtypes = [sp, P(C.c_double)]
         L.oracle_energy.argtypes = [sp, C.c_int, P(N.PbgpuEnergyOut)]
         L.oracle_get_node_coeffs.argtypes = [sp, P(C.c_double), P(C.c_double)]
@@ -136,9 +138,12 @@ class Oracle:
         self._ok(self.L.oracle_set_system(self.s, self.n, rp.ctypes.data_as(P(C.c_int64)),
                                           col.ctypes.data_as(P(C.c_int32)), _d(val), _d(rhs)))
 
-    def solve(self, method="cg", tol=1e-12, max_iter=100000, threads=0):
+    def solve(self, method="cg", tol=1e-12, max_iter=100000, threads=0, precond="jacobi", conv_cond=0, tol_w=1.0):
         rel = C.c_double()
-        it = self.L.oracle_solve(self.s, 0 if method == "cg" else 1, tol, max_iter, threads, C.byref(rel))
+        pc = {"none": N.PBGPU_PRECOND_NONE, "jacobi": N.PBGPU_PRECOND_JACOBI,
+              "block_jacobi": N.PBGPU_PRECOND_BLOCK_JACOBI}[precond]
+        m = {"cg": N.PBGPU_CG, "bicgstab": N.PBGPU_BICGSTAB, "cgs": N.PBGPU_CGS}[method]
+        it = self.L.oracle_solve_ex(self.s, m, pc, conv_cond, tol, tol_w, max_iter, threads, C.byref(rel))
         if it < 0:
             raise RuntimeError("oracle_solve failed")
         phi = np.zeros(self.n)

@@ -34,8 +34,14 @@ def test_bindings_cover_header():
 def test_parse_lis_options():
     o = parse_lis_options("-i bicgstab -p jacobi -tol 1.e-8")
     assert (o.method, o.precond, o.tol) == (N.PBGPU_BICGSTAB, N.PBGPU_PRECOND_JACOBI, 1e-8)
+    # the reference's default solver_options (src/pb_class.cpp:970)
     o = parse_lis_options("-p ssor -ssor_omega 0.51 -i cgs -tol 1.e-6 -print 2 -conv_cond 2 -tol_w 0")
-    assert (o.method, o.precond, o.tol) == (N.PBGPU_BICGSTAB, N.PBGPU_PRECOND_BLOCK_JACOBI, 1e-6)
+    assert (o.method, o.precond, o.tol) == (N.PBGPU_CGS, N.PBGPU_PRECOND_BLOCK_JACOBI, 1e-6)
+    assert (o.conv_cond, o.tol_w) == (2, 0.0)
+    o = parse_lis_options("-i bicgstab")
+    assert (o.conv_cond, o.tol_w) == (0, 1.0)
+    with pytest.raises(Exception):
+        parse_lis_options("-conv_cond 3")
     o = parse_lis_options("-i cg -p jacobi -tol 1e-10 -maxiter 77")
     assert (o.method, o.max_iter, o.tol) == (N.PBGPU_CG, 77, 1e-10)
     with pytest.raises(Exception):

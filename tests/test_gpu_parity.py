@@ -152,6 +152,131 @@ def test_sell_layouts_agree(chunk, sigma, group):
     assert np.linalg.norm(g.phi() - ophi) / np.linalg.norm(ophi) < 1e-6
 
 
+@pytest.mark.parametrize("method,precision,cols", [("cg", "fp64", 16), ("bicgstab", "fp64", 16),
+                                                   ("cg", "mixed", 16), ("cg", "fp64", 8), ("bicgstab", "fp64", 12),
+                                                   ("cg", "mixed", 8)])
+def test_staged_and_direct_spmv_agree(monkeypatch, method, precision, cols):
+    """The C = 32, G = 1 layout runs the SpMV staged through shared memory by
+    bulk copies; PBGPU_SPMV=direct selects the per-row kernel on the same
+    matrix.  Both solve to the same potential within the solve tolerance (the
+    order of the dot product partial sums differs, so iterates differ in the
+    last bits)."""
+    prob = CASES["mol150"]().build()
+    g = GpuPath().load(prob)
+    g.create_markers()
+    g.create_density_map()
+    g.assemble(32, 2048, 1)
+    opts = solver_opts(method, tol=1e-10, precision=precision)
+    res = {}
+    for mode in ("staged", "direct"):
+        if mode == "direct":
+            monkeypatch.setenv("PBGPU_SPMV", "direct")
+        else:
+            monkeypatch.delenv("PBGPU_SPMV", raising=False)
+            monkeypatch.setenv("PBGPU_SPMV_COLS", str(cols))
+        st = g.solve(opts)
+        assert st.status == 0 and st.rel_residual <= 1e-10
+        res[mode] = (g.phi().copy(), st.iterations)
+    (pa, ia), (pb, ib) = res["staged"], res["direct"]
+    assert np.linalg.norm(pa - pb) / np.linalg.norm(pb) < 1e-7
+    # BiCGStab's iteration count is sensitive to the rounding of its scalars
+    assert abs(ia - ib) <= max(2, ib // (20 if method == "cg" else 4)), (ia, ib)
+    g.close()
+
+
+@pytest.mark.parametrize("case_name,method,precond,precision", [
+    ("born", "cg", "none", "fp64"), ("born", "bicgstab", "none", "fp64"),
+    ("mol150", "cg", "block_jacobi", "fp64"), ("mol150", "bicgstab", "block_jacobi", "fp64"),
+    ("mol150", "cg", "block_jacobi", "mixed"), ("born", "bicgstab", "block_jacobi", "fp64")])
+def test_preconditioners(case_name, method, precond, precision):
+    """The "-p none" and block-Jacobi preconditioners against the oracle's own
+    (same block partition, same FP32-stored inverse blocks): the iteration
+    counts agree up to rounding-order effects and the potential matches a tight
+    oracle solve."""
+    prob = CASES[case_name]().build()
+    o = Oracle(prob)
+    o.markers()
+    o.density()
+    o.assemble()
+    g = GpuPath().load(prob)
+    g.create_markers()
+    g.create_density_map()
+    g.assemble()
+    st = g.solve(solver_opts(method, tol=1e-8, precond=precond, precision=precision))
+    assert st.status == 0 and st.rel_residual <= 1e-8
+    if precision == "fp64":
+        _, oit, _ = o.solve(method, 1e-8, precond=precond)
+        # BiCGStab's iteration count is sensitive to the rounding of its scalars
+        assert abs(st.iterations - oit) <= max(2, oit // (25 if method == "cg" else 8)), (st.iterations, oit)
+    ophi, _, _ = o.solve("cg", 1e-12)
+    assert np.linalg.norm(g.phi() - ophi) / np.linalg.norm(ophi) < 1e-6
+    g.close()
+
+
+@pytest.mark.parametrize("case_name,precond,precision", [
+    ("born", "jacobi", "fp64"), ("mol150", "jacobi", "fp64"), ("mol150", "block_jacobi", "fp64"),
+    ("mol150", "jacobi", "mixed"), ("born", "none", "fp64")])
+def test_cgs_matches_oracle(case_name, precond, precision):
+    """CGS (LIS -i cgs) against the oracle's CGS with the same preconditioner."""
+    prob = CASES[case_name]().build()
+    o = Oracle(prob)
+    o.markers()
+    o.density()
+    o.assemble()
+    g = GpuPath().load(prob)
+    g.create_markers()
+    g.create_density_map()
+    g.assemble()
+    st = g.solve(solver_opts("cgs", tol=1e-9, precond=precond, precision=precision))
+    # CGS stops on its recursive residual, which drifts from the true one
+    assert st.status == 0 and st.rel_residual <= 1e-8
+    if precision == "fp64":
+        _, oit, orel = o.solve("cgs", 1e-9, precond=precond)
+        assert orel <= 1e-9
+        assert abs(st.iterations - oit) <= max(3, oit // 10), (st.iterations, oit)
+    ophi, _, _ = o.solve("cg", 1e-12)
+    assert np.linalg.norm(g.phi() - ophi) / np.linalg.norm(ophi) < 1e-6
+    g.close()
+
+
+def test_reference_default_solver_options():
+    """The reference's default solver_options string (src/pb_class.cpp:970):
+    CGS, "-p ssor" served by block Jacobi, and conv_cond 2 (||r||_1 <= tol_w
+    ||b||_1 + tol with tol_w = 0, tol = 1e-6)."""
+    from cudanextgenpb_b200 import parse_lis_options
+    opts = parse_lis_options("-p ssor -ssor_omega 0.51 -i cgs -tol 1.e-6 -print 2 -conv_cond 2 -tol_w 0")
+    prob = CASES["mol150"]().build()
+    o = Oracle(prob)
+    o.markers()
+    o.density()
+    o.assemble()
+    g = GpuPath().load(prob)
+    g.create_markers()
+    g.create_density_map()
+    g.assemble()
+    st = g.solve(opts)
+    assert st.status == 0
+    _, oit, _ = o.solve("cgs", 1e-6, precond="block_jacobi", conv_cond=2, tol_w=0.0)
+    assert abs(st.iterations - oit) <= max(3, oit // 10), (st.iterations, oit)
+    # the 1-norm rule was met: ||b - A phi||_1 <= 1e-6 (recomputed on the host)
+    rp, col, val, rhs = g.system()
+    import scipy.sparse as sp
+    A = sp.csr_matrix((val, col, rp), shape=(len(rp) - 1,) * 2)
+    assert np.abs(rhs - A @ g.phi()).sum() <= 2e-6
+    g.close()
+
+
+def test_block_jacobi_fewer_iterations_than_jacobi():
+    prob = CASES["mol150"]().build()
+    g = GpuPath().load(prob)
+    g.create_markers()
+    g.create_density_map()
+    g.assemble()
+    its = {pc: g.solve(solver_opts("cg", tol=1e-8, precond=pc)).iterations for pc in ("jacobi", "block_jacobi")}
+    assert its["block_jacobi"] < 0.9 * its["jacobi"], its
+    g.close()
+
+
 @pytest.mark.parametrize("bc", [0, 1, 2])
 def test_boundary_condition_types(bc):
     prob = configs.make_born_problem(4, 5, bc_type=bc).build()
@@ -234,3 +359,61 @@ def test_host_driver_path_matches():
     opts = prob.solver_opts()
     e, st2 = g.run(opts)
     assert e_host["sum"] == pytest.approx(e["sum"], rel=1e-9)
+
+
+def _mesh_from(d):
+    """A pbgpu_mesh over the numpy arrays of Problem.mesh() (kept alive by d)."""
+    import ctypes as C
+    P = C.POINTER
+    m = N.PbgpuMesh()
+    m.n_oct, m.n_nodes, m.n_hang = len(d["oct_level"]), len(d["node_xyz"]), len(d["hang_np"])
+    for k, t in (("oct_xyz", C.c_int32), ("oct_level", C.c_int8), ("oct_nodes", C.c_int32),
+                 ("node_xyz", C.c_int32), ("hang_np", C.c_int8), ("hang_par", C.c_int32)):
+        d[k] = np.ascontiguousarray(d[k])
+        setattr(m, k, d[k].ctypes.data_as(P(t)))
+    for a in range(3):
+        m.lo[a], m.hi[a] = d["lo"][a], d["hi"][a]
+    m.locate_tol = d["locate_tol"]
+    return m
+
+
+@pytest.mark.parametrize("field,index,value,msg", [
+    ("oct_level", 5, 19, "octant level"), ("oct_nodes", (7, 3), -1, "bad node id"),
+    ("node_xyz", (11, 2), (1 << 19) + 1, "node coordinate"), ("hang_np", 0, 3, "2 or 4 parents"),
+    ("hang_par", (1, 0), -5, "hanging parent")])
+def test_set_mesh_rejects_bad_input(field, index, value, msg):
+    """The mesh checks run on the device; a rejected mesh leaves the context
+    without a mesh until a valid one is set."""
+    import ctypes as C
+    prob = CASES["mol60"]().build()
+    g = GpuPath().load(prob)
+    lib = g._lib
+    d = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in prob.mesh().items()}
+    d[field][index] = value
+    bad = _mesh_from(d)
+    assert lib.pbgpu_set_mesh(g._ctx, C.byref(bad)) == N.PBGPU_ERR_ARG
+    assert msg in lib.pbgpu_last_error(g._ctx).decode()
+    assert lib.pbgpu_create_markers(g._ctx) == N.PBGPU_ERR_STATE
+    good = prob.mesh_struct()
+    assert lib.pbgpu_set_mesh(g._ctx, C.byref(good)) == 0
+    g.create_markers()
+    g.close()
+
+
+def test_set_rays_rejects_unsorted_keys():
+    import ctypes as C
+    prob = CASES["mol60"]().build()
+    g = GpuPath().load(prob)
+    r = prob.rays(2)
+    keys = r["keys"].copy()
+    keys[[3, 4]] = keys[[4, 3]]
+    rs = N.PbgpuRays()
+    rs.n_rays = len(keys)
+    rs.keys = keys.ctypes.data_as(C.POINTER(C.c_uint64))
+    rs.ptr = r["ptr"].ctypes.data_as(C.POINTER(C.c_int64))
+    rs.inters = r["inters"].ctypes.data_as(C.POINTER(C.c_double))
+    normals = np.ascontiguousarray(r["normals"])
+    rs.normals = normals.ctypes.data_as(C.POINTER(C.c_double))
+    assert g._lib.pbgpu_set_rays(g._ctx, 2, C.byref(rs)) == N.PBGPU_ERR_ARG
+    assert "keys not strictly ascending" in g._lib.pbgpu_last_error(g._ctx).decode()
+    g.close()

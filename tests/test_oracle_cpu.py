@@ -140,3 +140,37 @@ def test_golden_born_fixture(born):
     e = o.energy()
     for k in ("energy_pol", "energy_react", "charge_flux"):
         assert e[k] == pytest.approx(g["energy"][k], rel=1e-9)
+
+
+@pytest.mark.parametrize("method", ["cg", "bicgstab"])
+def test_preconditioners_same_solution(born, method):
+    """-p none / jacobi / block Jacobi: the same solution, preconditioned runs
+    need fewer iterations than the unpreconditioned one."""
+    prob, o, _ = born
+    ref, _, _ = o.solve("cg", 1e-12)
+    its = {}
+    for pc in ("none", "jacobi", "block_jacobi"):
+        phi, it, rel = o.solve(method, 1e-10, precond=pc)
+        assert rel <= 1e-10
+        assert np.linalg.norm(phi - ref) / np.linalg.norm(ref) < 1e-8
+        its[pc] = it
+    assert its["jacobi"] < its["none"] and its["block_jacobi"] < its["none"]
+
+
+def test_cgs_and_conv_cond(born):
+    """CGS reaches the CG solution; conv_cond 2 (||r||_1 <= tol_w ||b||_1 +
+    tol) stops on the 1-norm of the residual."""
+    prob, o, (rp, col, val, rhs) = born
+    ref, _, _ = o.solve("cg", 1e-12)
+    for pc in ("jacobi", "block_jacobi"):
+        phi, it, rel = o.solve("cgs", 1e-10, precond=pc)
+        assert rel <= 1e-10 and np.linalg.norm(phi - ref) / np.linalg.norm(ref) < 1e-8
+    n = len(rp) - 1
+    A = sp.csr_matrix((val, col, rp), shape=(n, n))
+    for tol in (1e-4, 1e-6):
+        phi, it, rel = o.solve("cgs", tol, precond="block_jacobi", conv_cond=2, tol_w=0.0)
+        assert np.abs(rhs - A @ phi).sum() <= 1.01 * tol
+    # a looser rule stops earlier
+    _, it4, _ = o.solve("cgs", 1e-4, precond="block_jacobi", conv_cond=2, tol_w=0.0)
+    _, it6, _ = o.solve("cgs", 1e-6, precond="block_jacobi", conv_cond=2, tol_w=0.0)
+    assert it4 < it6
