@@ -124,13 +124,20 @@ def measured_peak():
 
 
 def spmv_traffic():
-    """DRAM bytes per SpMV launch from the committed ncu summary, scaled to the
-    bench workload by nnz when the capture was on a smaller case."""
+    """DRAM bytes per SpMV launch of each kernel from the committed ncu
+    summaries (captured on a smaller case; scaled to the bench workload by nnz)."""
     p = os.path.join(ROOT, "profiles", "spmv_traffic.json")
     try:
         return json.load(open(p))
     except Exception:
         return None
+
+
+def spmv_kernel_name(args):
+    """The CG SpMV kernel the solve runs for the bench's layout."""
+    if args.chunk == 32 and args.group == 1 and os.environ.get("PBGPU_SPMV") != "direct":
+        return "k_cg_spmv_tma<double, %s>" % os.environ.get("PBGPU_SPMV_COLS", "16")
+    return "k_cg_spmv<double, %d>" % args.group
 
 
 def build_problem(name):
@@ -311,10 +318,11 @@ def run_ours(args, rank, world, local):
         peak, peak_kind = measured_peak()
         spmv_avg_ms = cnt["spmv_ms"] / max(cnt["spmv_launches"], 1)
         achieved = cnt["spmv_bytes"] / (spmv_avg_ms / 1e3) / 1e9 if cnt["spmv_launches"] else None
+        kname = spmv_kernel_name(args)
         tr = spmv_traffic()
         traffic = None
-        if tr:
-            traffic = tr["dram_bytes_per_launch"] * (info_nnz(g) / tr["nnz"]) if tr.get("nnz") else None
+        if tr and kname in tr.get("kernels", {}):
+            traffic = tr["kernels"][kname]["dram_bytes_per_launch"] * (info_nnz(g) / tr["nnz"])
         result = {
             "metric": METRIC,
             "value": value,
@@ -343,7 +351,7 @@ def run_ours(args, rank, world, local):
             },
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": pin["h2d_bytes"],
                     "d2h_bytes_per_step": int(8 * pin["na"] + 48)},
-            "roofline": {"kernel": "k_cg_spmv<double> (SELL-C-sigma SpMV fused with p.Ap)", "bound": "hbm",
+            "roofline": {"kernel": kname + " (SELL-C-sigma SpMV fused with p.Ap)", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": cnt["spmv_bytes"],
@@ -439,17 +447,232 @@ def run_reference(args, rank, world):
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+BATCHES = {
+    # name: (molecules, min atoms, max atoms, seed, surface levels)
+    "batch96": (96, 50, 3000, 96, 1),
+    "batch16": (16, 50, 600, 16, 1),
+}
+
+
+def build_pool(specs, levels, workers=8):
+    """Host problems of a molecule pool, built by a thread pool (the host
+    mesh build releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from cudanextgenpb_b200 import configs
+
+    def one(spec):
+        na, rad, net, seed = spec
+        return configs.make_globular_problem(na, rad, net, seed, scale=2.0, levels=levels).build()
+
+    t0 = time.time()
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        probs = list(ex.map(one, specs))
+    log("host pool of %d molecules built in %.1fs" % (len(probs), time.time() - t0))
+    return probs
+
+
+def run_batch(args, rank, world, local):
+    """Batched workload: many independent molecules, each with its own octree,
+    solved together by the persistent multi-system kernel, against the plain
+    path that solves them one at a time.  A step solves every molecule once."""
+    import torch
+
+    from cudanextgenpb_b200 import Batch, GpuPath, configs, solver_opts
+
+    if rank != 0 and world > 1:
+        return None
+    torch.cuda.set_device(local)
+    count, lo, hi, seed, levels = BATCHES[args.workload]
+    specs = configs.molecule_specs(count, lo, hi, seed)
+    probs = build_pool(specs, levels)
+    ctxs = [GpuPath(local).load(p) for p in probs]
+    n_dof = sum(p.info()["n_nodes"] for p in probs)
+    plain_opts = solver_opts("cg", tol=args.tol, max_iter=50000)
+    batch_opts = solver_opts("cg", tol=args.tol, max_iter=50000, precision=args.precision, inner_tol=1e-4,
+                             check_every=64)
+
+    def setup(g):
+        g.create_markers()
+        g.create_density_map()
+        g.assemble(32, 2048, 4)
+
+    def plain_step():
+        out = []
+        for g in ctxs:
+            setup(g)
+            g.solve(plain_opts)
+            out.append(g.energy(False)["sum"])
+        return out
+
+    b = Batch(local)
+    for g in ctxs:
+        setup(g)
+        b.add(g)
+
+    def batch_step():
+        for g in ctxs:
+            setup(g)
+        stats = b.solve(batch_opts)
+        return [g.energy(False)["sum"] for g in ctxs], stats
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = None
+        lat = []
+        for _ in range(k):
+            a = time.perf_counter()
+            r = fn()
+            torch.cuda.synchronize()
+            lat.append(1e3 * (time.perf_counter() - a))
+        return (time.perf_counter() - t0), r, lat
+
+    for _ in range(args.warmup):
+        plain_step()
+        batch_step()
+    clocks = Clocks(local)
+    clocks.start()
+    t_plain, e_plain, _ = timed(plain_step, args.steps)
+    t_batch, (e_batch, stats), lat = timed(batch_step, args.steps)
+    ck = clocks.stop()
+    err = max(abs(x - y) / max(abs(y), 1e-300) for x, y in zip(e_batch, e_plain))
+    value = count * args.steps / t_batch
+    plain = count * args.steps / t_plain
+    iters = [s.iterations for s in stats.values()]
+    b.close()
+    for g in ctxs:
+        g.close()
+    return {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_batch / args.steps,
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64"
+        else "f32-inner/f64", "data": "synthetic",
+        "config": {"workload": "%d synthetic molecules, atoms log-uniform in %d-%d (seed %d), own octree each, "
+                               "scale 2/A, %d surface level(s); one persistent multi-system CG per step"
+                               % (count, lo, hi, seed, levels, ),
+                   "n_dof_total": n_dof, "tol": args.tol, "precision": args.precision,
+                   "inner_iterations_median": float(np.median(iters)),
+                   "plain_solves_per_s": plain, "speedup_vs_plain": value / plain,
+                   "max_rel_energy_err_vs_plain": err,
+                   "wall_clock": "host perf_counter around each step after a device synchronize"},
+        "clocks": ck,
+    }
+
+
+SERVES = {
+    # name: (pool size, min atoms, max atoms, seed, surface levels, arrivals per s, seconds)
+    "serve": (24, 200, 3000, 5, 1, 200.0, 10.0),
+    "serve_small": (8, 50, 400, 5, 1, 100.0, 3.0),
+}
+
+
+def run_serve(args, rank, world, local):
+    """Serving workload: a seeded Poisson request stream over a pool of
+    synthetic molecules, served by the continuous-batching server, against the
+    plain FP64 path taking the same requests one at a time.  Latency is from
+    each request's arrival time to its result (queueing included)."""
+    import torch
+
+    from cudanextgenpb_b200 import GpuPath, Server, configs, solver_opts
+
+    if rank != 0 and world > 1:
+        return None
+    torch.cuda.set_device(local)
+    npool, lo, hi, seed, levels, rate, seconds = SERVES[args.workload]
+    specs = configs.molecule_specs(npool, lo, hi, seed)
+    probs = build_pool(specs, levels)
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * seconds * 1.5)))
+    arrivals = arrivals[arrivals < seconds]
+    picks = rng.integers(0, npool, size=len(arrivals))
+    n_req = len(arrivals)
+
+    # served
+    srv = Server(local, tol=args.tol, precision=args.precision, max_members=args.max_members,
+                 steps_per_tick=32, inner_tol=1e-4)
+    reqs = [srv.request(p) for p in probs]
+    # warm-up: one request of each molecule
+    for r in reqs:
+        srv.submit(r)
+    got = 0
+    while got < npool:
+        got += len(srv.progress())
+    lat_s, e_served = {}, {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nxt = 0
+    while len(lat_s) < n_req:
+        now = time.perf_counter() - t0
+        while nxt < n_req and arrivals[nxt] <= now:
+            r = srv.request(probs[picks[nxt]], tag=nxt)
+            srv.submit(r)
+            nxt += 1
+        for res in srv.progress():
+            k = res["tag"]
+            lat_s[k] = 1e3 * (time.perf_counter() - t0 - arrivals[k])
+            e_served[k] = res["energy"]["sum"]
+        if nxt < n_req and not srv.pending()[0] and not srv.pending()[1]:
+            time.sleep(max(0.0, min(arrivals[nxt] - (time.perf_counter() - t0), 0.002)))
+    t_served = time.perf_counter() - t0
+    srv.close()
+
+    # plain FP64, one at a time, same stream
+    g = GpuPath(local)
+    plain_opts = solver_opts("cg", tol=args.tol, max_iter=50000)
+    e_plain = {}
+    for k in range(npool):
+        g.load(probs[k])
+        g.run(plain_opts)
+    lat_p = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(n_req):
+        now = time.perf_counter() - t0
+        if arrivals[k] > now:
+            time.sleep(arrivals[k] - now)
+        g.load(probs[picks[k]])
+        e, _ = g.run(plain_opts)
+        e_plain[k] = e["sum"]
+        lat_p[k] = 1e3 * (time.perf_counter() - t0 - arrivals[k])
+    t_plain = time.perf_counter() - t0
+    g.close()
+    err = max(abs(e_served[k] - e_plain[k]) / max(abs(e_plain[k]), 1e-300) for k in range(n_req))
+    ls = np.array([lat_s[k] for k in range(n_req)])
+    lp = np.array([lat_p[k] for k in range(n_req)])
+    value = n_req / t_served
+    plain = n_req / t_plain
+    pct = lambda a: {"p50": float(np.percentile(a, 50)), "p95": float(np.percentile(a, 95)),
+                     "p99": float(np.percentile(a, 99))}
+    return {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": n_req, "warmup": npool,
+        "ms_per_step": 1e3 * t_served / n_req, "latency_ms": pct(ls), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32-inner/f64", "data": "synthetic",
+        "config": {"workload": "Poisson stream %.0f req/s for %.0f s (seed %d) over %d synthetic molecules, atoms "
+                               "log-uniform in %d-%d, scale 2/A, %d surface level(s); continuous-batching server"
+                               % (rate, seconds, seed, npool, lo, hi, levels),
+                   "requests": n_req, "tol": args.tol, "precision": args.precision,
+                   "max_members": args.max_members,
+                   "plain_solves_per_s": plain, "plain_latency_ms": pct(lp), "speedup_vs_plain": value / plain,
+                   "max_rel_energy_err_vs_plain": err,
+                   "wall_clock": "host perf_counter; latency from each request's scheduled arrival"},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mol2000", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="mol2000", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(SERVES))
+    ap.add_argument("--max-members", type=int, default=64)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--chunk", type=int, default=32)
     ap.add_argument("--sigma", type=int, default=2048)
-    ap.add_argument("--group", type=int, default=1)
+    ap.add_argument("--group", type=int, default=4)
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "block_jacobi", "none"])
     ap.add_argument("--cpu-iters", type=int, default=30)
     ap.add_argument("--ref-iters", type=int, default=0)
@@ -460,7 +683,13 @@ def main():
     from cudanextgenpb_b200 import build as b
     if rank == 0:
         b.build_all()
-    if args.impl == "reference":
+    if args.workload in SERVES:
+        res = run_serve(args, rank, world, local) if args.impl == "ours" else {
+            "impl": "reference", "unavailable": "the serving workload is measured against the plain GPU path"}
+    elif args.workload in BATCHES:
+        res = run_batch(args, rank, world, local) if args.impl == "ours" else {
+            "impl": "reference", "unavailable": "batched workloads are measured against the plain GPU path"}
+    elif args.impl == "reference":
         res = run_reference(args, rank, world)
     else:
         res = run_ours(args, rank, world, local)

@@ -57,7 +57,23 @@ class PbgpuEnergyOut(C.Structure):
 
 class PbgpuCounters(C.Structure):
     _fields_ = [("launches", i64), ("spmv_launches", i64), ("spmv_ms", dbl), ("spmv_bytes", dbl),
-                ("krylov_iterations", i64), ("energy_points", i64), ("energy_pairs", i64)]
+                ("krylov_iterations", i64), ("energy_points", i64), ("energy_pairs", i64),
+                ("device_bytes", i64)]
+
+
+class PbgpuRequest(C.Structure):
+    _fields_ = [("mesh", P(PbgpuMesh)), ("rays", PbgpuRays * 3), ("n_atoms", i64), ("pos", P(dbl)),
+                ("charge", P(dbl)), ("model", P(PbgpuModel)), ("user_tag", i64)]
+
+
+class PbgpuResult(C.Structure):
+    _fields_ = [("id", i64), ("user_tag", i64), ("status", C.c_int), ("energy", PbgpuEnergyOut),
+                ("stats", PbgpuSolveStats), ("latency_ms", dbl), ("queue_ms", dbl)]
+
+
+class PbgpuServerOpts(C.Structure):
+    _fields_ = [("hbm_budget_bytes", dbl), ("max_members", C.c_int), ("steps_per_tick", C.c_int),
+                ("blocks_per_sm", C.c_int), ("solver", PbgpuSolverOpts), ("energy_fast", C.c_int)]
 
 
 class PbhostInfo(C.Structure):
@@ -107,6 +123,25 @@ PBGPU_FUNCS = {
     "pbgpu_get_counters": (C.c_int, [ctx_p, P(PbgpuCounters)]),
     "pbgpu_reset_counters": (C.c_int, [ctx_p]),
     "pbgpu_coulomb_energy_static": (C.c_int, [C.c_void_p, i64, dbl, dbl, C.c_void_p, C.c_void_p]),
+    "pbgpu_batch_create": (C.c_int, [P(C.c_void_p), C.c_int, C.c_void_p]),
+    "pbgpu_batch_destroy": (None, [C.c_void_p]),
+    "pbgpu_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "pbgpu_batch_add": (C.c_int, [C.c_void_p, ctx_p, P(C.c_int)]),
+    "pbgpu_batch_remove": (C.c_int, [C.c_void_p, C.c_int]),
+    "pbgpu_batch_size": (C.c_int, [C.c_void_p]),
+    "pbgpu_batch_solve": (C.c_int, [C.c_void_p, P(PbgpuSolverOpts), P(PbgpuSolveStats)]),
+    "pbgpu_batch_begin": (C.c_int, [C.c_void_p, P(PbgpuSolverOpts)]),
+    "pbgpu_batch_step": (C.c_int, [C.c_void_p, C.c_int, P(C.c_int)]),
+    "pbgpu_batch_member": (C.c_int, [C.c_void_p, C.c_int, P(C.c_int), P(PbgpuSolveStats)]),
+    "pbgpu_batch_set_blocks_per_sm": (C.c_int, [C.c_void_p, C.c_int]),
+    "pbgpu_default_server_opts": (None, [P(PbgpuServerOpts)]),
+    "pbgpu_server_create": (C.c_int, [P(C.c_void_p), C.c_int, P(PbgpuServerOpts)]),
+    "pbgpu_server_destroy": (None, [C.c_void_p]),
+    "pbgpu_server_last_error": (C.c_char_p, [C.c_void_p]),
+    "pbgpu_server_submit": (C.c_int, [C.c_void_p, P(PbgpuRequest), P(i64)]),
+    "pbgpu_server_progress": (C.c_int, [C.c_void_p, P(PbgpuResult), C.c_int, P(C.c_int)]),
+    "pbgpu_server_pending": (C.c_int, [C.c_void_p, P(C.c_int), P(C.c_int), P(i64)]),
+    "pbgpu_request_bytes_estimate": (i64, [P(PbgpuRequest)]),
 }
 
 host_p = C.c_void_p

@@ -157,3 +157,29 @@ def make_born_problem(unilevel=5, maxlevel=6, half=8.0, bc_type=3):
     prob = Problem(born_options(unilevel, maxlevel, half, bc_type))
     prob.set_atoms(*BORN_ATOM)
     return prob
+
+
+def radius_for(n_atoms: int) -> float:
+    """Smallest radius (0.5 A steps) whose sphere holds the n atoms at <= 90%
+    of the FCC lattice sites (the 2,000-atom configuration uses 18 A)."""
+    a = 2.5 * math.sqrt(2.0)
+    r = max(4.0, round((n_atoms / 0.9 / (4.0 / a ** 3) / (4.0 / 3.0 * math.pi)) ** (1.0 / 3.0) * 2) / 2)
+    while True:
+        m = int(math.ceil(r / a)) + 1
+        g = np.arange(-m, m + 1)
+        base = np.array(np.meshgrid(g, g, g, indexing="ij")).reshape(3, -1).T.astype(np.float64)
+        offs = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+        sites = (base[:, None, :] + offs[None, :, :]).reshape(-1, 3) * a
+        if (np.linalg.norm(sites, axis=1) <= r).sum() * 0.9 >= n_atoms:
+            return r
+        r += 0.5
+
+
+def molecule_specs(count: int, lo: int, hi: int, seed: int):
+    """Seeded molecule specs for batches and request streams: atom counts
+    log-uniform in [lo, hi], integer net charges in [-5, 5]; each spec is
+    (n_atoms, radius, net_charge, seed)."""
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(math.log(lo), math.log(hi), size=count)).astype(int)
+    net = rng.integers(-5, 6, size=count)
+    return [(int(k), radius_for(int(k)), float(c), int(seed * 1000 + j)) for j, (k, c) in enumerate(zip(n, net))]

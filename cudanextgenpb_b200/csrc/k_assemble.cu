@@ -405,7 +405,7 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   if (!c->have_density) return c->fail(PBGPU_ERR_STATE, "assemble: create_density_map has not run");
   int C = (o && o->chunk > 0) ? o->chunk : 32;
   int sigma = (o && o->sigma > 0) ? o->sigma : 2048;
-  int G = (o && o->group > 0) ? o->group : 1;
+  int G = (o && o->group > 0) ? o->group : 4;
   if (C % 32 != 0 || C > 1024) return c->fail(PBGPU_ERR_ARG, "SELL chunk must be a multiple of 32, at most 1024");
   if (sigma % C != 0 && sigma != 1) return c->fail(PBGPU_ERR_ARG, "SELL sigma must be 1 or a multiple of the chunk");
   if (G != 1 && G != 2 && G != 4) return c->fail(PBGPU_ERR_ARG, "SELL group must be 1, 2 or 4");

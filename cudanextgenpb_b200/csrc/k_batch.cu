@@ -1,0 +1,818 @@
+// Multi-system Krylov solve: many assembled systems (one per context) advanced
+// together by ONE persistent cooperative kernel per chunk of steps.  This is
+// the batching layer over lis_compute_electric_potential
+// (src/pb_class.cpp:2244-2329): the reference solves one system per process;
+// here independent molecules share the GPU in one launch.
+//
+// Design:
+//  * Every member keeps its own SELL matrix and vectors; the kernel walks a
+//    table of member descriptors.  Rows are grouped in row-blocks of 256 rows,
+//    each row-block belongs to one member (rb_sys table), and the persistent
+//    blocks stride over all row-blocks.
+//  * Reductions are per member and deterministic: each row-block writes its
+//    partial sums, and after a grid barrier one warp per member sums that
+//    member's row-block partials in a fixed order and updates its scalars.
+//  * Each member runs Jacobi-preconditioned CG on A d = r in the inner type
+//    TI (float: FP32 matrix and vectors; double: plain FP64) with the
+//    solution accumulated in FP64.  In FP32 the CG uses reliable updates:
+//    whenever its recursive residual has fallen by 10x since the last FP64
+//    residual, x += d, the residual b - A x is recomputed in FP64 and the CG
+//    continues from it keeping its search direction, so the iteration count
+//    stays that of FP64 CG.  The FP64 residual also makes the final
+//    convergence test.  Members move through these phases independently:
+//    one step of the kernel does one CG iteration for members in the inner
+//    phase and the residual / start / update work for the others.
+//  * A step has five row phases separated by a grid barrier (bounded spin:
+//    a barrier that times out sets an error flag and every block returns).
+//  * The kernel leaves early once every member is done.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "pbgpu_internal.cuh"
+#include "sell.cuh"
+#include "tma.cuh"
+
+namespace pbgpu {
+
+constexpr int kRowBlock = kBlock;  // rows per row-block
+constexpr int kBatchMinBlocks = 4;
+
+// Phases of a member: Outer (first FP64 residual), Start (CG start on it),
+// Inner (CG iterations in TI), Apply (inner target met: x += xi, then FP64
+// residual), Reliable (mixed precision: the TI residual fell by delta since
+// the last FP64 residual: x += xi, FP64 residual), Resume (continue CG from
+// the fresh FP64 residual keeping the search direction), Done.
+enum { kPhOuter = 0, kPhStart = 1, kPhInner = 2, kPhApply = 3, kPhDone = 4, kPhReliable = 5, kPhResume = 6 };
+
+template <typename TI>
+struct BMember {
+  SellT<double> A;       // FP64 system (SELL order)
+  const double* b;
+  double* x;             // solution
+  SellT<TI> Ai;          // inner matrix (FP32 copy or the FP64 values)
+  const TI* dinv;        // 1 / diag in TI
+  TI* bi;                // inner right-hand side = outer residual
+  TI* xi;                // inner solution = correction
+  TI* r;
+  TI* p;
+  TI* q;
+  int64_t rb0;           // first global row-block
+  int nrb;               // row-blocks of this member
+};
+
+struct BState {
+  double bb, rr64, tol2;      // ||b||^2, ||b - A x||^2, tol^2 ||b||^2
+  double rz, alpha, beta, rri, tol2i;
+  double inner_tol;
+  double rr_ref;              // ||b - A x||^2 at the last FP64 residual
+  double delta2;              // reliable update when the TI residual^2 < delta2 * rr_ref (0: off)
+  int phase, iters, inner_it, outer, status, max_iter, inner_cap, plain;
+};
+
+struct GridBar {
+  unsigned count;
+  unsigned gen;
+  int err;
+  unsigned active[2];  // members not done, per step parity
+};
+
+// Generation barrier over all blocks of a cooperative launch; the wait is
+// bounded (about 2 s of wall time), after which err is set and every caller
+// returns false.
+__device__ __forceinline__ bool grid_barrier(GridBar* g) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = &g->gen;
+    const unsigned gen = *vgen;
+    __threadfence();
+    if (atomicAdd(&g->count, 1u) == gridDim.x - 1) {
+      g->count = 0;
+      __threadfence();
+      atomicAdd(&g->gen, 1u);
+    } else {
+      const uint64_t t0 = global_ns();
+      uint32_t it = 0;
+      while (*vgen == gen) {
+        if ((++it & 255u) == 0 && global_ns() - t0 > 2000000000ull) {
+          atomicExch(&g->err, 1);
+          break;
+        }
+        if (*reinterpret_cast<volatile int*>(&g->err)) break;
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *reinterpret_cast<volatile int*>(&g->err) == 0;
+}
+
+// Loads of data that other blocks of the running kernel write (gathered
+// vector entries, member scalars, row-block partials) go through L2 only
+// (ld.global.cg), never through the SM's L1 or the read-only path; every row is
+// owned by the same thread in every phase, so a thread's own rows need no care.
+template <typename T>
+__device__ __forceinline__ T ldcg(const T* p) {
+  return __ldcg(p);
+}
+
+// y_i = sum_j A(i, j) x_j of a G = 4 SELL row (sell_elem layout), x gathered
+// through L2.
+template <typename T>
+__device__ __forceinline__ T batch_row(const SellT<T>& A, int64_t p, const T* x) {
+  const int64_t s = p / A.C;
+  const int lane = (int)(p - s * A.C);
+  const int W = A.slice_w[s];
+  const int64_t sb = A.slice_ptr[s];
+  const int64_t base = sb + 4 * lane;
+  const int64_t stride = 4 * (int64_t)A.C;
+  T acc = 0;
+#pragma unroll 2
+  for (int g = 0; g < (W >> 2); ++g) {
+    const int64_t k = base + g * stride;
+    const int4 c = __ldcs(reinterpret_cast<const int4*>(A.scol + k));
+    if constexpr (sizeof(T) == 8) {
+      const double2 v0 = __ldcs(reinterpret_cast<const double2*>(A.sval + k));
+      const double2 v1 = __ldcs(reinterpret_cast<const double2*>(A.sval + k + 2));
+      acc += v0.x * ldcg(x + c.x);
+      acc += v0.y * ldcg(x + c.y);
+      acc += v1.x * ldcg(x + c.z);
+      acc += v1.y * ldcg(x + c.w);
+    } else {
+      const float4 v = __ldcs(reinterpret_cast<const float4*>(A.sval + k));
+      acc += v.x * ldcg(x + c.x);
+      acc += v.y * ldcg(x + c.y);
+      acc += v.z * ldcg(x + c.z);
+      acc += v.w * ldcg(x + c.w);
+    }
+  }
+  const int Wg = W & ~3;
+  const int64_t tb = sb + (int64_t)Wg * A.C + lane;
+  for (int j = Wg; j < W; ++j) {
+    const int64_t k = tb + (int64_t)(j - Wg) * A.C;
+    acc += __ldcs(A.sval + k) * ldcg(x + __ldcs(A.scol + k));
+  }
+  return acc;
+}
+
+// Sum of this member's row-block partials (K per row-block) by one warp, in a
+// fixed order; valid in all lanes.
+template <int K>
+__device__ __forceinline__ void member_sum(const double* part, int64_t rb0, int nrb, double (&out)[K]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < K; ++k) out[k] = 0.0;
+  for (int j = lane; j < nrb; j += 32)
+#pragma unroll
+    for (int k = 0; k < K; ++k) out[k] += ldcg(part + (rb0 + j) * 2 + k);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    for (int o = 16; o > 0; o >>= 1) out[k] += __shfl_xor_sync(0xffffffffu, out[k], o);
+}
+
+template <typename TI>
+__global__ void __launch_bounds__(kBlock, kBatchMinBlocks)
+    k_batch_cg(const BMember<TI>* __restrict__ mem, int n_mem, const int32_t* __restrict__ rb_sys, int64_t n_rb,
+               BState* st, double* part, GridBar* bar, int steps) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  __shared__ int ph_s;
+  for (int step = 0; step < steps; ++step) {
+    // ---- P1: outer residual (outer / apply) or q = A p (inner)
+    for (int64_t rb = blockIdx.x; rb < n_rb; rb += gridDim.x) {
+      const int s = rb_sys[rb];
+      if (threadIdx.x == 0) ph_s = ldcg(&st[s].phase);
+      __syncthreads();
+      const int ph = ph_s;
+      const BMember<TI>& M = mem[s];
+      const int64_t i = (rb - M.rb0) * kRowBlock + threadIdx.x;
+      double v[2] = {0.0, 0.0};
+      if ((ph == kPhOuter || ph == kPhApply || ph == kPhReliable) && i < M.A.n_pad) {
+        const double ri = M.b[i] - batch_row<double>(M.A, i, M.x);
+        M.bi[i] = (TI)ri;
+        v[0] = ri * ri;
+        v[1] = M.b[i] * M.b[i];
+      } else if (ph == kPhInner && i < M.A.n_pad) {
+        const TI y = batch_row<TI>(M.Ai, i, M.p);
+        M.q[i] = y;
+        v[0] = (double)M.p[i] * (double)y;
+      }
+      block_sum<2>(v);
+      if (threadIdx.x == 0) {
+        part[rb * 2] = v[0];
+        part[rb * 2 + 1] = v[1];
+      }
+    }
+    if (!grid_barrier(bar)) return;
+    // ---- P2: per-member decisions
+    if (blockIdx.x == 0 && threadIdx.x == 0) bar->active[(step + 1) & 1] = 0;
+    for (int64_t s = gwarp; s < n_mem; s += nwarps) {
+      BState& S = st[s];
+      const int ph = ldcg(&S.phase);
+      if (ph == kPhDone || ph == kPhStart || ph == kPhResume) continue;
+      double a[2];
+      member_sum<2>(part, mem[s].rb0, mem[s].nrb, a);
+      if (lane != 0) continue;
+      if (ph == kPhOuter || ph == kPhApply || ph == kPhReliable) {
+        if (S.outer == 0) {
+          S.bb = a[1];
+          S.tol2 = S.tol2 * a[1];  // tol^2 was stored; scale by ||b||^2
+        }
+        S.rr64 = a[0];
+        S.outer += 1;
+        if (!isfinite(a[0])) {
+          S.status = PBGPU_BREAKDOWN;
+          S.phase = kPhDone;
+        } else if (a[0] <= S.tol2) {
+          S.phase = kPhDone;
+        } else if (S.iters >= S.max_iter) {
+          S.status = PBGPU_NOT_CONVERGED;
+          S.phase = kPhDone;
+        } else {
+          // the TI recursion aims at the final target; with reliable updates
+          // (mixed precision) its residual is refreshed from FP64 on the way
+          S.rr_ref = a[0];
+          S.tol2i = S.tol2;
+          S.phase = ph == kPhOuter ? kPhStart : kPhResume;
+          S.inner_it = 0;
+        }
+      } else {  // inner
+        const double alpha = S.rz / a[0];
+        if (!(a[0] > 0.0) || !isfinite(alpha)) {
+          S.status = PBGPU_BREAKDOWN;
+          S.phase = kPhDone;
+        } else {
+          S.alpha = alpha;
+        }
+      }
+    }
+    if (!grid_barrier(bar)) return;
+    // ---- P3: inner start (xi = 0, r = bi, p = z) or inner update
+    for (int64_t rb = blockIdx.x; rb < n_rb; rb += gridDim.x) {
+      const int s = rb_sys[rb];
+      if (threadIdx.x == 0) ph_s = ldcg(&st[s].phase);
+      __syncthreads();
+      const int ph = ph_s;
+      const BMember<TI>& M = mem[s];
+      const int64_t i = (rb - M.rb0) * kRowBlock + threadIdx.x;
+      double v[2] = {0.0, 0.0};
+      if ((ph == kPhStart || ph == kPhResume) && i < M.A.n_pad) {
+        const TI ri = M.bi[i];
+        const TI zi = M.dinv[i] * ri;
+        M.xi[i] = 0;
+        M.r[i] = ri;
+        if (ph == kPhStart) M.p[i] = zi;
+        v[0] = (double)ri * (double)zi;
+      } else if (ph == kPhInner && i < M.A.n_pad) {
+        const TI alpha = (TI)ldcg(&st[s].alpha);
+        M.xi[i] += alpha * M.p[i];
+        const TI ri = M.r[i] - alpha * M.q[i];
+        M.r[i] = ri;
+        v[0] = (double)ri * (double)(M.dinv[i] * ri);
+        v[1] = (double)ri * (double)ri;
+      }
+      block_sum<2>(v);
+      if (threadIdx.x == 0) {
+        part[rb * 2] = v[0];
+        part[rb * 2 + 1] = v[1];
+      }
+    }
+    if (!grid_barrier(bar)) return;
+    // ---- P4: per-member inner bookkeeping
+    for (int64_t s = gwarp; s < n_mem; s += nwarps) {
+      BState& S = st[s];
+      const int ph = ldcg(&S.phase);
+      if (ph == kPhStart || ph == kPhResume || ph == kPhInner) {
+        double a[2];
+        member_sum<2>(part, mem[s].rb0, mem[s].nrb, a);
+        if (lane == 0) {
+          if (ph == kPhStart) {
+            S.rz = a[0];
+            S.phase = kPhInner;
+          } else if (ph == kPhResume) {
+            // CG continues from the fresh residual: p = z + beta p in P5
+            S.beta = a[0] / S.rz;
+            S.rz = a[0];
+            S.phase = isfinite(S.beta) ? kPhInner : kPhDone;
+            if (S.phase == kPhDone) S.status = PBGPU_BREAKDOWN;
+          } else {
+            S.iters += 1;
+            S.inner_it += 1;
+            S.rri = a[1];
+            if (!isfinite(a[0]) || !isfinite(a[1])) {
+              S.status = PBGPU_BREAKDOWN;
+              S.phase = kPhDone;
+            } else if (a[1] <= S.tol2i || S.inner_it >= S.inner_cap || S.iters >= S.max_iter) {
+              S.phase = kPhApply;
+            } else if (a[1] <= S.delta2 * S.rr_ref) {
+              S.phase = kPhReliable;
+            } else {
+              S.beta = a[0] / S.rz;
+              S.rz = a[0];
+            }
+          }
+        }
+      }
+      if (lane == 0 && S.phase != kPhDone) atomicAdd(&bar->active[step & 1], 1u);
+    }
+    if (!grid_barrier(bar)) return;
+    // ---- P5: p = z + beta p (inner) or x += xi (apply)
+    for (int64_t rb = blockIdx.x; rb < n_rb; rb += gridDim.x) {
+      const int s = rb_sys[rb];
+      if (threadIdx.x == 0) ph_s = ldcg(&st[s].phase);
+      __syncthreads();
+      const int ph = ph_s;
+      const BMember<TI>& M = mem[s];
+      const int64_t i = (rb - M.rb0) * kRowBlock + threadIdx.x;
+      if (ph == kPhInner && i < M.A.n_pad) {
+        const TI beta = (TI)ldcg(&st[s].beta);
+        M.p[i] = M.dinv[i] * M.r[i] + beta * M.p[i];
+      } else if ((ph == kPhApply || ph == kPhReliable) && i < M.A.n_pad) {
+        M.x[i] += (double)M.xi[i];
+      }
+      __syncthreads();
+    }
+    const unsigned active = *reinterpret_cast<volatile unsigned*>(&bar->active[step & 1]);
+    if (!grid_barrier(bar)) return;
+    if (active == 0) return;
+  }
+}
+
+template <typename TI>
+__global__ void k_batch_gather(const BMember<TI>* __restrict__ mem, int s, int64_t n,
+                               const int32_t* __restrict__ iperm, double* __restrict__ phi) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) phi[i] = mem[s].x[iperm[i]];
+}
+
+__global__ void k_batch_to_f32(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+}  // namespace pbgpu
+
+using namespace pbgpu;
+
+// A batch keeps one descriptor and one state per slot; slots without a member
+// are "done" and own no row-blocks.  A session (begin .. step ..) fixes the
+// solver options; members added during a session start at the next step.
+struct pbgpu_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sm_count = 148;
+  int blocks_per_sm = 0;  // 0: as many as fit
+  std::string err;
+  std::vector<pbgpu_ctx*> slots;
+  std::vector<char> pending;  // member needs its vectors and state set up
+  bool session = false;
+  bool mixed = false;
+  pbgpu_solver_opts opts{};
+  bool dirty = true;          // row-block table out of date
+  int64_t n_rb = 0;
+  DBuf<BMember<double>> m64;
+  DBuf<BMember<float>> m32;
+  std::vector<BMember<double>> h64;
+  std::vector<BMember<float>> h32;
+  DBuf<int32_t> rb_sys;
+  DBuf<double> part;
+  DBuf<BState> st;
+  DBuf<GridBar> bar;
+  BState* st_host = nullptr;
+  size_t st_cap = 0;
+  int64_t launches = 0;
+  float last_ms = 0.f;
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+};
+
+namespace {
+
+int bfail(pbgpu_batch* b, cudaError_t e, const char* what) {
+  cudaGetLastError();
+  return b->fail(PBGPU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define BATCH_CUDA(b, expr)                                                   \
+  do {                                                                        \
+    cudaError_t _e = (expr);                                                  \
+    if (_e != cudaSuccess) return bfail((b), _e, #expr);                      \
+  } while (0)
+
+// Per-slot device arrays sized for every slot index.
+int ensure_capacity(pbgpu_batch* B) {
+  const size_t n = std::max<size_t>(B->slots.size(), 1);
+  if (B->st_cap >= n) return PBGPU_OK;
+  const size_t cap = std::max<size_t>(n, 2 * B->st_cap);
+  BState* h = nullptr;
+  BATCH_CUDA(B, cudaMallocHost(&h, cap * sizeof(BState)));
+  for (size_t k = 0; k < cap; ++k) {
+    h[k] = BState{};
+    h[k].phase = kPhDone;
+  }
+  if (B->st_host) {
+    std::memcpy(h, B->st_host, B->st_cap * sizeof(BState));
+    cudaFreeHost(B->st_host);
+  }
+  B->st_host = h;
+  // device copies: grow and carry the live states over
+  DBuf<BState> nst;
+  BATCH_CUDA(B, nst.alloc(cap));
+  BATCH_CUDA(B, cudaMemcpyAsync(nst.get(), h, cap * sizeof(BState), cudaMemcpyHostToDevice, B->stream));
+  if (B->st.get() && B->st_cap)
+    BATCH_CUDA(B, cudaMemcpyAsync(nst.get(), B->st.get(), B->st_cap * sizeof(BState), cudaMemcpyDeviceToDevice,
+                                  B->stream));
+  BATCH_CUDA(B, cudaStreamSynchronize(B->stream));
+  std::swap(B->st.p, nst.p);
+  std::swap(B->st.n, nst.n);
+  B->h64.resize(cap);
+  B->h32.resize(cap);
+  BATCH_CUDA(B, B->m64.alloc(cap));
+  BATCH_CUDA(B, B->m32.alloc(cap));
+  B->st_cap = cap;
+  return PBGPU_OK;
+}
+
+// Vectors, FP32 copies and descriptor of a new member; its state starts at
+// the first outer step with x = 0.
+template <typename TI>
+int prepare_member(pbgpu_batch* B, int slot) {
+  Context* c = &B->slots[slot]->c;
+  AcctScope acct(&c->dev_bytes);
+  BATCH_CUDA(B, cudaStreamSynchronize(c->stream));  // the member's assembly is complete
+  if (c->G != 4 || c->C != 32) return B->fail(PBGPU_ERR_ARG, "batch: members must be assembled with chunk 32, group 4");
+  const int64_t n_pad = c->n_slices * c->C;
+  const bool mixed = std::is_same<TI, float>::value;
+  cudaError_t e = cudaSuccess;
+  DBuf<double>* v64[] = {&c->x, &c->r, &c->p, &c->q, &c->rh, &c->s};
+  for (DBuf<double>* d : v64)
+    if (e == cudaSuccess) e = d->alloc(n_pad);
+  if (mixed) {
+    DBuf<float>* v32[] = {&c->x32, &c->r32, &c->p32, &c->q32, &c->b32, &c->dinv32};
+    for (DBuf<float>* d : v32)
+      if (e == cudaSuccess) e = d->alloc(n_pad);
+    if (e == cudaSuccess) e = c->sval32.alloc(c->sell_len);
+  }
+  if (e != cudaSuccess) return bfail(B, e, "batch: member vectors");
+  BATCH_CUDA(B, cudaMemsetAsync(c->x.get(), 0, n_pad * sizeof(double), B->stream));
+  if (mixed) {
+    const int g = (int)std::min<int64_t>((c->sell_len + kBlock - 1) / kBlock, (int64_t)B->sm_count * 8);
+    k_batch_to_f32<<<g, kBlock, 0, B->stream>>>(c->sell_len, c->sval.get(), c->sval32.get());
+    k_batch_to_f32<<<g, kBlock, 0, B->stream>>>(n_pad, c->dinv.get(), c->dinv32.get());
+    B->launches += 2;
+    BATCH_CUDA(B, cudaGetLastError());
+  }
+  BMember<TI> M{};
+  M.A = SellT<double>{c->slice_ptr.get(), c->slice_w.get(), c->scol.get(), c->sval.get(), n_pad, c->C, c->G};
+  M.b = c->b.get();
+  M.x = c->x.get();
+  if constexpr (std::is_same<TI, float>::value) {
+    M.Ai = SellT<float>{c->slice_ptr.get(), c->slice_w.get(), c->scol.get(), c->sval32.get(), n_pad, c->C, c->G};
+    M.dinv = c->dinv32.get();
+    M.bi = c->b32.get();
+    M.xi = c->x32.get();
+    M.r = c->r32.get();
+    M.p = c->p32.get();
+    M.q = c->q32.get();
+    B->h32[slot] = M;
+  } else {
+    M.Ai = M.A;
+    M.dinv = c->dinv.get();
+    M.bi = c->rh.get();
+    M.xi = c->s.get();
+    M.r = c->r.get();
+    M.p = c->p.get();
+    M.q = c->q.get();
+    B->h64[slot] = M;
+  }
+  const pbgpu_solver_opts& o = B->opts;
+  BState S{};
+  S.tol2 = o.tol * o.tol;  // scaled by ||b||^2 at the first outer step
+  S.inner_tol = o.inner_tol > 0 ? o.inner_tol : 1e-5;
+  S.phase = kPhOuter;
+  S.status = PBGPU_OK;
+  S.max_iter = o.max_iter;
+  S.inner_cap = o.max_iter;
+  S.plain = mixed ? 0 : 1;
+  S.delta2 = mixed ? 0.01 : 0.0;  // reliable update every 10x residual reduction in FP32
+  B->st_host[slot] = S;
+  BATCH_CUDA(B, cudaMemcpyAsync(B->st.get() + slot, &B->st_host[slot], sizeof(BState), cudaMemcpyHostToDevice,
+                                B->stream));
+  B->pending[slot] = 0;
+  B->dirty = true;
+  return PBGPU_OK;
+}
+
+// Descriptors and the row-block -> slot table of the current members.
+template <typename TI>
+int upload_tables(pbgpu_batch* B) {
+  std::vector<BMember<TI>>& hm = *[&]() {
+    if constexpr (std::is_same<TI, float>::value)
+      return &B->h32;
+    else
+      return &B->h64;
+  }();
+  std::vector<int32_t> rbs;
+  for (size_t k = 0; k < B->slots.size(); ++k) {
+    if (!B->slots[k]) {
+      hm[k] = BMember<TI>{};
+      continue;
+    }
+    hm[k].rb0 = (int64_t)rbs.size();
+    hm[k].nrb = (int)((hm[k].A.n_pad + kRowBlock - 1) / kRowBlock);
+    for (int j = 0; j < hm[k].nrb; ++j) rbs.push_back((int32_t)k);
+  }
+  B->n_rb = (int64_t)rbs.size();
+  BMember<TI>* dm;
+  if constexpr (std::is_same<TI, float>::value)
+    dm = B->m32.get();
+  else
+    dm = B->m64.get();
+  BATCH_CUDA(B, cudaMemcpyAsync(dm, hm.data(), B->slots.size() * sizeof(BMember<TI>), cudaMemcpyHostToDevice,
+                                B->stream));
+  BATCH_CUDA(B, B->rb_sys.alloc(std::max<int64_t>(B->n_rb, 1)));
+  if (B->n_rb)
+    BATCH_CUDA(B, cudaMemcpyAsync(B->rb_sys.get(), rbs.data(), B->n_rb * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                  B->stream));
+  BATCH_CUDA(B, B->part.alloc(2 * std::max<int64_t>(B->n_rb, 1)));
+  B->dirty = false;
+  return PBGPU_OK;
+}
+
+template <typename TI>
+int batch_step(pbgpu_batch* B, int steps, int* n_active) {
+  int rc;
+  if ((rc = ensure_capacity(B)) != PBGPU_OK) return rc;
+  for (size_t k = 0; k < B->slots.size(); ++k)
+    if (B->slots[k] && B->pending[k] && (rc = prepare_member<TI>(B, (int)k)) != PBGPU_OK) return rc;
+  if (B->dirty && (rc = upload_tables<TI>(B)) != PBGPU_OK) return rc;
+  const int nm = (int)B->slots.size();
+  int active = 0;
+  if (B->n_rb > 0 && steps > 0) {
+    if (!B->bar.get()) {
+      BATCH_CUDA(B, B->bar.alloc(1));
+      BATCH_CUDA(B, cudaMemsetAsync(B->bar.get(), 0, sizeof(GridBar), B->stream));
+    }
+    int occ = 0;
+    BATCH_CUDA(B, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_cg<TI>, kBlock, 0));
+    if (occ <= 0) return B->fail(PBGPU_ERR_CUDA, "batch: kernel cannot be resident");
+    if (B->blocks_per_sm > 0) occ = std::min(occ, B->blocks_per_sm);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)occ * B->sm_count, B->n_rb));
+    const BMember<TI>* a_mem;
+    if constexpr (std::is_same<TI, float>::value)
+      a_mem = B->m32.get();
+    else
+      a_mem = B->m64.get();
+    int a_nm = nm;
+    const int32_t* a_rb = B->rb_sys.get();
+    int64_t a_nrb = B->n_rb;
+    BState* a_st = B->st.get();
+    double* a_part = B->part.get();
+    GridBar* a_bar = B->bar.get();
+    int a_steps = steps;
+    void* args[] = {&a_mem, &a_nm, &a_rb, &a_nrb, &a_st, &a_part, &a_bar, &a_steps};
+    cudaEvent_t e0, e1;
+    BATCH_CUDA(B, cudaEventCreate(&e0));
+    BATCH_CUDA(B, cudaEventCreate(&e1));
+    cudaEventRecord(e0, B->stream);
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_batch_cg<TI>, dim3(grid), dim3(kBlock), args, 0,
+                                                B->stream);
+    if (e == cudaSuccess) B->launches += 1;
+    cudaEventRecord(e1, B->stream);
+    GridBar hb{};
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(B->st_host, B->st.get(), nm * sizeof(BState), cudaMemcpyDeviceToHost, B->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hb, B->bar.get(), sizeof(GridBar), cudaMemcpyDeviceToHost, B->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
+    float ms = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return bfail(B, e, "batch: persistent kernel");
+    B->last_ms += ms;
+    if (hb.err) return B->fail(PBGPU_TIMEOUT, "batch: grid barrier wait timed out");
+  } else {
+    BATCH_CUDA(B, cudaMemcpyAsync(B->st_host, B->st.get(), nm * sizeof(BState), cudaMemcpyDeviceToHost, B->stream));
+    BATCH_CUDA(B, cudaStreamSynchronize(B->stream));
+  }
+  for (int k = 0; k < nm; ++k) active += B->slots[k] && B->st_host[k].phase != kPhDone;
+  if (n_active) *n_active = active;
+  return PBGPU_OK;
+}
+
+// Potential of a finished member into its context (node order) and its stats.
+template <typename TI>
+int finish_member(pbgpu_batch* B, int slot, pbgpu_solve_stats* stats) {
+  Context* c = &B->slots[slot]->c;
+  AcctScope acct(&c->dev_bytes);
+  const BState& S = B->st_host[slot];
+  BATCH_CUDA(B, c->phi.alloc(c->n));
+  const BMember<TI>* dm;
+  if constexpr (std::is_same<TI, float>::value)
+    dm = B->m32.get();
+  else
+    dm = B->m64.get();
+  k_batch_gather<TI><<<(int)((c->n + 255) / 256), 256, 0, B->stream>>>(dm, slot, c->n, c->iperm.get(), c->phi.get());
+  B->launches += 1;
+  BATCH_CUDA(B, cudaGetLastError());
+  BATCH_CUDA(B, cudaStreamSynchronize(B->stream));
+  c->have_phi = true;
+  c->krylov_iters += S.iters;
+  if (stats) {
+    stats->status = S.phase == kPhDone ? S.status : PBGPU_NOT_CONVERGED;
+    stats->iterations = S.iters;
+    stats->outer = S.outer;
+    stats->rel_residual = S.bb > 0 ? std::sqrt(S.rr64 / S.bb) : 0.0;
+    stats->device_ms = B->last_ms;
+  }
+  return PBGPU_OK;
+}
+
+int check_opts(pbgpu_batch* b, const pbgpu_solver_opts& o) {
+  if (o.method != PBGPU_CG) return b->fail(PBGPU_ERR_ARG, "batch: members are solved with CG");
+  if (o.precond != PBGPU_PRECOND_JACOBI) return b->fail(PBGPU_ERR_ARG, "batch: members use the Jacobi preconditioner");
+  if (o.conv_cond == 2) return b->fail(PBGPU_ERR_ARG, "batch: conv_cond 0 or 1 (relative 2-norm)");
+  if (!(o.tol > 0) || o.max_iter <= 0) return b->fail(PBGPU_ERR_ARG, "batch: tol and max_iter must be positive");
+  return PBGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pbgpu_batch_create(pbgpu_batch** out, int device, void* cuda_stream) {
+  if (!out) return PBGPU_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return PBGPU_ERR_CUDA;
+  }
+  if (device < 0 || device >= ndev) return PBGPU_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return PBGPU_ERR_CUDA;
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+  if (!coop) return PBGPU_ERR_CUDA;
+  pbgpu_batch* b = new (std::nothrow) pbgpu_batch();
+  if (!b) return PBGPU_ERR_OOM;
+  b->device = device;
+  cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (cuda_stream) {
+    b->stream = static_cast<cudaStream_t>(cuda_stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete b;
+      return PBGPU_ERR_CUDA;
+    }
+    b->own_stream = true;
+  }
+  *out = b;
+  return PBGPU_OK;
+}
+
+void pbgpu_batch_destroy(pbgpu_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->st_host) cudaFreeHost(b->st_host);
+  cudaStream_t s = b->stream;
+  const bool own = b->own_stream;
+  delete b;
+  if (own && s) cudaStreamDestroy(s);
+}
+
+const char* pbgpu_batch_last_error(const pbgpu_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int pbgpu_batch_add(pbgpu_batch* b, pbgpu_ctx* ctx, int* slot) {
+  if (!b || !ctx) return PBGPU_ERR_ARG;
+  if (ctx->c.device != b->device) return b->fail(PBGPU_ERR_ARG, "batch_add: context is on another device");
+  if (!ctx->c.have_system) return b->fail(PBGPU_ERR_STATE, "batch_add: the context has no assembled system");
+  for (pbgpu_ctx* m : b->slots)
+    if (m == ctx) return b->fail(PBGPU_ERR_ARG, "batch_add: context is already a member");
+  int k = -1;
+  for (size_t j = 0; j < b->slots.size(); ++j)
+    if (!b->slots[j]) {
+      k = (int)j;
+      break;
+    }
+  if (k < 0) {
+    k = (int)b->slots.size();
+    b->slots.push_back(nullptr);
+    b->pending.push_back(0);
+  }
+  b->slots[k] = ctx;
+  b->pending[k] = 1;
+  b->dirty = true;
+  if (slot) *slot = k;
+  return PBGPU_OK;
+}
+
+int pbgpu_batch_remove(pbgpu_batch* b, int slot) {
+  if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot]) return PBGPU_ERR_ARG;
+  b->slots[slot] = nullptr;
+  b->pending[slot] = 0;
+  if (b->st_host && (size_t)slot < b->st_cap) {
+    b->st_host[slot].phase = kPhDone;
+    if (cudaSetDevice(b->device) != cudaSuccess) return PBGPU_ERR_CUDA;
+    const cudaError_t e = cudaMemcpyAsync(b->st.get() + slot, &b->st_host[slot], sizeof(BState),
+                                          cudaMemcpyHostToDevice, b->stream);
+    if (e != cudaSuccess) return bfail(b, e, "batch_remove");
+    if ((size_t)slot + 1 == b->slots.size()) cudaStreamSynchronize(b->stream);
+  }
+  b->dirty = true;
+  return PBGPU_OK;
+}
+
+int pbgpu_batch_size(const pbgpu_batch* b) {
+  if (!b) return -1;
+  int n = 0;
+  for (pbgpu_ctx* m : b->slots) n += m != nullptr;
+  return n;
+}
+
+int pbgpu_batch_set_blocks_per_sm(pbgpu_batch* b, int blocks) {
+  if (!b || blocks < 0) return PBGPU_ERR_ARG;
+  b->blocks_per_sm = blocks;
+  return PBGPU_OK;
+}
+
+int pbgpu_batch_begin(pbgpu_batch* b, const pbgpu_solver_opts* opts) {
+  if (!b) return PBGPU_ERR_ARG;
+  pbgpu_solver_opts o;
+  if (opts)
+    o = *opts;
+  else
+    pbgpu_default_solver_opts(&o);
+  const int rc = check_opts(b, o);
+  if (rc != PBGPU_OK) return rc;
+  b->opts = o;
+  b->mixed = o.precision == PBGPU_MIXED;
+  b->session = true;
+  b->last_ms = 0.f;
+  for (size_t k = 0; k < b->slots.size(); ++k) b->pending[k] = b->slots[k] != nullptr;
+  b->dirty = true;
+  return PBGPU_OK;
+}
+
+int pbgpu_batch_step(pbgpu_batch* b, int steps, int* n_active) {
+  if (!b || steps < 0) return PBGPU_ERR_ARG;
+  if (!b->session) return b->fail(PBGPU_ERR_STATE, "batch_step: no session (pbgpu_batch_begin)");
+  if (cudaSetDevice(b->device) != cudaSuccess) return PBGPU_ERR_CUDA;
+  cudaGetLastError();
+  return b->mixed ? batch_step<float>(b, steps, n_active) : batch_step<double>(b, steps, n_active);
+}
+
+int pbgpu_batch_member(pbgpu_batch* b, int slot, int* done, pbgpu_solve_stats* stats) {
+  if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot]) return PBGPU_ERR_ARG;
+  if (!b->session || b->pending[slot] || !b->st_host) {
+    if (done) *done = 0;
+    return PBGPU_OK;
+  }
+  const bool fin = b->st_host[slot].phase == kPhDone;
+  if (done) *done = fin;
+  if (!fin) return PBGPU_OK;
+  if (cudaSetDevice(b->device) != cudaSuccess) return PBGPU_ERR_CUDA;
+  return b->mixed ? finish_member<float>(b, slot, stats) : finish_member<double>(b, slot, stats);
+}
+
+int pbgpu_batch_solve(pbgpu_batch* b, const pbgpu_solver_opts* opts, pbgpu_solve_stats* stats) {
+  int rc = pbgpu_batch_begin(b, opts);
+  if (rc != PBGPU_OK) return rc;
+  const pbgpu_solver_opts& o = b->opts;
+  const int chunk = o.check_every > 0 ? std::max(o.check_every, 16) : 64;
+  const int max_outer = o.max_outer > 0 ? o.max_outer : 50;
+  const int64_t max_steps = (int64_t)o.max_iter + 4LL * (max_outer + 2);
+  int active = 1;
+  for (int64_t done = 0; done < max_steps && active > 0; done += chunk)
+    if ((rc = pbgpu_batch_step(b, chunk, &active)) != PBGPU_OK) return rc;
+  int worst = PBGPU_OK;
+  for (size_t k = 0; k < b->slots.size(); ++k) {
+    if (!b->slots[k]) continue;
+    pbgpu_solve_stats t{};
+    int fin = 0;
+    if (b->st_host[k].phase != kPhDone) {
+      // iteration budget used up: report the member as not converged
+      b->st_host[k].phase = kPhDone;
+      b->st_host[k].status = PBGPU_NOT_CONVERGED;
+    }
+    if ((rc = pbgpu_batch_member(b, (int)k, &fin, &t)) != PBGPU_OK) return rc;
+    if (stats) stats[k] = t;
+    if (t.status != PBGPU_OK && worst == PBGPU_OK) worst = t.status;
+  }
+  b->session = false;
+  if (worst == PBGPU_NOT_CONVERGED) return b->fail(worst, "batch: a member reached the iteration limit");
+  if (worst == PBGPU_BREAKDOWN) return b->fail(worst, "batch: a member broke down");
+  return PBGPU_OK;
+}
+
+}  // extern "C"

@@ -33,100 +33,10 @@
 #include <type_traits>
 
 #include "pbgpu_internal.cuh"
+#include "sell.cuh"
 #include "tma.cuh"
 
 namespace pbgpu {
-
-constexpr int kBlock = 256;
-// resident blocks per SM the SpMV kernels are compiled for (registers <= 65536 / (256 * 5));
-// kernels with three or more fused reductions get 4 (64 registers, no spills)
-constexpr int kSpmvMinBlocks = 5;
-constexpr int kSpmvMinBlocksWide = 4;
-
-template <typename T>
-struct SellT {
-  const int64_t* slice_ptr;
-  const int32_t* slice_w;
-  const int32_t* scol;
-  const T* sval;
-  int64_t n_pad;
-  int C;
-  int G;  // columns per row stored contiguously: 1, 2 or 4
-};
-
-template <typename T>
-struct V2 {};
-template <>
-struct V2<double> {
-  using t = double2;
-};
-template <>
-struct V2<float> {
-  using t = float2;
-};
-
-// y_p = sum_j A(p, j) x_j for SELL row p, element j at sell_elem(): the
-// first W - W % G columns in groups of G (one vector load per group, a warp's
-// loads of one group contiguous), the remaining W % G columns one per lane.
-template <typename T, int G>
-__device__ __forceinline__ T sell_row(const SellT<T>& A, int64_t p, const T* __restrict__ x) {
-  const int64_t s = p / A.C;
-  const int lane = (int)(p - s * A.C);
-  const int W = A.slice_w[s];
-  const int64_t sb = A.slice_ptr[s];
-  T acc = 0;
-  if constexpr (G == 1) {
-    const int64_t base = sb + lane;
-    const int64_t stride = A.C;
-#pragma unroll 4
-    for (int j = 0; j < W; ++j) {
-      const int64_t k = base + j * stride;
-      acc += __ldcs(A.sval + k) * x[__ldcs(A.scol + k)];
-    }
-    return acc;
-  } else if constexpr (G == 2) {
-    const int64_t base = sb + 2 * lane;
-    const int64_t stride = 2 * (int64_t)A.C;
-#pragma unroll 2
-    for (int g = 0; g < (W >> 1); ++g) {
-      const int64_t k = base + g * stride;
-      const int2 c = __ldcs(reinterpret_cast<const int2*>(A.scol + k));
-      const typename V2<T>::t v = __ldcs(reinterpret_cast<const typename V2<T>::t*>(A.sval + k));
-      acc += v.x * x[c.x];
-      acc += v.y * x[c.y];
-    }
-  } else {
-    const int64_t base = sb + 4 * lane;
-    const int64_t stride = 4 * (int64_t)A.C;
-#pragma unroll 2
-    for (int g = 0; g < (W >> 2); ++g) {
-      const int64_t k = base + g * stride;
-      const int4 c = __ldcs(reinterpret_cast<const int4*>(A.scol + k));
-      if constexpr (sizeof(T) == 8) {
-        const double2 v0 = __ldcs(reinterpret_cast<const double2*>(A.sval + k));
-        const double2 v1 = __ldcs(reinterpret_cast<const double2*>(A.sval + k + 2));
-        acc += v0.x * x[c.x];
-        acc += v0.y * x[c.y];
-        acc += v1.x * x[c.z];
-        acc += v1.y * x[c.w];
-      } else {
-        const float4 v = __ldcs(reinterpret_cast<const float4*>(A.sval + k));
-        acc += v.x * x[c.x];
-        acc += v.y * x[c.y];
-        acc += v.z * x[c.z];
-        acc += v.w * x[c.w];
-      }
-    }
-  }
-  // tail columns, one per lane
-  const int Wg = W - W % G;
-  const int64_t tb = sb + (int64_t)Wg * A.C + lane;
-  for (int j = Wg; j < W; ++j) {
-    const int64_t k = tb + (int64_t)(j - Wg) * A.C;
-    acc += __ldcs(A.sval + k) * x[__ldcs(A.scol + k)];
-  }
-  return acc;
-}
 
 // ---------------------------------------------------------------------------
 // SpMV with the matrix staged through shared memory by bulk async copies
@@ -244,29 +154,6 @@ __device__ __forceinline__ bool spmv_tma_rows(const SellT<T>& A, const T* __rest
   return true;
 }
 
-// Block-wide sum of K values; result valid in thread 0.
-template <int K>
-__device__ __forceinline__ void block_sum(double (&v)[K]) {
-  __shared__ double sh[K][kBlock / 32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    double a = v[k];
-    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
-    if (lane == 0) sh[k][wid] = a;
-  }
-  __syncthreads();
-  if (wid == 0) {
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      double a = lane < kBlock / 32 ? sh[k][lane] : 0.0;
-      for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
-      v[k] = a;
-    }
-  }
-  __syncthreads();
-}
-
 // Write this block's partials; returns true in the last block to finish, whose
 // thread 0 then holds the grid-wide sums in v (summed in block order).
 template <int K>
@@ -353,11 +240,10 @@ template <typename T, int G>
 __global__ void __launch_bounds__(kBlock, G == 1 ? kSpmvMinBlocks : kSpmvMinBlocksWide) k_cg_spmv(SellT<T> A, const T* __restrict__ p, T* __restrict__ q, KrylovScalars* ks, double* partials) {
   if (ks->done) return;
   double v[1] = {0.0};
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x) {
-    const T y = sell_row<T, G>(A, i, p);
+  spmv_direct_rows<T, G>(A, p, [&](int64_t i, T y) {
     q[i] = y;
     v[0] += (double)p[i] * (double)y;
-  }
+  });
   if (grid_sum<1>(v, partials, &ks->ticket[1]) && threadIdx.x == 0) {
     ks->pq = v[0];
     ks->alpha = ks->rz / v[0];
@@ -576,11 +462,10 @@ __global__ void __launch_bounds__(kBlock, G == 1 ? kSpmvMinBlocks : kSpmvMinBloc
                          KrylovScalars* ks, double* partials) {
   if (ks->done) return;
   double s[1] = {0.0};
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x) {
-    const T y = sell_row<T, G>(A, i, ph);
+  spmv_direct_rows<T, G>(A, ph, [&](int64_t i, T y) {
     v[i] = y;
     s[0] += (double)rh[i] * (double)y;
-  }
+  });
   if (grid_sum<1>(s, partials, &ks->ticket[1]) && threadIdx.x == 0) {
     ks->alpha = ks->rv / s[0];
     if (s[0] == 0.0 || !finite(ks->alpha)) {
@@ -617,12 +502,11 @@ __global__ void __launch_bounds__(kBlock, kSpmvMinBlocksWide) k_bicg_t(SellT<T> 
                          KrylovScalars* ks, double* partials) {
   if (ks->done || ks->s_conv) return;
   double a[2] = {0.0, 0.0};
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x) {
-    const T y = sell_row<T, G>(A, i, sh);
+  spmv_direct_rows<T, G>(A, sh, [&](int64_t i, T y) {
     t[i] = y;
     a[0] += (double)y * (double)s[i];
     a[1] += (double)y * (double)y;
-  }
+  });
   if (grid_sum<2>(a, partials, &ks->ticket[3]) && threadIdx.x == 0) {
     ks->ts = a[0];
     ks->tt = a[1];
@@ -688,15 +572,15 @@ template <int G>
 __global__ void __launch_bounds__(kBlock, kSpmvMinBlocksWide) k_residual(SellT<double> A, int64_t n, const double* __restrict__ b, const double* __restrict__ x,
                            double* __restrict__ r, float* __restrict__ r32, KrylovScalars* ks, double* partials) {
   double a[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x) {
-    const double ri = i < n ? b[i] - sell_row<double, G>(A, i, x) : 0.0;
+  spmv_direct_rows<double, G>(A, x, [&](int64_t i, double y) {
+    const double ri = i < n ? b[i] - y : 0.0;
     if (r) r[i] = ri;
     if (r32) r32[i] = (float)ri;
     a[0] += ri * ri;
     a[1] += i < n ? b[i] * b[i] : 0.0;
     a[2] += fabs(ri);
     a[3] += i < n ? fabs(b[i]) : 0.0;
-  }
+  });
   if (grid_sum<4>(a, partials, &ks->ticket[5]) && threadIdx.x == 0) {
     ks->rr = a[0];
     ks->bb = a[1];
@@ -708,7 +592,9 @@ __global__ void __launch_bounds__(kBlock, kSpmvMinBlocksWide) k_residual(SellT<d
 // ---------------------------------------------------------------------------
 // The SpMV kernels again with the matrix staged by bulk async copies (C = 32,
 // G = 1).  A bounded wait that gives up ends the solve with PBGPU_TIMEOUT.
-constexpr int kTmaMinBlocks = 2;
+// resident blocks per SM of the staged kernels: their FP64 shared memory
+// (2 buffers x NC columns x 8 warps) allows 4 blocks at NC = 8, 3 at 12, 2 at 16
+__host__ __device__ constexpr int tma_min_blocks(int nc) { return nc <= 8 ? 4 : nc <= 12 ? 3 : 2; }
 
 __device__ __forceinline__ void tma_timeout(KrylovScalars* ks) {
   if ((threadIdx.x & 31) == 0) {
@@ -733,7 +619,7 @@ __device__ __forceinline__ bool timed_out(const KrylovScalars* ks) {
 }
 
 template <typename T, int NC>
-__global__ void __launch_bounds__(kBlock, kTmaMinBlocks)
+__global__ void __launch_bounds__(kBlock, tma_min_blocks(NC))
     k_cg_spmv_tma(SellT<T> A, const T* __restrict__ p, T* __restrict__ q, KrylovScalars* ks, double* partials) {
   if (block_skip(ks, false)) return;
   double v[1] = {0.0};
@@ -753,7 +639,7 @@ __global__ void __launch_bounds__(kBlock, kTmaMinBlocks)
 }
 
 template <typename T, int NC>
-__global__ void __launch_bounds__(kBlock, kTmaMinBlocks)
+__global__ void __launch_bounds__(kBlock, tma_min_blocks(NC))
     k_bicg_v_tma(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh,
                  KrylovScalars* ks, double* partials) {
   if (block_skip(ks, false)) return;
@@ -773,7 +659,7 @@ __global__ void __launch_bounds__(kBlock, kTmaMinBlocks)
 }
 
 template <typename T, int NC>
-__global__ void __launch_bounds__(kBlock, kTmaMinBlocks)
+__global__ void __launch_bounds__(kBlock, tma_min_blocks(NC))
     k_bicg_t_tma(SellT<T> A, const T* __restrict__ sh, T* __restrict__ t, const T* __restrict__ s,
                  KrylovScalars* ks, double* partials) {
   if (block_skip(ks, true)) return;
@@ -792,7 +678,7 @@ __global__ void __launch_bounds__(kBlock, kTmaMinBlocks)
 }
 
 template <int NC>
-__global__ void __launch_bounds__(kBlock, kTmaMinBlocks)
+__global__ void __launch_bounds__(kBlock, tma_min_blocks(NC))
     k_residual_tma(SellT<double> A, int64_t n, const double* __restrict__ b, const double* __restrict__ x,
                    double* __restrict__ r, float* __restrict__ r32, KrylovScalars* ks, double* partials) {
   double a[4] = {0.0, 0.0, 0.0, 0.0};
@@ -893,15 +779,14 @@ __device__ __forceinline__ bool spmv_rows(const SellT<T>& A, const T* __restrict
   if constexpr (NC > 0) {
     return spmv_tma_rows<T, NC>(A, x, fn);
   } else {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x)
-      fn(i, sell_row<T, G>(A, i, x));
+    spmv_direct_rows<T, G>(A, x, fn);
     return true;
   }
 }
 
 // v = A ph;  alpha = rho / (rh, v)
 template <typename T, int G, int NC>
-__global__ void __launch_bounds__(kBlock, NC > 0 ? kTmaMinBlocks : G == 1 ? kSpmvMinBlocks : kSpmvMinBlocksWide)
+__global__ void __launch_bounds__(kBlock, NC > 0 ? tma_min_blocks(NC) : G == 1 ? kSpmvMinBlocks : kSpmvMinBlocksWide)
     k_cgs_v(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh, KrylovScalars* ks,
             double* partials) {
   if (block_skip(ks, false)) return;
@@ -922,7 +807,7 @@ __global__ void __launch_bounds__(kBlock, NC > 0 ? kTmaMinBlocks : G == 1 ? kSpm
 
 // r -= alpha A uh;  x += alpha uh;  (r, r), (rh, r), ||r||_1; convergence; beta
 template <typename T, int G, int NC>
-__global__ void __launch_bounds__(kBlock, NC > 0 ? kTmaMinBlocks : kSpmvMinBlocksWide)
+__global__ void __launch_bounds__(kBlock, NC > 0 ? tma_min_blocks(NC) : kSpmvMinBlocksWide)
     k_cgs_r(SellT<T> A, const T* __restrict__ uh, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ rh,
             KrylovScalars* ks, double* partials) {
   if (block_skip(ks, false)) return;

@@ -68,6 +68,7 @@ using namespace pbgpu;
 // runtime call of this thread left behind (reported on stderr when PBGPU_DEBUG
 // is set), so it is not blamed on this call's launches.
 #define SET_DEVICE(C)                                                                         \
+  AcctScope _acct(&(C)->dev_bytes);                                                           \
   do {                                                                                        \
     cudaError_t _e = cudaSetDevice((C)->device);                                              \
     if (_e != cudaSuccess) return cuda_fail((C), _e, "cudaSetDevice");                        \
@@ -558,6 +559,7 @@ int pbgpu_get_counters(pbgpu_ctx* h, pbgpu_counters* out) {
   out->krylov_iterations = c.krylov_iters;
   out->energy_points = c.energy_points;
   out->energy_pairs = c.energy_pairs;
+  out->device_bytes = c.dev_bytes;
   return PBGPU_OK;
 }
 

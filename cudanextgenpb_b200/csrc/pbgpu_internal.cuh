@@ -19,27 +19,48 @@ constexpr int kMaxIncidence = 160;  // (octant, corner) incidences of one node
 constexpr uint64_t kEmptyKey = ~0ull;
 
 // ---------------------------------------------------------------------------
+// Device bytes held per context: a buffer charges the counter that is current
+// on this thread when it allocates (AcctScope, set at every API entry) and
+// credits the same counter when it frees.
+inline thread_local int64_t* tl_acct = nullptr;
+
+struct AcctScope {
+  int64_t* prev;
+  explicit AcctScope(int64_t* a) : prev(tl_acct) { tl_acct = a; }
+  ~AcctScope() { tl_acct = prev; }
+};
+
 // Device buffer owned by a context.
 template <typename T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0;
+  int64_t* acct = nullptr;
   DBuf() = default;
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
   ~DBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaFree(p);
+      if (acct) *acct -= (int64_t)(n * sizeof(T));
+    }
     p = nullptr;
     n = 0;
+    acct = nullptr;
   }
   cudaError_t alloc(size_t count) {
     if (count <= n && p) return cudaSuccess;
     release();
     if (count == 0) return cudaSuccess;
     cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-    if (e == cudaSuccess) n = count;
-    else p = nullptr;
+    if (e == cudaSuccess) {
+      n = count;
+      acct = tl_acct;
+      if (acct) *acct += (int64_t)(count * sizeof(T));
+    } else {
+      p = nullptr;
+    }
     return e;
   }
   T* get() const { return p; }
@@ -110,6 +131,7 @@ struct Scratch {
 };
 
 struct Context {
+  int64_t dev_bytes = 0;     // device memory held by this context's buffers
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;

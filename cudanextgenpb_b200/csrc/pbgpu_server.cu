@@ -1,0 +1,283 @@
+// PB solve server: continuous batching of requests of different molecule sizes
+// on one GPU.  No counterpart in the reference, whose driver
+// (src/poisson_boltzmann.cpp:192-299) runs one molecule per process.
+//
+// A tick of pbgpu_server_progress:
+//   1. admits queued requests (FIFO) while the member cap and the HBM budget
+//      allow: the request's inputs are set on an idle context (or a new one)
+//      and its markers, density map and SELL system are built on that
+//      context's own stream;
+//   2. advances every member system with one persistent launch of the
+//      multi-system solver (pbgpu_batch_step), which holds the matrices and
+//      Krylov states of all members on the device;
+//   3. retires the members that converged: potential at atoms and energies on
+//      their context, result returned, context back to the idle pool.
+// Setup of new requests (1) is issued on the member contexts' streams while
+// the persistent kernel of the previous tick may still run on the batch
+// stream; the persistent kernel is limited to blocks_per_sm resident blocks
+// so other kernels fit beside it.
+// Admission counts the device bytes every context holds (idle ones included,
+// their buffers are kept for reuse) plus an estimate for the request; idle
+// contexts are destroyed, largest first, when the budget needs the room.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <string>
+#include <vector>
+
+#include "pbgpu_internal.cuh"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_since(Clock::time_point t) {
+  return std::chrono::duration<double, std::milli>(Clock::now() - t).count();
+}
+
+struct Pending {
+  int64_t id;
+  pbgpu_request req;
+  Clock::time_point t_submit;
+};
+
+struct Running {
+  int64_t id;
+  int64_t tag;
+  int slot;
+  pbgpu_ctx* ctx;
+  int64_t n_atoms;
+  Clock::time_point t_submit, t_admit;
+};
+
+int64_t ctx_bytes(pbgpu_ctx* c) { return c ? c->c.dev_bytes : 0; }
+
+}  // namespace
+
+struct pbgpu_server {
+  int device = 0;
+  pbgpu_server_opts opts{};
+  pbgpu_batch* batch = nullptr;
+  std::deque<Pending> queue;
+  std::vector<Running> running;
+  std::vector<pbgpu_ctx*> idle;
+  int64_t next_id = 1;
+  bool in_session = false;
+  std::string err;
+  int64_t admitted = 0, completed = 0;
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+};
+
+extern "C" {
+
+int64_t pbgpu_request_bytes_estimate(const pbgpu_request* r) {
+  if (!r || !r->mesh) return 0;
+  const double no = (double)r->mesh->n_oct, n = (double)r->mesh->n_nodes, nh = (double)r->mesh->n_hang;
+  // mesh, incidence lists, per-octant local coefficients (assembly scratch),
+  // SELL matrix (~11 nonzeros per row, 12 B each), Krylov vectors (FP64 and
+  // FP32), energy scratch; per unit of each size
+  return (int64_t)(330.0 * no + 330.0 * n + 40.0 * nh) + ((int64_t)64 << 20);
+}
+
+void pbgpu_default_server_opts(pbgpu_server_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->hbm_budget_bytes = 160e9;
+  o->max_members = 64;
+  o->steps_per_tick = 32;
+  o->blocks_per_sm = 2;
+  pbgpu_default_solver_opts(&o->solver);
+  o->solver.method = PBGPU_CG;
+  o->solver.precond = PBGPU_PRECOND_JACOBI;
+  o->solver.precision = PBGPU_MIXED;
+  o->solver.tol = 1e-8;
+  o->solver.inner_tol = 1e-4;
+  o->solver.max_iter = 50000;
+  o->energy_fast = 0;
+}
+
+int pbgpu_server_create(pbgpu_server** out, int device, const pbgpu_server_opts* opts) {
+  if (!out) return PBGPU_ERR_ARG;
+  *out = nullptr;
+  pbgpu_server* s = new (std::nothrow) pbgpu_server();
+  if (!s) return PBGPU_ERR_OOM;
+  s->device = device;
+  if (opts)
+    s->opts = *opts;
+  else
+    pbgpu_default_server_opts(&s->opts);
+  if (s->opts.max_members <= 0) s->opts.max_members = 64;
+  if (s->opts.steps_per_tick <= 0) s->opts.steps_per_tick = 32;
+  if (!(s->opts.hbm_budget_bytes > 0)) s->opts.hbm_budget_bytes = 160e9;
+  int st = pbgpu_batch_create(&s->batch, device, nullptr);
+  if (st != PBGPU_OK) {
+    delete s;
+    return st;
+  }
+  pbgpu_batch_set_blocks_per_sm(s->batch, s->opts.blocks_per_sm);
+  *out = s;
+  return PBGPU_OK;
+}
+
+void pbgpu_server_destroy(pbgpu_server* s) {
+  if (!s) return;
+  if (s->batch) pbgpu_batch_destroy(s->batch);
+  for (Running& r : s->running) pbgpu_ctx_destroy(r.ctx);
+  for (pbgpu_ctx* c : s->idle) pbgpu_ctx_destroy(c);
+  delete s;
+}
+
+const char* pbgpu_server_last_error(const pbgpu_server* s) { return s ? s->err.c_str() : "null server"; }
+
+int pbgpu_server_submit(pbgpu_server* s, const pbgpu_request* req, int64_t* id) {
+  if (!s || !req || !req->mesh || !req->model || req->n_atoms < 0 || (req->n_atoms > 0 && (!req->pos || !req->charge)))
+    return PBGPU_ERR_ARG;
+  Pending p{s->next_id++, *req, Clock::now()};
+  s->queue.push_back(p);
+  if (id) *id = p.id;
+  return PBGPU_OK;
+}
+
+int pbgpu_server_pending(const pbgpu_server* s, int* queued, int* running, int64_t* device_bytes) {
+  if (!s) return PBGPU_ERR_ARG;
+  if (queued) *queued = (int)s->queue.size();
+  if (running) *running = (int)s->running.size();
+  if (device_bytes) {
+    int64_t b = 0;
+    for (const Running& r : s->running) b += ctx_bytes(r.ctx);
+    for (pbgpu_ctx* c : s->idle) b += ctx_bytes(c);
+    *device_bytes = b;
+  }
+  return PBGPU_OK;
+}
+
+// Inputs, markers, density map and SELL system of one request on `ctx`.
+static int setup_request(pbgpu_server* s, pbgpu_ctx* ctx, const pbgpu_request& r) {
+  int st;
+  if ((st = pbgpu_set_mesh(ctx, r.mesh)) != PBGPU_OK) return st;
+  for (int a = 0; a < 3; ++a)
+    if ((st = pbgpu_set_rays(ctx, a, &r.rays[a])) != PBGPU_OK) return st;
+  if ((st = pbgpu_set_atoms(ctx, r.n_atoms, r.pos, r.charge)) != PBGPU_OK) return st;
+  if ((st = pbgpu_set_model(ctx, r.model)) != PBGPU_OK) return st;
+  if ((st = pbgpu_create_markers(ctx)) != PBGPU_OK) return st;
+  if ((st = pbgpu_create_density_map(ctx)) != PBGPU_OK) return st;
+  pbgpu_sell_opts so{32, 2048, 4};
+  return pbgpu_assemble(ctx, &so);
+  (void)s;
+}
+
+static int64_t held_bytes(const pbgpu_server* s) {
+  int64_t b = 0;
+  for (const Running& r : s->running) b += ctx_bytes(r.ctx);
+  for (pbgpu_ctx* c : s->idle) b += ctx_bytes(c);
+  return b;
+}
+
+int pbgpu_server_progress(pbgpu_server* s, pbgpu_result* out, int cap, int* n_out) {
+  if (!s || (cap > 0 && !out)) return PBGPU_ERR_ARG;
+  if (n_out) *n_out = 0;
+  int st;
+  if (!s->in_session) {
+    if ((st = pbgpu_batch_begin(s->batch, &s->opts.solver)) != PBGPU_OK)
+      return s->fail(st, std::string("server: ") + pbgpu_batch_last_error(s->batch));
+    s->in_session = true;
+  }
+  // 1. admission
+  while (!s->queue.empty() && (int)s->running.size() < s->opts.max_members) {
+    const Pending& p = s->queue.front();
+    const int64_t need = pbgpu_request_bytes_estimate(&p.req);
+    // the idle context whose buffers are closest above the need, else the largest
+    int pick = -1;
+    for (size_t k = 0; k < s->idle.size(); ++k) {
+      const int64_t b = ctx_bytes(s->idle[k]);
+      if (pick < 0) {
+        pick = (int)k;
+        continue;
+      }
+      const int64_t bp = ctx_bytes(s->idle[pick]);
+      const bool fits = b >= need, fits_p = bp >= need;
+      if ((fits && (!fits_p || b < bp)) || (!fits && !fits_p && b > bp)) pick = (int)k;
+    }
+    int64_t held = held_bytes(s);
+    const int64_t reuse = pick >= 0 ? ctx_bytes(s->idle[pick]) : 0;
+    int64_t after = held - reuse + std::max(reuse, need);
+    // free idle contexts (largest first, never the picked one) until it fits
+    while (after > (int64_t)s->opts.hbm_budget_bytes) {
+      int big = -1;
+      for (size_t k = 0; k < s->idle.size(); ++k)
+        if ((int)k != pick && (big < 0 || ctx_bytes(s->idle[k]) > ctx_bytes(s->idle[big]))) big = (int)k;
+      if (big < 0) break;
+      after -= ctx_bytes(s->idle[big]);
+      pbgpu_ctx_destroy(s->idle[big]);
+      s->idle.erase(s->idle.begin() + big);
+      if (pick > big) --pick;
+    }
+    if (after > (int64_t)s->opts.hbm_budget_bytes && !s->running.empty()) break;  // wait for members to finish
+    pbgpu_ctx* ctx = nullptr;
+    if (pick >= 0) {
+      ctx = s->idle[pick];
+      s->idle.erase(s->idle.begin() + pick);
+    } else if ((st = pbgpu_ctx_create(&ctx, s->device, nullptr)) != PBGPU_OK) {
+      return s->fail(st, "server: context creation failed");
+    }
+    Running r{p.id, p.req.user_tag, -1, ctx, p.req.n_atoms, p.t_submit, Clock::now()};
+    st = setup_request(s, ctx, p.req);
+    if (st == PBGPU_OK) st = pbgpu_batch_add(s->batch, ctx, &r.slot);
+    if (st != PBGPU_OK) {
+      // the request fails alone: report it, keep serving
+      if (n_out && *n_out < cap) {
+        pbgpu_result& o = out[(*n_out)++];
+        std::memset(&o, 0, sizeof(o));
+        o.id = p.id;
+        o.user_tag = p.req.user_tag;
+        o.status = st;
+        o.latency_ms = ms_since(p.t_submit);
+      }
+      s->idle.push_back(ctx);
+      s->queue.pop_front();
+      continue;
+    }
+    s->running.push_back(r);
+    s->queue.pop_front();
+    ++s->admitted;
+  }
+  // 2. one persistent launch over all members
+  int active = 0;
+  if (!s->running.empty() && (st = pbgpu_batch_step(s->batch, s->opts.steps_per_tick, &active)) != PBGPU_OK)
+    return s->fail(st, std::string("server: ") + pbgpu_batch_last_error(s->batch));
+  // 3. retire converged members (as many as the output array holds)
+  for (size_t k = 0; k < s->running.size();) {
+    if (n_out && *n_out >= cap) break;
+    Running& r = s->running[k];
+    int done = 0;
+    pbgpu_solve_stats stats{};
+    if ((st = pbgpu_batch_member(s->batch, r.slot, &done, &stats)) != PBGPU_OK)
+      return s->fail(st, std::string("server: ") + pbgpu_batch_last_error(s->batch));
+    if (!done) {
+      ++k;
+      continue;
+    }
+    pbgpu_result& o = out[(*n_out)++];
+    std::memset(&o, 0, sizeof(o));
+    o.id = r.id;
+    o.user_tag = r.tag;
+    o.status = stats.status;
+    o.stats = stats;
+    if (stats.status == PBGPU_OK) o.status = pbgpu_energy(r.ctx, s->opts.energy_fast, &o.energy);
+    o.latency_ms = ms_since(r.t_submit);
+    o.queue_ms = std::chrono::duration<double, std::milli>(r.t_admit - r.t_submit).count();
+    pbgpu_batch_remove(s->batch, r.slot);
+    s->idle.push_back(r.ctx);
+    s->running.erase(s->running.begin() + k);
+    ++s->completed;
+  }
+  return PBGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,139 @@
+// SELL-C-sigma matrix view, the per-row product and the block reduction shared
+// by the single-system Krylov kernels (k_krylov.cu) and the multi-system
+// persistent kernels (k_batch.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "pbgpu_internal.cuh"
+
+namespace pbgpu {
+
+constexpr int kBlock = 256;
+// resident blocks per SM the direct SpMV kernels are compiled for
+// (registers <= 65536 / (256 * blocks)): 4, i.e. 64 registers, which the
+// grouped loads and up to four fused reductions need without spills
+constexpr int kSpmvMinBlocks = 4;
+constexpr int kSpmvMinBlocksWide = 4;
+
+template <typename T>
+struct SellT {
+  const int64_t* slice_ptr;
+  const int32_t* slice_w;
+  const int32_t* scol;
+  const T* sval;
+  int64_t n_pad;
+  int C;
+  int G;  // columns per row stored contiguously: 1, 2 or 4
+};
+
+template <typename T>
+struct V2 {};
+template <>
+struct V2<double> {
+  using t = double2;
+};
+template <>
+struct V2<float> {
+  using t = float2;
+};
+
+// y_p = sum_j A(p, j) x_j for SELL row p, element j at sell_elem(): the
+// first W - W % G columns in groups of G (one vector load per group, a warp's
+// loads of one group contiguous), the remaining W % G columns one per lane.
+// (W and sb: width and first element of the row's slice)
+template <typename T, int G>
+__device__ __forceinline__ T sell_row(const SellT<T>& A, int64_t p, const T* __restrict__ x, int W, int64_t sb) {
+  const int lane = (int)(p % A.C);
+  T acc = 0;
+  if constexpr (G == 1) {
+    const int64_t base = sb + lane;
+    const int64_t stride = A.C;
+#pragma unroll 4
+    for (int j = 0; j < W; ++j) {
+      const int64_t k = base + j * stride;
+      acc += __ldcs(A.sval + k) * x[__ldcs(A.scol + k)];
+    }
+    return acc;
+  } else if constexpr (G == 2) {
+    const int64_t base = sb + 2 * lane;
+    const int64_t stride = 2 * (int64_t)A.C;
+#pragma unroll 2
+    for (int g = 0; g < (W >> 1); ++g) {
+      const int64_t k = base + g * stride;
+      const int2 c = __ldcs(reinterpret_cast<const int2*>(A.scol + k));
+      const typename V2<T>::t v = __ldcs(reinterpret_cast<const typename V2<T>::t*>(A.sval + k));
+      acc += v.x * x[c.x];
+      acc += v.y * x[c.y];
+    }
+  } else {
+    const int64_t base = sb + 4 * lane;
+    const int64_t stride = 4 * (int64_t)A.C;
+#pragma unroll 2
+    for (int g = 0; g < (W >> 2); ++g) {
+      const int64_t k = base + g * stride;
+      const int4 c = __ldcs(reinterpret_cast<const int4*>(A.scol + k));
+      if constexpr (sizeof(T) == 8) {
+        const double2 v0 = __ldcs(reinterpret_cast<const double2*>(A.sval + k));
+        const double2 v1 = __ldcs(reinterpret_cast<const double2*>(A.sval + k + 2));
+        acc += v0.x * x[c.x];
+        acc += v0.y * x[c.y];
+        acc += v1.x * x[c.z];
+        acc += v1.y * x[c.w];
+      } else {
+        const float4 v = __ldcs(reinterpret_cast<const float4*>(A.sval + k));
+        acc += v.x * x[c.x];
+        acc += v.y * x[c.y];
+        acc += v.z * x[c.z];
+        acc += v.w * x[c.w];
+      }
+    }
+  }
+  // tail columns, one per lane
+  const int Wg = W - W % G;
+  const int64_t tb = sb + (int64_t)Wg * A.C + lane;
+  for (int j = Wg; j < W; ++j) {
+    const int64_t k = tb + (int64_t)(j - Wg) * A.C;
+    acc += __ldcs(A.sval + k) * x[__ldcs(A.scol + k)];
+  }
+  return acc;
+}
+
+template <typename T, int G>
+__device__ __forceinline__ T sell_row(const SellT<T>& A, int64_t p, const T* __restrict__ x) {
+  const int64_t s = p / A.C;
+  return sell_row<T, G>(A, p, x, A.slice_w[s], A.slice_ptr[s]);
+}
+
+// fn(i, (A x)_i) for the rows of this thread (grid-stride loop).  (Loading
+// the next row's slice metadata ahead of the current row measured slower for
+// G = 4: it costs registers the gathers need.)
+template <typename T, int G, typename Fn>
+__device__ __forceinline__ void spmv_direct_rows(const SellT<T>& A, const T* __restrict__ x, Fn&& fn) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x)
+    fn(i, sell_row<T, G>(A, i, x));
+}
+
+// Block-wide sum of K values; result valid in thread 0.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K]) {
+  __shared__ double sh[K][kBlock / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double a = v[k];
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if (lane == 0) sh[k][wid] = a;
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double a = lane < kBlock / 32 ? sh[k][lane] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+      v[k] = a;
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace pbgpu

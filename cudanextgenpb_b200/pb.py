@@ -221,7 +221,7 @@ class GpuPath:
     def create_density_map(self):
         self._check(self._lib.pbgpu_create_density_map(self._ctx))
 
-    def assemble(self, chunk=32, sigma=2048, group=1):
+    def assemble(self, chunk=32, sigma=2048, group=4):
         """SELL-C-sigma layout: slice height `chunk`, length-sorting window
         `sigma` rows, `group` columns stored contiguously per row."""
         o = N.PbgpuSellOpts(chunk, sigma, group)
@@ -304,10 +304,162 @@ class GpuPath:
     def reset_counters(self):
         self._check(self._lib.pbgpu_reset_counters(self._ctx))
 
-    def run(self, opts=None, fast=False, chunk=32, sigma=2048, group=1):
+    def run(self, opts=None, fast=False, chunk=32, sigma=2048, group=4):
         """create_markers .. energy in the driver's order; returns (energy dict, solve stats)."""
         self.create_markers()
         self.create_density_map()
         self.assemble(chunk, sigma, group)
         st = self.solve(opts)
         return self.energy(fast), st
+
+
+class Batch:
+    """Many assembled GpuPath systems solved together by one persistent
+    cooperative kernel per chunk of iterations (pbgpu_batch_*)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self._lib = N.load_gpu()
+        self._b = C.c_void_p()
+        st = self._lib.pbgpu_batch_create(C.byref(self._b), device, C.c_void_p(stream) if stream else None)
+        if st != 0:
+            raise PBError(st, "pbgpu_batch_create failed")
+        self.members: dict[int, GpuPath] = {}
+
+    def _check(self, st, ok=(0,)):
+        if st not in ok:
+            raise PBError(st, self._lib.pbgpu_batch_last_error(self._b).decode())
+
+    def add(self, g: GpuPath) -> int:
+        slot = C.c_int()
+        self._check(self._lib.pbgpu_batch_add(self._b, g._ctx, C.byref(slot)))
+        self.members[slot.value] = g
+        return slot.value
+
+    def remove(self, slot: int):
+        self._check(self._lib.pbgpu_batch_remove(self._b, slot))
+        del self.members[slot]
+
+    def solve(self, opts: N.PbgpuSolverOpts | None = None, allow_not_converged=False) -> dict:
+        n = max(self.members) + 1 if self.members else 0
+        stats = (N.PbgpuSolveStats * max(n, 1))()
+        ok = (0, N.PBGPU_NOT_CONVERGED) if allow_not_converged else (0,)
+        self._check(self._lib.pbgpu_batch_solve(self._b, C.byref(opts) if opts else None, stats), ok)
+        return {k: stats[k] for k in self.members}
+
+    def begin(self, opts: N.PbgpuSolverOpts | None = None):
+        self._check(self._lib.pbgpu_batch_begin(self._b, C.byref(opts) if opts else None))
+
+    def step(self, steps: int) -> int:
+        """One persistent launch of up to `steps` steps; returns the members not done."""
+        n = C.c_int()
+        self._check(self._lib.pbgpu_batch_step(self._b, steps, C.byref(n)))
+        return n.value
+
+    def member(self, slot: int):
+        """(done, stats) of a member; when done its potential is in its context."""
+        done, st = C.c_int(), N.PbgpuSolveStats()
+        self._check(self._lib.pbgpu_batch_member(self._b, slot, C.byref(done), C.byref(st)))
+        return bool(done.value), st
+
+    def set_blocks_per_sm(self, blocks: int):
+        self._check(self._lib.pbgpu_batch_set_blocks_per_sm(self._b, blocks))
+
+    def close(self):
+        if self._b:
+            self._lib.pbgpu_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching PB solve server on one GPU (pbgpu_server_*).
+
+    submit(problem) queues one molecule (its host arrays stay referenced until
+    its result comes back); progress() runs one tick and returns finished
+    requests as dicts."""
+
+    def __init__(self, device: int = 0, opts: N.PbgpuServerOpts | None = None, **kw):
+        self._lib = N.load_gpu()
+        if opts is None:
+            opts = N.PbgpuServerOpts()
+            self._lib.pbgpu_default_server_opts(C.byref(opts))
+        for k, v in kw.items():
+            if k in ("tol", "inner_tol", "max_iter", "precision", "check_every"):
+                if k == "precision":
+                    v = {"fp64": N.PBGPU_FP64, "mixed": N.PBGPU_MIXED}[v]
+                setattr(opts.solver, k, v)
+            else:
+                setattr(opts, k, v)
+        self.opts = opts
+        self._s = C.c_void_p()
+        st = self._lib.pbgpu_server_create(C.byref(self._s), device, C.byref(opts))
+        if st != 0:
+            raise PBError(st, "pbgpu_server_create failed")
+        self._keep: dict[int, tuple] = {}
+        self._out = (N.PbgpuResult * 256)()
+
+    def _check(self, st):
+        if st != 0:
+            raise PBError(st, self._lib.pbgpu_server_last_error(self._s).decode())
+
+    def request(self, prob: Problem, pos=None, q=None, tag: int = 0) -> N.PbgpuRequest:
+        """The request structure of a built host problem (optionally with other
+        charges on the same atoms)."""
+        m = prob.mesh_struct()
+        p0, q0, _ = prob.atoms()
+        pos = np.ascontiguousarray(p0 if pos is None else pos, dtype=np.float64).reshape(-1, 3)
+        q = np.ascontiguousarray(q0 if q is None else q, dtype=np.float64)
+        md = prob.model()
+        r = N.PbgpuRequest()
+        r.mesh = C.pointer(m)
+        for a in range(3):
+            r.rays[a] = prob.rays_struct(a)
+        r.n_atoms = len(q)
+        r.pos = _dptr(pos)
+        r.charge = _dptr(q)
+        r.model = C.pointer(md)
+        r.user_tag = tag
+        r._keep = (m, pos, q, md, prob)
+        return r
+
+    def submit(self, req: N.PbgpuRequest) -> int:
+        i = C.c_int64()
+        self._check(self._lib.pbgpu_server_submit(self._s, C.byref(req), C.byref(i)))
+        self._keep[i.value] = (req, req._keep)
+        return i.value
+
+    def progress(self) -> list[dict]:
+        n = C.c_int()
+        self._check(self._lib.pbgpu_server_progress(self._s, self._out, len(self._out), C.byref(n)))
+        res = []
+        for k in range(n.value):
+            r = self._out[k]
+            self._keep.pop(r.id, None)
+            res.append({"id": r.id, "tag": r.user_tag, "status": r.status, "energy": r.energy.as_dict(),
+                        "iterations": r.stats.iterations, "outer": r.stats.outer,
+                        "rel_residual": r.stats.rel_residual, "latency_ms": r.latency_ms, "queue_ms": r.queue_ms})
+        return res
+
+    def pending(self):
+        q, r, b = C.c_int(), C.c_int(), C.c_int64()
+        self._check(self._lib.pbgpu_server_pending(self._s, C.byref(q), C.byref(r), C.byref(b)))
+        return q.value, r.value, b.value
+
+    def estimate(self, req: N.PbgpuRequest) -> int:
+        return int(self._lib.pbgpu_request_bytes_estimate(C.byref(req)))
+
+    def close(self):
+        if self._s:
+            self._lib.pbgpu_server_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

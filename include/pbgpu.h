@@ -100,8 +100,10 @@ typedef struct {
 typedef struct {
   int chunk;                 /* SELL slice height C (multiple of 32; 0 = default 32) */
   int sigma;                 /* sorting window in rows (1 or a multiple of chunk; 0 = default 2048) */
-  int group;                 /* columns stored contiguously per row: 1, 2 or 4 (0 = default 1);
-                                a thread loads `group` values with one load instruction */
+  int group;                 /* columns stored contiguously per row: 1, 2 or 4 (0 = default 4);
+                                a thread loads `group` values with one load instruction;
+                                with chunk 32, group 1 selects the SpMV that stages slices
+                                through shared memory by bulk async copies */
 } pbgpu_sell_opts;
 
 typedef struct {
@@ -210,6 +212,7 @@ typedef struct {
   int64_t krylov_iterations;
   int64_t energy_points;     /* distinct surface points of the last energy call */
   int64_t energy_pairs;      /* surface point x charged atom pairs evaluated */
+  int64_t device_bytes;      /* device memory the context holds now */
 } pbgpu_counters;
 int pbgpu_set_profiling(pbgpu_ctx* ctx, int on);
 int pbgpu_get_counters(pbgpu_ctx* ctx, pbgpu_counters* out);
@@ -236,6 +239,92 @@ int pbgpu_reset_counters(pbgpu_ctx* ctx);
  * calls whose work overlaps on the GPU race and must be serialised. */
 int pbgpu_coulomb_energy_static(const double* atoms, int64_t n_atoms, double e_in, double T, double* out_energy,
                                 void* cuda_stream);
+
+/* ---- batches: many systems, one persistent launch ------------------------
+ * No counterpart in the reference, which solves one system per process
+ * (lis_compute_electric_potential, src/pb_class.cpp:2244-2329).  A batch holds
+ * contexts whose systems are assembled (pbgpu_assemble with chunk 32 and
+ * group 4) and solves them together: one persistent cooperative kernel per
+ * chunk of check_every iterations advances every member (Jacobi CG, FP64 or
+ * FP32-inner / FP64-refined, per-member scalars, convergence and
+ * deterministic reductions).  After pbgpu_batch_solve every member context
+ * holds its potential, so pbgpu_phi_on_atoms / pbgpu_energy run on it as
+ * after pbgpu_solve.  A member context must not be used by other calls while
+ * a batch call runs.  Results equal the member's own pbgpu_solve within the
+ * solve tolerance. */
+typedef struct pbgpu_batch pbgpu_batch;
+int pbgpu_batch_create(pbgpu_batch** out, int device, void* cuda_stream);
+void pbgpu_batch_destroy(pbgpu_batch* batch);
+const char* pbgpu_batch_last_error(const pbgpu_batch* batch);
+/* adds an assembled context; *slot receives its index (the lowest free one) */
+int pbgpu_batch_add(pbgpu_batch* batch, pbgpu_ctx* ctx, int* slot);
+int pbgpu_batch_remove(pbgpu_batch* batch, int slot);
+int pbgpu_batch_size(const pbgpu_batch* batch);
+/* opts: method PBGPU_CG, precond PBGPU_PRECOND_JACOBI, conv_cond 0 or 1;
+ * stats: NULL or one entry per slot index (members only are written) */
+int pbgpu_batch_solve(pbgpu_batch* batch, const pbgpu_solver_opts* opts, pbgpu_solve_stats* stats);
+/* Incremental use (continuous batching): begin fixes the options and starts
+ * every member afresh; each step call runs one persistent launch of up to
+ * `steps` steps (a step is one inner CG iteration of every member in its inner
+ * phase) and reports the members not yet done.  Members added after begin
+ * start at the next step; a member reported done by pbgpu_batch_member has its
+ * potential in its context and can be removed. */
+int pbgpu_batch_begin(pbgpu_batch* batch, const pbgpu_solver_opts* opts);
+int pbgpu_batch_step(pbgpu_batch* batch, int steps, int* n_active);
+int pbgpu_batch_member(pbgpu_batch* batch, int slot, int* done, pbgpu_solve_stats* stats);
+/* resident blocks per SM of the persistent kernel (0: as many as fit); fewer
+ * leave room for other streams' kernels to run beside it */
+int pbgpu_batch_set_blocks_per_sm(pbgpu_batch* batch, int blocks);
+
+/* ---- server: continuous batching of PB solves ----------------------------
+ * No counterpart in the reference.  Requests (one molecule each: mesh, rays,
+ * atoms, model) are queued by pbgpu_server_submit; every
+ * pbgpu_server_progress call admits queued requests FIFO while max_members and
+ * the HBM budget allow (device bytes held by all contexts plus an estimate for
+ * the request), builds their systems on their own contexts, advances all
+ * member systems with one persistent multi-system launch, and returns the
+ * requests that finished (energies, solve statistics, latency).  The arrays a
+ * request points to must stay valid until its result is returned. */
+typedef struct {
+  const pbgpu_mesh* mesh;
+  pbgpu_rays rays[3];
+  int64_t n_atoms;
+  const double* pos;         /* 3 n_atoms */
+  const double* charge;      /* n_atoms */
+  const pbgpu_model* model;
+  int64_t user_tag;
+} pbgpu_request;
+
+typedef struct {
+  int64_t id;                /* from pbgpu_server_submit */
+  int64_t user_tag;
+  int status;
+  pbgpu_energy_out energy;
+  pbgpu_solve_stats stats;
+  double latency_ms;         /* submit to completion (host wall clock) */
+  double queue_ms;           /* submit to admission */
+} pbgpu_result;
+
+typedef struct {
+  double hbm_budget_bytes;   /* device memory all server contexts may hold (default 160e9) */
+  int max_members;           /* systems solved at once (default 64) */
+  int steps_per_tick;        /* persistent-kernel steps per progress call (default 32) */
+  int blocks_per_sm;         /* persistent kernel residency (default 2; 0: as many as fit) */
+  pbgpu_solver_opts solver;  /* CG + Jacobi; PBGPU_MIXED by default (FP32 inner, FP64 refined) */
+  int energy_fast;           /* 1: energy_fast, 0: energy */
+} pbgpu_server_opts;
+
+typedef struct pbgpu_server pbgpu_server;
+void pbgpu_default_server_opts(pbgpu_server_opts* opts);
+int pbgpu_server_create(pbgpu_server** out, int device, const pbgpu_server_opts* opts);
+void pbgpu_server_destroy(pbgpu_server* server);
+const char* pbgpu_server_last_error(const pbgpu_server* server);
+int pbgpu_server_submit(pbgpu_server* server, const pbgpu_request* request, int64_t* id);
+/* one tick; writes up to `cap` finished requests to out[0 .. *n_out) */
+int pbgpu_server_progress(pbgpu_server* server, pbgpu_result* out, int cap, int* n_out);
+int pbgpu_server_pending(const pbgpu_server* server, int* queued, int* running, int64_t* device_bytes);
+/* device bytes the server plans for a request before it holds any */
+int64_t pbgpu_request_bytes_estimate(const pbgpu_request* request);
 
 #ifdef __cplusplus
 }
