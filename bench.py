@@ -221,14 +221,25 @@ def run_ours(args, rank, world, local):
     g = GpuPath(local).load(prob)
     # time on the context's own stream
     stream = torch.cuda.ExternalStream(g.stream_ptr(), device=local)
-    opts = solver_opts("cg", tol=args.tol, max_iter=50000, precond=args.precond)
+    opts = solver_opts("cg", tol=args.tol, max_iter=50000, precond=args.precond, precision=args.precision)
     info = prob.info()
+
+    batch = None
+    if args.via_batch:
+        from cudanextgenpb_b200 import Batch
+        batch = Batch(local)
+        opts = solver_opts("cg", tol=args.tol, max_iter=50000, precision=args.precision, check_every=64)
 
     def step():
         g.create_markers()
         g.create_density_map()
         g.assemble(args.chunk, args.sigma, args.group)
-        st = g.solve(opts)
+        if batch is not None:
+            batch.add(g)
+            st = batch.solve(opts)[0]
+            batch.remove(0)
+        else:
+            st = g.solve(opts)
         pa = g.phi_on_atoms()
         e = g.energy(False)
         return st, e, pa
@@ -335,13 +346,14 @@ def run_ours(args, rank, world, local):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64",
+            "dtype": "f64" if args.precision == "fp64" else "f32-inner/f64",
             "data": "synthetic",
             "config": {
                 "workload": workload_desc(args.workload, info),
                 "n_dof": info["n_nodes"], "n_octants": info["n_oct"], "n_hanging": info["n_hang"],
                 "n_atoms": info["n_atoms"], "nnz": info_nnz(g), "cg_iterations": int(np.median(iters)),
-                "tol": args.tol, "precond": args.precond,
+                "tol": args.tol, "precond": args.precond, "precision": args.precision,
+                "solver_path": "persistent multi-system kernel" if args.via_batch else "captured CUDA graph of kernels",
                 "sell": {"C": args.chunk, "sigma": args.sigma, "group": args.group},
                 "energy_kT": energies[-1],
                 "dof_iterations_per_s": world * info["n_nodes"] * float(np.median(iters)) / (ms / 1e3 / args.steps),
@@ -668,6 +680,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mol2000", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(SERVES))
     ap.add_argument("--max-members", type=int, default=64)
+    ap.add_argument("--via-batch", action="store_true", help="solve through the persistent multi-system kernel")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--chunk", type=int, default=32)

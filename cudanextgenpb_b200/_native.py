@@ -73,7 +73,8 @@ class PbgpuResult(C.Structure):
 
 class PbgpuServerOpts(C.Structure):
     _fields_ = [("hbm_budget_bytes", dbl), ("max_members", C.c_int), ("steps_per_tick", C.c_int),
-                ("blocks_per_sm", C.c_int), ("solver", PbgpuSolverOpts), ("energy_fast", C.c_int)]
+                ("blocks_per_sm", C.c_int), ("solver", PbgpuSolverOpts), ("energy_fast", C.c_int),
+                ("admit_per_tick", C.c_int)]
 
 
 class PbhostInfo(C.Structure):
@@ -123,6 +124,9 @@ PBGPU_FUNCS = {
     "pbgpu_get_counters": (C.c_int, [ctx_p, P(PbgpuCounters)]),
     "pbgpu_reset_counters": (C.c_int, [ctx_p]),
     "pbgpu_coulomb_energy_static": (C.c_int, [C.c_void_p, i64, dbl, dbl, C.c_void_p, C.c_void_p]),
+    "pbgpu_autotune": (C.c_int, [ctx_p, C.c_int, P(PbgpuSellOpts), P(C.c_int), P(dbl)]),
+    "pbgpu_solve_charges": (C.c_int, [ctx_p, C.c_int, P(dbl), P(PbgpuSolverOpts), C.c_int, P(PbgpuEnergyOut),
+                                      P(PbgpuSolveStats)]),
     "pbgpu_batch_create": (C.c_int, [P(C.c_void_p), C.c_int, C.c_void_p]),
     "pbgpu_batch_destroy": (None, [C.c_void_p]),
     "pbgpu_batch_last_error": (C.c_char_p, [C.c_void_p]),
@@ -134,6 +138,8 @@ PBGPU_FUNCS = {
     "pbgpu_batch_step": (C.c_int, [C.c_void_p, C.c_int, P(C.c_int)]),
     "pbgpu_batch_member": (C.c_int, [C.c_void_p, C.c_int, P(C.c_int), P(PbgpuSolveStats)]),
     "pbgpu_batch_set_blocks_per_sm": (C.c_int, [C.c_void_p, C.c_int]),
+    "pbgpu_batch_launch": (C.c_int, [C.c_void_p, C.c_int]),
+    "pbgpu_batch_wait": (C.c_int, [C.c_void_p, P(C.c_int)]),
     "pbgpu_default_server_opts": (None, [P(PbgpuServerOpts)]),
     "pbgpu_server_create": (C.c_int, [P(C.c_void_p), C.c_int, P(PbgpuServerOpts)]),
     "pbgpu_server_destroy": (None, [C.c_void_p]),

@@ -279,6 +279,8 @@ __device__ __forceinline__ int64_t sell_index(const SellOut& S, int64_t p, int W
 // Pass 2: values, columns (SELL numbering), right-hand side, 1/diagonal.
 // One thread per SELL position p < n (row perm[p]), so the 32 lanes of a warp
 // fill one slice and every store of element j is one contiguous warp store.
+// RHS_ONLY: the right-hand side alone (new charges on an assembled system).
+template <bool RHS_ONLY>
 __global__ void k_row_fill(AsmView A, LocalView L, SellOut S) {
   const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p >= A.n) return;
@@ -286,10 +288,11 @@ __global__ void k_row_fill(AsmView A, LocalView L, SellOut S) {
   const int W = S.slice_w[p / S.C];
   int j = 0;
   if (A.dirichlet[i]) {
+    S.b[p] = A.gval[i];
+    if (RHS_ONLY) return;
     const int64_t k = sell_index(S, p, W, j++);
     S.scol[k] = (int32_t)p;
     S.sval[k] = 1.0;
-    S.b[p] = A.gval[i];
     S.dinv[p] = 1.0;
   } else {
     RowAcc R;
@@ -302,12 +305,14 @@ __global__ void k_row_fill(AsmView A, LocalView L, SellOut S) {
         rhs -= R.val[u] * A.gval[cn];
         continue;
       }
+      if (RHS_ONLY) continue;
       if (cn == i) diag = R.val[u];
       const int64_t k = sell_index(S, p, W, j++);
       S.scol[k] = S.iperm[cn];
       S.sval[k] = R.val[u];
     }
     S.b[p] = rhs;
+    if (RHS_ONLY) return;
     S.dinv[p] = 1.0 / diag;
   }
   for (; j < W; ++j) {
@@ -400,6 +405,32 @@ __global__ void k_slice_width(const int32_t* __restrict__ perm, const int32_t* _
   elems[s] = (int64_t)mx * C;
 }
 
+// The assembly's view of a context (dirichlet / gval must be current).
+static AsmView asm_view(Context* c) {
+  AsmView A;
+  A.inc_ptr = c->inc_ptr.get();
+  A.inc = c->inc.get();
+  A.oct = c->oct.get();
+  A.oct_nodes = c->oct_nodes.get();
+  A.hang_par = c->hang_par.get();
+  A.hang_np = c->hang_np.get();
+  A.eps = c->eps.get();
+  A.react = c->react.get();
+  A.react_cell = c->model.stern_layer_surf == 1 ? c->react_cell.get() : nullptr;
+  A.rho = c->rho.get();
+  A.frac = c->frac.get();
+  A.border_pos = c->border_pos.get();
+  A.dirichlet = c->dirichlet.get();
+  A.gval = c->gval.get();
+  A.n = c->n;
+  A.stern = c->model.stern_layer_surf == 1;
+  for (int d = 0; d < 3; ++d) {
+    A.lo[d] = c->lo[d];
+    A.len[d] = c->len[d];
+  }
+  return A;
+}
+
 int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   if (!c->have_markers) return c->fail(PBGPU_ERR_STATE, "assemble: create_markers has not run");
   if (!c->have_density) return c->fail(PBGPU_ERR_STATE, "assemble: create_density_map has not run");
@@ -422,28 +453,7 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
                                                         c->dirichlet.get(), c->gval.get());
   PBGPU_LAUNCHED(c);
 
-  AsmView A;
-  A.inc_ptr = c->inc_ptr.get();
-  A.inc = c->inc.get();
-  A.oct = c->oct.get();
-  A.oct_nodes = c->oct_nodes.get();
-  A.hang_par = c->hang_par.get();
-  A.hang_np = c->hang_np.get();
-  A.eps = c->eps.get();
-  A.react = c->react.get();
-  A.react_cell = c->model.stern_layer_surf == 1 ? c->react_cell.get() : nullptr;
-  A.rho = c->rho.get();
-  A.frac = c->frac.get();
-  A.border_pos = c->border_pos.get();
-  A.dirichlet = c->dirichlet.get();
-  A.gval = c->gval.get();
-  A.n = n;
-  A.stern = c->model.stern_layer_surf == 1;
-  for (int d = 0; d < 3; ++d) {
-    A.lo[d] = c->lo[d];
-    A.len[d] = c->len[d];
-  }
-
+  const AsmView A = asm_view(c);
   PBGPU_CUDA(c, c->rowlen.alloc(n));
   Scratch<int> ovf(c, kScAsmOvf);
   PBGPU_CUDA(c, ovf.alloc(1));
@@ -524,7 +534,7 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   k_octant_local<<<grid_for(c->n_oct, 128), 128, 0, c->stream>>>(A, c->n_oct, ocond.get(), okd.get(), ofr.get());
   PBGPU_LAUNCHED(c);
   const LocalView L{ocond.get(), okd.get(), ofr.get()};
-  k_row_fill<<<grid_for(n, 128), 128, 0, c->stream>>>(A, L, S);
+  k_row_fill<false><<<grid_for(n, 128), 128, 0, c->stream>>>(A, L, S);
   PBGPU_LAUNCHED(c);
   if (n_pad > n) {
     k_pad_rows<<<grid_for(n_pad - n, 128), 128, 0, c->stream>>>(S, n, n_pad);
@@ -534,6 +544,35 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   c->have_system = true;
   c->bj_ready = false;
   c->have_phi = false;
+  return PBGPU_OK;
+}
+
+// Right-hand side of the assembled system for the context's current atoms and
+// density map (the matrix does not depend on the charges): Dirichlet values,
+// the octants' V/8 rho terms and the eliminated Dirichlet columns, summed as
+// in the full assembly.
+int run_rhs(Context* c) {
+  if (!c->have_system) return c->fail(PBGPU_ERR_STATE, "rhs: assemble has not run");
+  if (!c->have_density) return c->fail(PBGPU_ERR_STATE, "rhs: create_density_map has not run");
+  const int64_t n = c->n;
+  const double3 lo = make_double3(c->lo[0], c->lo[1], c->lo[2]);
+  const double3 len = make_double3(c->len[0], c->len[1], c->len[2]);
+  k_dirichlet<<<grid_for(n, 128), 128, 0, c->stream>>>(c->node_xyz.get(), n, c->model.bc_type, lo, len,
+                                                        c->atoms.get(), c->na, c->eps_in, c->eps_out, c->kappa,
+                                                        c->dirichlet.get(), c->gval.get());
+  PBGPU_LAUNCHED(c);
+  const AsmView A = asm_view(c);
+  SellOut S{c->slice_ptr.get(), c->slice_w.get(), c->iperm.get(), c->perm.get(), c->scol.get(), c->sval.get(),
+            c->b.get(), c->dinv.get(), c->C, c->G};
+  Scratch<double> ocond(c, kScAsmCond), okd(c, kScAsmKd), ofr(c, kScAsmFr);
+  PBGPU_CUDA(c, ocond.alloc(12 * c->n_oct));
+  PBGPU_CUDA(c, okd.alloc(8 * c->n_oct));
+  PBGPU_CUDA(c, ofr.alloc(8 * c->n_oct));
+  k_octant_local<<<grid_for(c->n_oct, 128), 128, 0, c->stream>>>(A, c->n_oct, ocond.get(), okd.get(), ofr.get());
+  PBGPU_LAUNCHED(c);
+  const LocalView L{ocond.get(), okd.get(), ofr.get()};
+  k_row_fill<true><<<grid_for(n, 128), 128, 0, c->stream>>>(A, L, S);
+  PBGPU_LAUNCHED(c);
   return PBGPU_OK;
 }
 

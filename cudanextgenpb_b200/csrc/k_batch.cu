@@ -388,6 +388,11 @@ struct pbgpu_batch {
   DBuf<GridBar> bar;
   BState* st_host = nullptr;
   size_t st_cap = 0;
+  GridBar* bar_host = nullptr;      // pinned copy of the barrier state
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool in_flight = false;           // a launch whose states are not yet read
+  bool kernel_in_flight = false;
+  int flight_members = 0;
   int64_t launches = 0;
   float last_ms = 0.f;
   int fail(int code, const std::string& m) {
@@ -549,15 +554,25 @@ int upload_tables(pbgpu_batch* B) {
   return PBGPU_OK;
 }
 
+// Launches one persistent kernel of up to `steps` steps over the current
+// members and queues the copy of their states to the host; returns without
+// waiting (batch_wait completes it).
 template <typename TI>
-int batch_step(pbgpu_batch* B, int steps, int* n_active) {
+int batch_launch(pbgpu_batch* B, int steps) {
   int rc;
   if ((rc = ensure_capacity(B)) != PBGPU_OK) return rc;
   for (size_t k = 0; k < B->slots.size(); ++k)
     if (B->slots[k] && B->pending[k] && (rc = prepare_member<TI>(B, (int)k)) != PBGPU_OK) return rc;
   if (B->dirty && (rc = upload_tables<TI>(B)) != PBGPU_OK) return rc;
   const int nm = (int)B->slots.size();
-  int active = 0;
+  B->flight_members = nm;
+  if (!B->ev0) {
+    BATCH_CUDA(B, cudaEventCreate(&B->ev0));
+    BATCH_CUDA(B, cudaEventCreate(&B->ev1));
+    BATCH_CUDA(B, cudaMallocHost(&B->bar_host, sizeof(GridBar)));
+  }
+  B->bar_host->err = 0;
+  B->kernel_in_flight = false;
   if (B->n_rb > 0 && steps > 0) {
     if (!B->bar.get()) {
       BATCH_CUDA(B, B->bar.alloc(1));
@@ -581,31 +596,34 @@ int batch_step(pbgpu_batch* B, int steps, int* n_active) {
     GridBar* a_bar = B->bar.get();
     int a_steps = steps;
     void* args[] = {&a_mem, &a_nm, &a_rb, &a_nrb, &a_st, &a_part, &a_bar, &a_steps};
-    cudaEvent_t e0, e1;
-    BATCH_CUDA(B, cudaEventCreate(&e0));
-    BATCH_CUDA(B, cudaEventCreate(&e1));
-    cudaEventRecord(e0, B->stream);
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_batch_cg<TI>, dim3(grid), dim3(kBlock), args, 0,
-                                                B->stream);
-    if (e == cudaSuccess) B->launches += 1;
-    cudaEventRecord(e1, B->stream);
-    GridBar hb{};
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(B->st_host, B->st.get(), nm * sizeof(BState), cudaMemcpyDeviceToHost, B->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&hb, B->bar.get(), sizeof(GridBar), cudaMemcpyDeviceToHost, B->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
-    float ms = 0.f;
-    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (e != cudaSuccess) return bfail(B, e, "batch: persistent kernel");
-    B->last_ms += ms;
-    if (hb.err) return B->fail(PBGPU_TIMEOUT, "batch: grid barrier wait timed out");
-  } else {
-    BATCH_CUDA(B, cudaMemcpyAsync(B->st_host, B->st.get(), nm * sizeof(BState), cudaMemcpyDeviceToHost, B->stream));
-    BATCH_CUDA(B, cudaStreamSynchronize(B->stream));
+    BATCH_CUDA(B, cudaEventRecord(B->ev0, B->stream));
+    BATCH_CUDA(B, cudaLaunchCooperativeKernel((const void*)k_batch_cg<TI>, dim3(grid), dim3(kBlock), args, 0,
+                                              B->stream));
+    B->launches += 1;
+    BATCH_CUDA(B, cudaEventRecord(B->ev1, B->stream));
+    BATCH_CUDA(B, cudaMemcpyAsync(B->bar_host, B->bar.get(), sizeof(GridBar), cudaMemcpyDeviceToHost, B->stream));
+    B->kernel_in_flight = true;
   }
-  for (int k = 0; k < nm; ++k) active += B->slots[k] && B->st_host[k].phase != kPhDone;
+  BATCH_CUDA(B, cudaMemcpyAsync(B->st_host, B->st.get(), nm * sizeof(BState), cudaMemcpyDeviceToHost, B->stream));
+  B->in_flight = true;
+  return PBGPU_OK;
+}
+
+int batch_wait(pbgpu_batch* B, int* n_active) {
+  if (B->in_flight) {
+    B->in_flight = false;
+    BATCH_CUDA(B, cudaStreamSynchronize(B->stream));
+    if (B->kernel_in_flight) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, B->ev0, B->ev1) == cudaSuccess) B->last_ms += ms;
+      B->kernel_in_flight = false;
+      if (B->bar_host->err) return B->fail(PBGPU_TIMEOUT, "batch: grid barrier wait timed out");
+    }
+  }
+  int active = 0;
+  for (int k = 0; k < B->flight_members && (size_t)k < B->slots.size(); ++k)
+    active += B->slots[k] && !B->pending[k] && B->st_host[k].phase != kPhDone;
+  for (size_t k = 0; k < B->slots.size(); ++k) active += B->slots[k] && B->pending[k];
   if (n_active) *n_active = active;
   return PBGPU_OK;
 }
@@ -685,6 +703,9 @@ void pbgpu_batch_destroy(pbgpu_batch* b) {
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->st_host) cudaFreeHost(b->st_host);
+  if (b->bar_host) cudaFreeHost(b->bar_host);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
   cudaStream_t s = b->stream;
   const bool own = b->own_stream;
   delete b;
@@ -719,6 +740,7 @@ int pbgpu_batch_add(pbgpu_batch* b, pbgpu_ctx* ctx, int* slot) {
 
 int pbgpu_batch_remove(pbgpu_batch* b, int slot) {
   if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot]) return PBGPU_ERR_ARG;
+  if (b->in_flight) return b->fail(PBGPU_ERR_STATE, "batch_remove: a launch is in flight (pbgpu_batch_wait)");
   b->slots[slot] = nullptr;
   b->pending[slot] = 0;
   if (b->st_host && (size_t)slot < b->st_cap) {
@@ -755,6 +777,7 @@ int pbgpu_batch_begin(pbgpu_batch* b, const pbgpu_solver_opts* opts) {
     pbgpu_default_solver_opts(&o);
   const int rc = check_opts(b, o);
   if (rc != PBGPU_OK) return rc;
+  if (b->in_flight) return b->fail(PBGPU_ERR_STATE, "batch_begin: a launch is in flight (pbgpu_batch_wait)");
   b->opts = o;
   b->mixed = o.precision == PBGPU_MIXED;
   b->session = true;
@@ -764,17 +787,31 @@ int pbgpu_batch_begin(pbgpu_batch* b, const pbgpu_solver_opts* opts) {
   return PBGPU_OK;
 }
 
-int pbgpu_batch_step(pbgpu_batch* b, int steps, int* n_active) {
+int pbgpu_batch_launch(pbgpu_batch* b, int steps) {
   if (!b || steps < 0) return PBGPU_ERR_ARG;
-  if (!b->session) return b->fail(PBGPU_ERR_STATE, "batch_step: no session (pbgpu_batch_begin)");
+  if (!b->session) return b->fail(PBGPU_ERR_STATE, "batch_launch: no session (pbgpu_batch_begin)");
+  if (b->in_flight) return b->fail(PBGPU_ERR_STATE, "batch_launch: the previous launch was not waited for");
   if (cudaSetDevice(b->device) != cudaSuccess) return PBGPU_ERR_CUDA;
   cudaGetLastError();
-  return b->mixed ? batch_step<float>(b, steps, n_active) : batch_step<double>(b, steps, n_active);
+  return b->mixed ? batch_launch<float>(b, steps) : batch_launch<double>(b, steps);
+}
+
+int pbgpu_batch_wait(pbgpu_batch* b, int* n_active) {
+  if (!b) return PBGPU_ERR_ARG;
+  if (cudaSetDevice(b->device) != cudaSuccess) return PBGPU_ERR_CUDA;
+  return batch_wait(b, n_active);
+}
+
+int pbgpu_batch_step(pbgpu_batch* b, int steps, int* n_active) {
+  const int rc = pbgpu_batch_launch(b, steps);
+  if (rc != PBGPU_OK) return rc;
+  return pbgpu_batch_wait(b, n_active);
 }
 
 int pbgpu_batch_member(pbgpu_batch* b, int slot, int* done, pbgpu_solve_stats* stats) {
   if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot]) return PBGPU_ERR_ARG;
-  if (!b->session || b->pending[slot] || !b->st_host) {
+  if (b->in_flight) return b->fail(PBGPU_ERR_STATE, "batch_member: a launch is in flight (pbgpu_batch_wait)");
+  if (!b->session || b->pending[slot] || !b->st_host || (size_t)slot >= b->st_cap) {
     if (done) *done = 0;
     return PBGPU_OK;
   }

@@ -369,6 +369,12 @@ int pbgpu_assemble(pbgpu_ctx* h, const pbgpu_sell_opts* o) {
   Context* c = &h->c;
   SET_DEVICE(c);
   StageTimer t(c, 2);
+  pbgpu_sell_opts tuned;
+  int cols = 0;
+  if (!o && c->have_mesh && tuned_layout(c->n, &tuned, &cols)) {  // pbgpu_autotune ran for this size class
+    c->spmv_cols = cols ? cols : c->spmv_cols;
+    return run_assemble(c, &tuned);
+  }
   return run_assemble(c, o);
 }
 
@@ -396,6 +402,15 @@ int pbgpu_energy(pbgpu_ctx* h, int fast, pbgpu_energy_out* out) {
   SET_DEVICE(c);
   StageTimer t(c, 5);
   return run_energy(c, fast, out);
+}
+
+int pbgpu_solve_charges(pbgpu_ctx* h, int k, const double* charges, const pbgpu_solver_opts* o, int fast,
+                        pbgpu_energy_out* energies, pbgpu_solve_stats* stats) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  SET_DEVICE(c);
+  StageTimer t(c, 3);
+  return run_solve_charges(c, k, charges, o, fast, energies, stats);
 }
 
 void pbgpu_default_solver_opts(pbgpu_solver_opts* o) {

@@ -208,6 +208,9 @@ struct Context {
   DBuf<double> ones;         // the "no preconditioner" diagonal
   DBuf<float> ones32;
   DBuf<float> bjinv;         // block-Jacobi inverse blocks (node order)
+  // many right-hand sides: n_pad x kp blocks (row-major), per-column scalars
+  DBuf<double> mr_b, mr_x, mr_r, mr_p, mr_q, mr_scal, mr_part, mr_q_dev;
+  DBuf<int> mr_int;
   bool bj_ready = false;     // bjinv belongs to the current system
   DBuf<double> partials;     // block partial sums
   DBuf<KrylovScalars> ks;
@@ -359,6 +362,10 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o);
 int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st);
 int run_phi_atoms(Context* c, double* out);
 int run_energy(Context* c, int fast, pbgpu_energy_out* out);
+int run_rhs(Context* c);
+bool tuned_layout(int64_t n, pbgpu_sell_opts* sell, int* cols);
+int run_solve_charges(Context* c, int k, const double* charges, const pbgpu_solver_opts* opts, int fast,
+                      pbgpu_energy_out* energies, pbgpu_solve_stats* stats);
 int export_system(Context* c, int64_t* nnz, int64_t* row_ptr, int32_t* col, double* val, double* rhs);
 
 // scratch for CUB temporaries

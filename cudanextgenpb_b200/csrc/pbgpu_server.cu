@@ -3,19 +3,19 @@
 // (src/poisson_boltzmann.cpp:192-299) runs one molecule per process.
 //
 // A tick of pbgpu_server_progress:
-//   1. admits queued requests (FIFO) while the member cap and the HBM budget
-//      allow: the request's inputs are set on an idle context (or a new one)
-//      and its markers, density map and SELL system are built on that
-//      context's own stream;
-//   2. advances every member system with one persistent launch of the
-//      multi-system solver (pbgpu_batch_step), which holds the matrices and
-//      Krylov states of all members on the device;
-//   3. retires the members that converged: potential at atoms and energies on
-//      their context, result returned, context back to the idle pool.
-// Setup of new requests (1) is issued on the member contexts' streams while
-// the persistent kernel of the previous tick may still run on the batch
-// stream; the persistent kernel is limited to blocks_per_sm resident blocks
-// so other kernels fit beside it.
+//   1. launches one persistent step of the multi-system solver over the
+//      members (pbgpu_batch_launch), which holds the matrices and Krylov
+//      states of all members on the device;
+//   2. meanwhile admits queued requests (FIFO) while the member cap, the
+//      per-tick admission cap and the HBM budget allow, and sets each one up
+//      (inputs, markers, density map, SELL system) on its own context and
+//      stream from its own host thread;
+//   3. waits for the persistent step;
+//   4. retires the members that converged: energies on their context, result
+//      returned, context back to the idle pool;
+//   5. adds the set-up requests to the batch; they start with the next tick.
+// The persistent kernel is limited to blocks_per_sm resident blocks so the
+// set-up kernels of (2) run beside it.
 // Admission counts the device bytes every context holds (idle ones included,
 // their buffers are kept for reuse) plus an estimate for the request; idle
 // contexts are destroyed, largest first, when the budget needs the room.
@@ -26,6 +26,7 @@
 #include <cstring>
 #include <deque>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pbgpu_internal.cuh"
@@ -92,6 +93,7 @@ void pbgpu_default_server_opts(pbgpu_server_opts* o) {
   o->max_members = 64;
   o->steps_per_tick = 32;
   o->blocks_per_sm = 2;
+  o->admit_per_tick = 16;
   pbgpu_default_solver_opts(&o->solver);
   o->solver.method = PBGPU_CG;
   o->solver.precond = PBGPU_PRECOND_JACOBI;
@@ -188,8 +190,23 @@ int pbgpu_server_progress(pbgpu_server* s, pbgpu_result* out, int cap, int* n_ou
       return s->fail(st, std::string("server: ") + pbgpu_batch_last_error(s->batch));
     s->in_session = true;
   }
-  // 1. admission
-  while (!s->queue.empty() && (int)s->running.size() < s->opts.max_members) {
+  // 1. the members of the previous ticks advance on the batch stream ...
+  const bool launched = !s->running.empty();
+  if (launched && (st = pbgpu_batch_launch(s->batch, s->opts.steps_per_tick)) != PBGPU_OK)
+    return s->fail(st, std::string("server: ") + pbgpu_batch_last_error(s->batch));
+  // 2. ... while admitted requests are set up on their own contexts, one host
+  //    thread each (their host waits overlap)
+  struct Admit {
+    Pending p;
+    pbgpu_ctx* ctx;
+    Clock::time_point t_admit;
+    int st;
+  };
+  std::vector<Admit> adm;
+  const int room = s->opts.max_members - (int)s->running.size();
+  const int max_new = std::min(room, s->opts.admit_per_tick > 0 ? s->opts.admit_per_tick : room);
+  int64_t held = held_bytes(s);
+  while (!s->queue.empty() && (int)adm.size() < max_new) {
     const Pending& p = s->queue.front();
     const int64_t need = pbgpu_request_bytes_estimate(&p.req);
     // the idle context whose buffers are closest above the need, else the largest
@@ -204,7 +221,6 @@ int pbgpu_server_progress(pbgpu_server* s, pbgpu_result* out, int cap, int* n_ou
       const bool fits = b >= need, fits_p = bp >= need;
       if ((fits && (!fits_p || b < bp)) || (!fits && !fits_p && b > bp)) pick = (int)k;
     }
-    int64_t held = held_bytes(s);
     const int64_t reuse = pick >= 0 ? ctx_bytes(s->idle[pick]) : 0;
     int64_t after = held - reuse + std::max(reuse, need);
     // free idle contexts (largest first, never the picked one) until it fits
@@ -214,44 +230,37 @@ int pbgpu_server_progress(pbgpu_server* s, pbgpu_result* out, int cap, int* n_ou
         if ((int)k != pick && (big < 0 || ctx_bytes(s->idle[k]) > ctx_bytes(s->idle[big]))) big = (int)k;
       if (big < 0) break;
       after -= ctx_bytes(s->idle[big]);
+      held -= ctx_bytes(s->idle[big]);
       pbgpu_ctx_destroy(s->idle[big]);
       s->idle.erase(s->idle.begin() + big);
       if (pick > big) --pick;
     }
-    if (after > (int64_t)s->opts.hbm_budget_bytes && !s->running.empty()) break;  // wait for members to finish
+    if (after > (int64_t)s->opts.hbm_budget_bytes && !(s->running.empty() && adm.empty())) break;
     pbgpu_ctx* ctx = nullptr;
     if (pick >= 0) {
       ctx = s->idle[pick];
       s->idle.erase(s->idle.begin() + pick);
     } else if ((st = pbgpu_ctx_create(&ctx, s->device, nullptr)) != PBGPU_OK) {
+      if (launched) pbgpu_batch_wait(s->batch, nullptr);
       return s->fail(st, "server: context creation failed");
     }
-    Running r{p.id, p.req.user_tag, -1, ctx, p.req.n_atoms, p.t_submit, Clock::now()};
-    st = setup_request(s, ctx, p.req);
-    if (st == PBGPU_OK) st = pbgpu_batch_add(s->batch, ctx, &r.slot);
-    if (st != PBGPU_OK) {
-      // the request fails alone: report it, keep serving
-      if (n_out && *n_out < cap) {
-        pbgpu_result& o = out[(*n_out)++];
-        std::memset(&o, 0, sizeof(o));
-        o.id = p.id;
-        o.user_tag = p.req.user_tag;
-        o.status = st;
-        o.latency_ms = ms_since(p.t_submit);
-      }
-      s->idle.push_back(ctx);
-      s->queue.pop_front();
-      continue;
-    }
-    s->running.push_back(r);
+    held += std::max(reuse, need) - reuse;
+    adm.push_back(Admit{p, ctx, Clock::now(), PBGPU_OK});
     s->queue.pop_front();
-    ++s->admitted;
   }
-  // 2. one persistent launch over all members
+  if (adm.size() == 1) {
+    adm[0].st = setup_request(s, adm[0].ctx, adm[0].p.req);
+  } else if (!adm.empty()) {
+    std::vector<std::thread> th;
+    th.reserve(adm.size());
+    for (Admit& a : adm) th.emplace_back([s, &a] { a.st = setup_request(s, a.ctx, a.p.req); });
+    for (std::thread& t : th) t.join();
+  }
+  // 3. the batch launch completes
   int active = 0;
-  if (!s->running.empty() && (st = pbgpu_batch_step(s->batch, s->opts.steps_per_tick, &active)) != PBGPU_OK)
+  if (launched && (st = pbgpu_batch_wait(s->batch, &active)) != PBGPU_OK)
     return s->fail(st, std::string("server: ") + pbgpu_batch_last_error(s->batch));
-  // 3. retire converged members (as many as the output array holds)
+  // 4. retire converged members (as many as the output array holds)
   for (size_t k = 0; k < s->running.size();) {
     if (n_out && *n_out >= cap) break;
     Running& r = s->running[k];
@@ -277,6 +286,28 @@ int pbgpu_server_progress(pbgpu_server* s, pbgpu_result* out, int cap, int* n_ou
     s->running.erase(s->running.begin() + k);
     ++s->completed;
   }
+  // 5. the newly set-up requests join the batch (they start next tick)
+  for (Admit& a : adm) {
+    Running r{a.p.id, a.p.req.user_tag, -1, a.ctx, a.p.req.n_atoms, a.p.t_submit, a.t_admit};
+    int stt = a.st;
+    if (stt == PBGPU_OK) stt = pbgpu_batch_add(s->batch, a.ctx, &r.slot);
+    if (stt != PBGPU_OK) {
+      // the request fails alone: report it (if there is room), keep serving
+      if (n_out && *n_out < cap) {
+        pbgpu_result& o = out[(*n_out)++];
+        std::memset(&o, 0, sizeof(o));
+        o.id = a.p.id;
+        o.user_tag = a.p.req.user_tag;
+        o.status = stt;
+        o.latency_ms = ms_since(a.p.t_submit);
+      }
+      s->idle.push_back(a.ctx);
+      continue;
+    }
+    s->running.push_back(r);
+    ++s->admitted;
+  }
+  (void)active;
   return PBGPU_OK;
 }
 

@@ -227,6 +227,12 @@ class GpuPath:
         o = N.PbgpuSellOpts(chunk, sigma, group)
         self._check(self._lib.pbgpu_assemble(self._ctx, C.byref(o)))
 
+    def autotune(self, iterations: int = 24) -> dict:
+        """Time the SpMV in each candidate SELL layout; the fastest stays assembled."""
+        so, cols, ms = N.PbgpuSellOpts(), C.c_int(), C.c_double()
+        self._check(self._lib.pbgpu_autotune(self._ctx, iterations, C.byref(so), C.byref(cols), C.byref(ms)))
+        return {"chunk": so.chunk, "sigma": so.sigma, "group": so.group, "cols": cols.value, "spmv_ms": ms.value}
+
     def solve(self, opts: N.PbgpuSolverOpts | None = None, allow_not_converged=False):
         s = N.PbgpuSolveStats()
         ok = (0, N.PBGPU_NOT_CONVERGED) if allow_not_converged else (0,)
@@ -463,3 +469,15 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def solve_charges(g: GpuPath, charges, opts: N.PbgpuSolverOpts | None = None, fast=False):
+    """k charge vectors (k x n_atoms) on g's assembled system in one multi-RHS
+    solve; returns (list of energy dicts, list of solve stats)."""
+    q = np.ascontiguousarray(charges, dtype=np.float64)
+    k = q.shape[0]
+    es = (N.PbgpuEnergyOut * k)()
+    ss = (N.PbgpuSolveStats * k)()
+    g._check(g._lib.pbgpu_solve_charges(g._ctx, k, _dptr(q), C.byref(opts) if opts else None, 1 if fast else 0,
+                                        es, ss))
+    return [e.as_dict() for e in es], list(ss)

@@ -240,6 +240,28 @@ int pbgpu_reset_counters(pbgpu_ctx* ctx);
 int pbgpu_coulomb_energy_static(const double* atoms, int64_t n_atoms, double e_in, double T, double* out_energy,
                                 void* cuda_stream);
 
+/* ---- SELL layout autotuner ----------------------------------------------
+ * No counterpart in the reference.  Assembles the context's system (markers
+ * and density map must be current) in each candidate layout (chunk 32 / 64,
+ * sigma 256 / 2048 / 16384, group 1 / 2 / 4, and for chunk 32 group 1 the
+ * staged SpMV's chunk width 12 / 16), times the CG SpMV over `iterations`
+ * Jacobi-CG iterations (0: 24) with CUDA events, and leaves the fastest layout
+ * assembled.  The choice is remembered per matrix size class (log2 of the
+ * row count) for later pbgpu_assemble(ctx, NULL) calls in this process.
+ * best_cols is 0 unless the staged kernel won. */
+int pbgpu_autotune(pbgpu_ctx* ctx, int iterations, pbgpu_sell_opts* best, int* best_cols, double* best_spmv_ms);
+
+/* ---- many charge vectors on one system ----------------------------------
+ * No counterpart in the reference (one charge set per run).  The context's
+ * assembled matrix is shared by k <= 64 charge vectors (charges: k x n_atoms,
+ * same atom positions): each gets its density map and right-hand side, the k
+ * systems are solved by k Jacobi-CG recurrences sharing every SpMV (FP64,
+ * relative 2-norm tolerance), and energies[j] / stats[j] are those of charge
+ * vector j (either may be NULL).  Afterwards the context holds its own charges
+ * again and the potential of the last vector. */
+int pbgpu_solve_charges(pbgpu_ctx* ctx, int k, const double* charges, const pbgpu_solver_opts* opts, int fast,
+                        pbgpu_energy_out* energies, pbgpu_solve_stats* stats);
+
 /* ---- batches: many systems, one persistent launch ------------------------
  * No counterpart in the reference, which solves one system per process
  * (lis_compute_electric_potential, src/pb_class.cpp:2244-2329).  A batch holds
@@ -272,6 +294,11 @@ int pbgpu_batch_solve(pbgpu_batch* batch, const pbgpu_solver_opts* opts, pbgpu_s
 int pbgpu_batch_begin(pbgpu_batch* batch, const pbgpu_solver_opts* opts);
 int pbgpu_batch_step(pbgpu_batch* batch, int steps, int* n_active);
 int pbgpu_batch_member(pbgpu_batch* batch, int slot, int* done, pbgpu_solve_stats* stats);
+/* pbgpu_batch_step in two halves: launch returns once the persistent kernel
+ * is queued (other contexts' work can be issued meanwhile); wait completes it.
+ * Between them members may be added but not removed or queried. */
+int pbgpu_batch_launch(pbgpu_batch* batch, int steps);
+int pbgpu_batch_wait(pbgpu_batch* batch, int* n_active);
 /* resident blocks per SM of the persistent kernel (0: as many as fit); fewer
  * leave room for other streams' kernels to run beside it */
 int pbgpu_batch_set_blocks_per_sm(pbgpu_batch* batch, int blocks);
@@ -312,6 +339,7 @@ typedef struct {
   int blocks_per_sm;         /* persistent kernel residency (default 2; 0: as many as fit) */
   pbgpu_solver_opts solver;  /* CG + Jacobi; PBGPU_MIXED by default (FP32 inner, FP64 refined) */
   int energy_fast;           /* 1: energy_fast, 0: energy */
+  int admit_per_tick;        /* requests set up per progress call (default 16; 0: no cap) */
 } pbgpu_server_opts;
 
 typedef struct pbgpu_server pbgpu_server;

@@ -130,3 +130,34 @@ def test_batch_continuous_membership():
     for j, e in finished.items():
         assert e == pytest.approx(alone[j], rel=1e-6)
     b.close()
+
+
+@pytest.mark.parametrize("k", [5, 40])
+def test_many_charge_vectors_equal_single_solves(k):
+    """pbgpu_solve_charges: k charge vectors on one assembled matrix give, for
+    every vector, the energy of a plain solve with those charges."""
+    from cudanextgenpb_b200 import solve_charges
+    prob, g = _member(MOLS[1])
+    pos, q, _ = prob.atoms()
+    rng = np.random.default_rng(64)
+    Q = np.repeat(q[None, :], k, axis=0)
+    for j in range(k):
+        sites = rng.choice(len(q), size=8, replace=False)
+        Q[j, sites] += rng.choice([-1.0, 1.0], size=8)
+    opts = solver_opts("cg", tol=1e-10)
+    es, ss = solve_charges(g, Q, opts)
+    assert all(s.status == 0 and s.rel_residual <= 1e-10 for s in ss)
+    # the context keeps its own charges
+    e0, _ = g.run(opts)
+    ref0 = GpuPath().load(prob)
+    e_ref0, _ = ref0.run(opts)
+    assert e0["sum"] == pytest.approx(e_ref0["sum"], rel=1e-9)
+    for j in (0, k // 2, k - 1):
+        h = GpuPath().load(prob)
+        h.set_atoms(pos, Q[j])
+        e, st = h.run(opts)
+        assert es[j]["sum"] == pytest.approx(e["sum"], rel=1e-6)
+        assert abs(ss[j].iterations - st.iterations) <= max(3, st.iterations // 20)
+        h.close()
+    ref0.close()
+    g.close()
