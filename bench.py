@@ -53,6 +53,23 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+def max_over_ranks(value, dist, device="cuda"):
+    """The largest of the ranks' values: a multi-GPU step takes as long as its
+    slowest rank."""
+    if not dist:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_throughput(world, steps, ms_max):
+    """Whole-job solves/s of `world` independent replicas that each ran
+    `steps` solves, timed by the slowest rank."""
+    return world * steps / (ms_max / 1e3)
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -277,10 +294,8 @@ def run_ours(args, rank, world, local):
     cnt = g.counters()
     stage = g.stage_ms()
     g.set_profiling(False)
+    ms = max_over_ranks(ms, dist)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
 
     # end to end through the C ABI from pinned host buffers
@@ -316,16 +331,12 @@ def run_ours(args, rank, world, local):
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_e2e = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), dist)
 
     result = None
     if rank == 0:
-        value = world * args.steps / (ms / 1e3)
-        e2e = world * args.steps / (ms_e2e / 1e3)
+        value = replicas_throughput(world, args.steps, ms)
+        e2e = replicas_throughput(world, args.steps, ms_e2e)
         peak, peak_kind = measured_peak()
         spmv_avg_ms = cnt["spmv_ms"] / max(cnt["spmv_launches"], 1)
         achieved = cnt["spmv_bytes"] / (spmv_avg_ms / 1e3) / 1e9 if cnt["spmv_launches"] else None
@@ -603,7 +614,8 @@ def run_serve(args, rank, world, local):
 
     # served
     srv = Server(local, tol=args.tol, precision=args.precision, max_members=args.max_members,
-                 steps_per_tick=32, inner_tol=1e-4)
+                 steps_per_tick=32, inner_tol=1e-4, mode=1 if args.server_mode == "concurrent" else 0,
+                 workers=args.workers)
     reqs = [srv.request(p) for p in probs]
     # warm-up: one request of each molecule
     for r in reqs:
@@ -665,7 +677,7 @@ def run_serve(args, rank, world, local):
                                "log-uniform in %d-%d, scale 2/A, %d surface level(s); continuous-batching server"
                                % (rate, seconds, seed, npool, lo, hi, levels),
                    "requests": n_req, "tol": args.tol, "precision": args.precision,
-                   "max_members": args.max_members,
+                   "max_members": args.max_members, "server_mode": args.server_mode, "workers": args.workers,
                    "plain_solves_per_s": plain, "plain_latency_ms": pct(lp), "speedup_vs_plain": value / plain,
                    "max_rel_energy_err_vs_plain": err,
                    "wall_clock": "host perf_counter; latency from each request's scheduled arrival"},
@@ -681,6 +693,8 @@ def main():
     ap.add_argument("--workload", default="mol2000", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(SERVES))
     ap.add_argument("--max-members", type=int, default=64)
     ap.add_argument("--via-batch", action="store_true", help="solve through the persistent multi-system kernel")
+    ap.add_argument("--server-mode", default="concurrent", choices=["concurrent", "batched"])
+    ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--chunk", type=int, default=32)

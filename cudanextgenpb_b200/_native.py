@@ -74,7 +74,7 @@ class PbgpuResult(C.Structure):
 class PbgpuServerOpts(C.Structure):
     _fields_ = [("hbm_budget_bytes", dbl), ("max_members", C.c_int), ("steps_per_tick", C.c_int),
                 ("blocks_per_sm", C.c_int), ("solver", PbgpuSolverOpts), ("energy_fast", C.c_int),
-                ("admit_per_tick", C.c_int)]
+                ("admit_per_tick", C.c_int), ("mode", C.c_int), ("workers", C.c_int)]
 
 
 class PbhostInfo(C.Structure):

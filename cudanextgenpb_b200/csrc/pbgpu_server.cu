@@ -23,6 +23,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
+#include <mutex>
 #include <cstring>
 #include <deque>
 #include <string>
@@ -62,6 +64,15 @@ struct pbgpu_server {
   int device = 0;
   pbgpu_server_opts opts{};
   pbgpu_batch* batch = nullptr;
+  // concurrent mode: worker threads, each with its own context and stream
+  std::vector<std::thread> workers;
+  std::vector<pbgpu_ctx*> worker_ctx;
+  std::mutex mu;
+  std::condition_variable cv_job, cv_done;
+  std::deque<Pending> jobs;
+  std::deque<pbgpu_result> finished;
+  int in_flight = 0;
+  bool stop = false;
   std::deque<Pending> queue;
   std::vector<Running> running;
   std::vector<pbgpu_ctx*> idle;
@@ -74,6 +85,53 @@ struct pbgpu_server {
     return code;
   }
 };
+
+// Inputs, markers, density map and SELL system of one request on `ctx`.
+static int setup_request(pbgpu_server* s, pbgpu_ctx* ctx, const pbgpu_request& r) {
+  int st;
+  if ((st = pbgpu_set_mesh(ctx, r.mesh)) != PBGPU_OK) return st;
+  for (int a = 0; a < 3; ++a)
+    if ((st = pbgpu_set_rays(ctx, a, &r.rays[a])) != PBGPU_OK) return st;
+  if ((st = pbgpu_set_atoms(ctx, r.n_atoms, r.pos, r.charge)) != PBGPU_OK) return st;
+  if ((st = pbgpu_set_model(ctx, r.model)) != PBGPU_OK) return st;
+  if ((st = pbgpu_create_markers(ctx)) != PBGPU_OK) return st;
+  if ((st = pbgpu_create_density_map(ctx)) != PBGPU_OK) return st;
+  pbgpu_sell_opts so{32, 2048, 4};
+  return pbgpu_assemble(ctx, &so);
+  (void)s;
+}
+
+// Concurrent mode: a worker takes dispatched requests one at a time and runs
+// the whole path for each on its own context (and stream).
+static void worker_loop(pbgpu_server* s, int w) {
+  pbgpu_ctx* ctx = s->worker_ctx[w];
+  while (true) {
+    Pending p;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_job.wait(lk, [s] { return s->stop || !s->jobs.empty(); });
+      if (s->jobs.empty()) return;
+      p = s->jobs.front();
+      s->jobs.pop_front();
+    }
+    pbgpu_result o;
+    std::memset(&o, 0, sizeof(o));
+    o.id = p.id;
+    o.user_tag = p.req.user_tag;
+    o.queue_ms = ms_since(p.t_submit);
+    int st = setup_request(s, ctx, p.req);
+    if (st == PBGPU_OK) st = pbgpu_solve(ctx, &s->opts.solver, &o.stats);
+    if (st == PBGPU_OK) st = pbgpu_energy(ctx, s->opts.energy_fast, &o.energy);
+    o.status = st;
+    o.latency_ms = ms_since(p.t_submit);
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->finished.push_back(o);
+      --s->in_flight;
+    }
+    s->cv_done.notify_one();
+  }
+}
 
 extern "C" {
 
@@ -94,6 +152,8 @@ void pbgpu_default_server_opts(pbgpu_server_opts* o) {
   o->steps_per_tick = 32;
   o->blocks_per_sm = 2;
   o->admit_per_tick = 16;
+  o->mode = 0;
+  o->workers = 4;
   pbgpu_default_solver_opts(&o->solver);
   o->solver.method = PBGPU_CG;
   o->solver.precond = PBGPU_PRECOND_JACOBI;
@@ -117,6 +177,22 @@ int pbgpu_server_create(pbgpu_server** out, int device, const pbgpu_server_opts*
   if (s->opts.max_members <= 0) s->opts.max_members = 64;
   if (s->opts.steps_per_tick <= 0) s->opts.steps_per_tick = 32;
   if (!(s->opts.hbm_budget_bytes > 0)) s->opts.hbm_budget_bytes = 160e9;
+  if (s->opts.mode == 1) {
+    const int nw = s->opts.workers > 0 ? s->opts.workers : 4;
+    for (int w = 0; w < nw; ++w) {
+      pbgpu_ctx* c = nullptr;
+      const int st = pbgpu_ctx_create(&c, device, nullptr);
+      if (st != PBGPU_OK) {
+        for (pbgpu_ctx* x : s->worker_ctx) pbgpu_ctx_destroy(x);
+        delete s;
+        return st;
+      }
+      s->worker_ctx.push_back(c);
+    }
+    for (int w = 0; w < nw; ++w) s->workers.emplace_back(worker_loop, s, w);
+    *out = s;
+    return PBGPU_OK;
+  }
   int st = pbgpu_batch_create(&s->batch, device, nullptr);
   if (st != PBGPU_OK) {
     delete s;
@@ -129,6 +205,16 @@ int pbgpu_server_create(pbgpu_server** out, int device, const pbgpu_server_opts*
 
 void pbgpu_server_destroy(pbgpu_server* s) {
   if (!s) return;
+  if (!s->workers.empty()) {
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->stop = true;
+      s->jobs.clear();
+    }
+    s->cv_job.notify_all();
+    for (std::thread& t : s->workers) t.join();
+    for (pbgpu_ctx* c : s->worker_ctx) pbgpu_ctx_destroy(c);
+  }
   if (s->batch) pbgpu_batch_destroy(s->batch);
   for (Running& r : s->running) pbgpu_ctx_destroy(r.ctx);
   for (pbgpu_ctx* c : s->idle) pbgpu_ctx_destroy(c);
@@ -146,8 +232,20 @@ int pbgpu_server_submit(pbgpu_server* s, const pbgpu_request* req, int64_t* id) 
   return PBGPU_OK;
 }
 
-int pbgpu_server_pending(const pbgpu_server* s, int* queued, int* running, int64_t* device_bytes) {
-  if (!s) return PBGPU_ERR_ARG;
+int pbgpu_server_pending(const pbgpu_server* sc, int* queued, int* running, int64_t* device_bytes) {
+  if (!sc) return PBGPU_ERR_ARG;
+  pbgpu_server* s = const_cast<pbgpu_server*>(sc);
+  if (s->opts.mode == 1) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (queued) *queued = (int)(s->queue.size() + s->jobs.size());
+    if (running) *running = s->in_flight - (int)s->jobs.size() + (int)s->finished.size();
+    if (device_bytes) {
+      int64_t b = 0;
+      for (pbgpu_ctx* c : s->worker_ctx) b += ctx_bytes(c);
+      *device_bytes = b;
+    }
+    return PBGPU_OK;
+  }
   if (queued) *queued = (int)s->queue.size();
   if (running) *running = (int)s->running.size();
   if (device_bytes) {
@@ -159,20 +257,6 @@ int pbgpu_server_pending(const pbgpu_server* s, int* queued, int* running, int64
   return PBGPU_OK;
 }
 
-// Inputs, markers, density map and SELL system of one request on `ctx`.
-static int setup_request(pbgpu_server* s, pbgpu_ctx* ctx, const pbgpu_request& r) {
-  int st;
-  if ((st = pbgpu_set_mesh(ctx, r.mesh)) != PBGPU_OK) return st;
-  for (int a = 0; a < 3; ++a)
-    if ((st = pbgpu_set_rays(ctx, a, &r.rays[a])) != PBGPU_OK) return st;
-  if ((st = pbgpu_set_atoms(ctx, r.n_atoms, r.pos, r.charge)) != PBGPU_OK) return st;
-  if ((st = pbgpu_set_model(ctx, r.model)) != PBGPU_OK) return st;
-  if ((st = pbgpu_create_markers(ctx)) != PBGPU_OK) return st;
-  if ((st = pbgpu_create_density_map(ctx)) != PBGPU_OK) return st;
-  pbgpu_sell_opts so{32, 2048, 4};
-  return pbgpu_assemble(ctx, &so);
-  (void)s;
-}
 
 static int64_t held_bytes(const pbgpu_server* s) {
   int64_t b = 0;
@@ -181,9 +265,46 @@ static int64_t held_bytes(const pbgpu_server* s) {
   return b;
 }
 
+// Concurrent mode: dispatch queued requests to the workers while the budget
+// allows, then hand back the finished ones (waiting briefly when work is in
+// flight and nothing has finished yet).
+static int progress_concurrent(pbgpu_server* s, pbgpu_result* out, int cap, int* n_out) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  const int nw = (int)s->workers.size();
+  int64_t held = 0, largest = 0;
+  for (pbgpu_ctx* c : s->worker_ctx) {
+    held += ctx_bytes(c);
+    largest = std::max(largest, ctx_bytes(c));
+  }
+  while (!s->queue.empty() && s->in_flight < nw) {
+    const int64_t need = pbgpu_request_bytes_estimate(&s->queue.front().req);
+    // a worker may grow to this request's size: at worst all of them do
+    if (held - largest + (int64_t)nw * std::max(largest, need) > (int64_t)s->opts.hbm_budget_bytes &&
+        s->in_flight > 0)
+      break;
+    s->jobs.push_back(s->queue.front());
+    s->queue.pop_front();
+    ++s->in_flight;
+    ++s->admitted;
+  }
+  s->cv_job.notify_all();
+  if (s->finished.empty() && s->in_flight > 0)
+    s->cv_done.wait_for(lk, std::chrono::milliseconds(2), [s] { return !s->finished.empty(); });
+  while (!s->finished.empty() && *n_out < cap) {
+    out[(*n_out)++] = s->finished.front();
+    s->finished.pop_front();
+    ++s->completed;
+  }
+  return PBGPU_OK;
+}
+
 int pbgpu_server_progress(pbgpu_server* s, pbgpu_result* out, int cap, int* n_out) {
   if (!s || (cap > 0 && !out)) return PBGPU_ERR_ARG;
   if (n_out) *n_out = 0;
+  if (s->opts.mode == 1) {
+    int dummy = 0;
+    return progress_concurrent(s, out, cap, n_out ? n_out : &dummy);
+  }
   int st;
   if (!s->in_session) {
     if ((st = pbgpu_batch_begin(s->batch, &s->opts.solver)) != PBGPU_OK)

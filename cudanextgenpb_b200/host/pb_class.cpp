@@ -521,10 +521,17 @@ std::vector<uint8_t> poisson_boltzmann::corner_inside_z(const std::vector<uint8_
 // never fire and are not reproduced here.
 void poisson_boltzmann::refine_surface() {
   const int cycles = (maxlevel - unilevel) > (unilevel - minlevel) ? (maxlevel - unilevel) : (unilevel - minlevel);
+  double t_hm = 0, t_in = 0, t_ref = 0, t_crs = 0;
+  auto tick = [](double& acc, double t0) { acc += omp_get_wtime() - t0; };
   for (int kk = 0; kk < cycles; ++kk) {
     {
+      double t = omp_get_wtime();
       const std::vector<uint8_t> hm = tmsh.hanging_masks();
+      tick(t_hm, t);
+      t = omp_get_wtime();
       const std::vector<uint8_t> in = corner_inside_z(hm);
+      tick(t_in, t);
+      t = omp_get_wtime();
       std::vector<uint8_t> marks(tmsh.size(), 0);
 #pragma omp parallel for schedule(static)
       for (int64_t i = 0; i < tmsh.size(); ++i) {
@@ -539,10 +546,16 @@ void poisson_boltzmann::refine_surface() {
         if (mxv > 0.5 && mn < 0.5) marks[i] = 1;
       }
       tmsh.refine(marks);
+      tick(t_ref, t);
     }
     {
+      double t = omp_get_wtime();
       const std::vector<uint8_t> hm = tmsh.hanging_masks();
+      tick(t_hm, t);
+      t = omp_get_wtime();
       const std::vector<uint8_t> in = corner_inside_z(hm);
+      tick(t_in, t);
+      t = omp_get_wtime();
       std::vector<uint8_t> marks(tmsh.size(), 0);
 #pragma omp parallel for schedule(static)
       for (int64_t i = 0; i < tmsh.size(); ++i) {
@@ -557,8 +570,12 @@ void poisson_boltzmann::refine_surface() {
         if (mn > 0.5 || mxv < 0.5) marks[i] = 1;
       }
       tmsh.coarsen(marks);
+      tick(t_crs, t);
     }
   }
+  if (verbose)
+    std::fprintf(stderr, "refine_surface: hanging masks %g s, corner classification %g s, refine %g s, coarsen %g s\n",
+                 t_hm, t_in, t_ref, t_crs);
 }
 
 void poisson_boltzmann::finalize_mesh() {

@@ -340,6 +340,10 @@ typedef struct {
   pbgpu_solver_opts solver;  /* CG + Jacobi; PBGPU_MIXED by default (FP32 inner, FP64 refined) */
   int energy_fast;           /* 1: energy_fast, 0: energy */
   int admit_per_tick;        /* requests set up per progress call (default 16; 0: no cap) */
+  int mode;                  /* 0: members advance together in the persistent multi-system kernel;
+                                1: `workers` host threads each run whole requests on their own
+                                context and stream, overlapping on the device */
+  int workers;               /* mode 1 (default 4) */
 } pbgpu_server_opts;
 
 typedef struct pbgpu_server pbgpu_server;

@@ -25,14 +25,14 @@ def pool():
     return out
 
 
-@pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_server_results_equal_alone(pool, precision):
-    srv = Server(tol=1e-10, precision=precision, max_members=3, steps_per_tick=24)
+@pytest.mark.parametrize("precision,mode", [("mixed", 0), ("fp64", 0), ("mixed", 1), ("fp64", 1)])
+def test_server_results_equal_alone(pool, precision, mode):
+    srv = Server(tol=1e-10, precision=precision, max_members=3, steps_per_tick=24, mode=mode, workers=3)
     ids = {}
     for k, (prob, _) in enumerate(pool[:3]):
         ids[srv.submit(srv.request(prob, tag=k))] = k
     results = {}
-    for tick in range(3000):
+    for tick in range(20000):
         for r in srv.progress():
             results[r["tag"]] = r
         if tick == 2:  # more requests arrive while the first ones run
