@@ -41,6 +41,10 @@ WORKLOADS = {
     "mol2000l2": (2000, 18.0, -3.0, 2000, 2.0, 2),
     "mol300": (300, 11.0, -3.0, 300, 2.0, 2),
     "mol60": (60, 7.0, -3.0, 60, 2.0, 1),
+    # the 25,000-atom complex (radius 45 A, net +7 e, seed 25000) at scale 2/A
+    # with 2 surface levels: the mixed-precision configuration, scaled so the
+    # host mesh build stays within a minute
+    "mol25k": (25000, 45.0, 7.0, 25000, 2.0, 2),
 }
 # Jacobi-CG iterations to ||r|| <= 1e-8 ||b|| on the large workloads (the same
 # count on the GPU and on the CPU oracle: one algorithm, differing only in
@@ -382,6 +386,24 @@ def run_ours(args, rank, world, local):
             "gpu_launches": cnt["launches"],
             "clocks": ck,
         }
+        if args.compare_fp64 and args.precision == "mixed":
+            # the same molecule solved in plain FP64 on the GPU: error of the
+            # mixed-precision potential and energy against it, and the bytes
+            # each CG iteration moves in either precision
+            phi_m = g.phi().copy()
+            e_m = energies[-1]
+            st64 = g.solve(solver_opts("cg", tol=args.tol, max_iter=50000))
+            phi_64 = g.phi()
+            e_64 = g.energy(False)["sum"]
+            nnz = info_nnz(g)
+            n = info["n_nodes"]
+            result["config"]["vs_fp64"] = {
+                "phi_rel_l2_err": float(np.linalg.norm(phi_m - phi_64) / np.linalg.norm(phi_64)),
+                "energy_rel_err": abs(e_m - e_64) / abs(e_64),
+                "fp64_cg_iterations": st64.iterations,
+                "bytes_per_iteration_fp64": 12 * nnz + 104 * n,
+                "bytes_per_iteration_fp32_inner": 8 * nnz + 52 * n,
+            }
         if world == 1 and not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(prob, g, int(np.median(iters)), args)
     g.close()
@@ -694,6 +716,7 @@ def main():
     ap.add_argument("--max-members", type=int, default=64)
     ap.add_argument("--via-batch", action="store_true", help="solve through the persistent multi-system kernel")
     ap.add_argument("--server-mode", default="concurrent", choices=["concurrent", "batched"])
+    ap.add_argument("--compare-fp64", action="store_true", help="mixed precision: error against a plain FP64 solve")
     ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--tol", type=float, default=1e-8)

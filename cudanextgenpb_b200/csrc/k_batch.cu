@@ -113,17 +113,23 @@ __device__ __forceinline__ bool grid_barrier(GridBar* g) {
   return *reinterpret_cast<volatile int*>(&g->err) == 0;
 }
 
-// Loads of data that other blocks of the running kernel write (gathered
-// vector entries, member scalars, row-block partials) go through L2 only
-// (ld.global.cg), never through the SM's L1 or the read-only path; every row is
-// owned by the same thread in every phase, so a thread's own rows need no care.
+// Member scalars and row-block partials, which other blocks of the running
+// kernel write, are read through L2 only (ld.global.cg).  The gathered vector
+// entries are plain loads (L1-cached): they are read only after a grid
+// barrier whose acquire fence (fence.sc.gpu) orders them after the writers'
+// release, never through the read-only path.  Every row is owned by the same
+// thread in every phase, so a thread's own rows need no care.
 template <typename T>
 __device__ __forceinline__ T ldcg(const T* p) {
   return __ldcg(p);
 }
 
-// y_i = sum_j A(i, j) x_j of a G = 4 SELL row (sell_elem layout), x gathered
-// through L2.
+template <typename T>
+__device__ __forceinline__ T ld_plain(const T* p) {
+  return *p;
+}
+
+// y_i = sum_j A(i, j) x_j of a G = 4 SELL row (sell_elem layout).
 template <typename T>
 __device__ __forceinline__ T batch_row(const SellT<T>& A, int64_t p, const T* x) {
   const int64_t s = p / A.C;
@@ -140,23 +146,23 @@ __device__ __forceinline__ T batch_row(const SellT<T>& A, int64_t p, const T* x)
     if constexpr (sizeof(T) == 8) {
       const double2 v0 = __ldcs(reinterpret_cast<const double2*>(A.sval + k));
       const double2 v1 = __ldcs(reinterpret_cast<const double2*>(A.sval + k + 2));
-      acc += v0.x * ldcg(x + c.x);
-      acc += v0.y * ldcg(x + c.y);
-      acc += v1.x * ldcg(x + c.z);
-      acc += v1.y * ldcg(x + c.w);
+      acc += v0.x * ld_plain(x + c.x);
+      acc += v0.y * ld_plain(x + c.y);
+      acc += v1.x * ld_plain(x + c.z);
+      acc += v1.y * ld_plain(x + c.w);
     } else {
       const float4 v = __ldcs(reinterpret_cast<const float4*>(A.sval + k));
-      acc += v.x * ldcg(x + c.x);
-      acc += v.y * ldcg(x + c.y);
-      acc += v.z * ldcg(x + c.z);
-      acc += v.w * ldcg(x + c.w);
+      acc += v.x * ld_plain(x + c.x);
+      acc += v.y * ld_plain(x + c.y);
+      acc += v.z * ld_plain(x + c.z);
+      acc += v.w * ld_plain(x + c.w);
     }
   }
   const int Wg = W & ~3;
   const int64_t tb = sb + (int64_t)Wg * A.C + lane;
   for (int j = Wg; j < W; ++j) {
     const int64_t k = tb + (int64_t)(j - Wg) * A.C;
-    acc += __ldcs(A.sval + k) * ldcg(x + __ldcs(A.scol + k));
+    acc += __ldcs(A.sval + k) * ld_plain(x + __ldcs(A.scol + k));
   }
   return acc;
 }

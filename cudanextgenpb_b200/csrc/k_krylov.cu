@@ -197,6 +197,7 @@ struct ConvRule {
 __device__ __forceinline__ void set_conv(KrylovScalars* ks, const ConvRule& cr, double bb, double b1) {
   ks->conv = cr.mode;
   ks->bb = bb;
+  ks->rr_ref = bb;
   ks->b1 = b1;
   ks->tol2 = cr.tol * cr.tol * bb;
   ks->tol1 = cr.tol_w * b1 + cr.tol;
@@ -275,6 +276,8 @@ __global__ void k_cg_update(int64_t n, T* __restrict__ x, T* __restrict__ r, con
     if (!finite(v[0]) || !finite(v[1])) {
       ks->status = PBGPU_BREAKDOWN;
       ks->done = 1;
+    } else if (ks->reliable && (conv_met(ks, v[1], v[2]) || v[1] <= ks->delta2 * ks->rr_ref)) {
+      ks->ru = 1;  // the FP64 residual (k_ru_residual) decides and supplies beta
     } else if (conv_met(ks, v[1], v[2])) {
       ks->done = 1;
     } else if (ks->iter >= ks->max_iter) {
@@ -283,6 +286,55 @@ __global__ void k_cg_update(int64_t n, T* __restrict__ x, T* __restrict__ r, con
     } else if (dinv) {  // block Jacobi: beta comes from k_bj_apply
       ks->beta = v[0] / ks->rz;
       ks->rz = v[0];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Reliable updates of the FP32 CG (mixed precision): once its recursive
+// residual has fallen by delta since the last FP64 residual (or meets the
+// target), the FP32 correction is added to the FP64 solution, b - A x is
+// recomputed in FP64 and the CG continues from it with its search direction,
+// so it needs the iterations of FP64 CG.  Both kernels return at once unless
+// an update is due.
+__global__ void k_ru_apply(int64_t n, double* __restrict__ x, float* __restrict__ d, const KrylovScalars* ks) {
+  if (ks->done || !ks->ru) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    x[i] += (double)d[i];
+    d[i] = 0.f;
+  }
+}
+
+template <int G>
+__global__ void __launch_bounds__(kBlock, kSpmvMinBlocksWide)
+    k_ru_residual(SellT<double> A, int64_t n, const double* __restrict__ b, const double* __restrict__ x,
+                  float* __restrict__ r32, const float* __restrict__ dinv32, KrylovScalars* ks, double* partials) {
+  if (ks->done || !ks->ru) return;
+  double a[3] = {0.0, 0.0, 0.0};
+  spmv_direct_rows<double, G>(A, x, [&](int64_t i, double y) {
+    const double ri = i < n ? b[i] - y : 0.0;
+    const float rf = (float)ri;
+    r32[i] = rf;
+    a[0] += ri * ri;
+    a[1] += (double)rf * (double)(dinv32[i] * rf);
+    a[2] += fabs(ri);
+  });
+  if (grid_sum<3>(a, partials, &ks->ticket[7]) && threadIdx.x == 0) {
+    ks->rr = a[0];
+    ks->r1 = a[2];
+    ks->ru = 0;
+    if (!finite(a[0]) || !finite(a[1])) {
+      ks->status = PBGPU_BREAKDOWN;
+      ks->done = 1;
+    } else if (conv_met(ks, a[0], a[2])) {
+      ks->done = 1;
+    } else if (ks->iter >= ks->max_iter) {
+      ks->status = PBGPU_NOT_CONVERGED;
+      ks->done = 1;
+    } else {
+      ks->beta = a[1] / ks->rz;
+      ks->rz = a[1];
+      ks->rr_ref = a[0];
     }
   }
 }
@@ -922,6 +974,11 @@ struct KrylovVecs {
   const T *b, *dinv;  // dinv: 1 / diag (Jacobi), ones (no preconditioner), null (block Jacobi)
   SellT<T> A;
   T* z = nullptr;                   // block Jacobi: preconditioned residual (CG)
+  // reliable updates (T = float): the FP64 system and solution
+  const SellT<double>* A64 = nullptr;
+  const double* b64 = nullptr;
+  double* x64 = nullptr;
+  int64_t n_rows = 0;
   const float* bj = nullptr;        // block Jacobi: inverse blocks, node order
   const int32_t* iperm = nullptr;   // node -> SELL position
   int64_t n_nodes = 0;
@@ -940,6 +997,12 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
   PBGPU_CUDA(c, cudaMemsetAsync(ks, 0, sizeof(KrylovScalars), c->stream));
   int mi = max_iter;
   PBGPU_CUDA(c, cudaMemcpyAsync(&ks->max_iter, &mi, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  if (K.x64 && method == PBGPU_CG) {
+    static const int on = 1;
+    static const double delta2 = 0.01;  // an FP64 residual every 10x reduction of the FP32 one
+    PBGPU_CUDA(c, cudaMemcpyAsync(&ks->reliable, &on, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    PBGPU_CUDA(c, cudaMemcpyAsync(&ks->delta2, &delta2, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  }
   const bool bj = K.dinv == nullptr;
   const int Gb = grid_blocks(c, (K.n_nodes + kBjBlock - 1) / kBjBlock * kBjBlock);
   // z = M^-1 r (with (r, z) and beta when `dot`)
@@ -988,7 +1051,8 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
   PBGPU_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   int kernels_per_chunk = 0;
   for (int k = 0; k < check_every; ++k) {
-    kernels_per_chunk += (method == PBGPU_CG ? 3 : method == PBGPU_CGS ? 4 : 5) + (bj ? (method == PBGPU_CG ? 1 : 2) : 0);
+    kernels_per_chunk += (method == PBGPU_CG ? 3 : method == PBGPU_CGS ? 4 : 5) + (bj ? (method == PBGPU_CG ? 1 : 2) : 0) +
+                         (K.x64 && method == PBGPU_CG ? 2 : 0);
     if (method == PBGPU_CG) {
       mark(k, 0, 0);
       if (tg)
@@ -997,6 +1061,16 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
         k_cg_spmv<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.p, K.q, ks, part);
       mark(k, 0, 1);
       k_cg_update<T><<<G, kBlock, 0, c->stream>>>(n, K.x, K.r, K.p, K.q, K.dinv, ks, part);
+      if constexpr (std::is_same<T, float>::value) {
+        if (K.x64) {
+          k_ru_apply<<<G, kBlock, 0, c->stream>>>(n, K.x64, K.x, ks);
+          switch (K.A64->G) {
+            case 1: k_ru_residual<1><<<G, kBlock, 0, c->stream>>>(*K.A64, K.n_rows, K.b64, K.x64, K.r, K.dinv, ks, part); break;
+            case 2: k_ru_residual<2><<<G, kBlock, 0, c->stream>>>(*K.A64, K.n_rows, K.b64, K.x64, K.r, K.dinv, ks, part); break;
+            default: k_ru_residual<4><<<G, kBlock, 0, c->stream>>>(*K.A64, K.n_rows, K.b64, K.x64, K.r, K.dinv, ks, part); break;
+          }
+        }
+      }
       if (bj) bj_apply(K.r, K.z, true);
       k_cg_pupdate<T><<<G, kBlock, 0, c->stream>>>(n, K.p, K.r, K.dinv, K.z, ks);
     } else if (method == PBGPU_CGS) {
@@ -1273,7 +1347,27 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
       K.sh = sh32.get();
     }
     status = PBGPU_NOT_CONVERGED;
-    for (outer = 1; outer <= max_outer; ++outer) {
+    const bool reliable = opt.method == PBGPU_CG && !bj;
+    if (reliable) {
+      // FP32 CG with reliable FP64 residual updates: one Krylov run
+      k_to_f32<<<grid_blocks(c, n_pad), kBlock, 0, c->stream>>>(n_pad, c->b.get(), c->b32.get());
+      PBGPU_LAUNCHED(c);
+      K.A64 = &A64;
+      K.b64 = c->b.get();
+      K.x64 = c->x.get();
+      K.n_rows = n;
+      int it = 0, ist = 0;
+      int rc = krylov<float>(c, opt.method, K, rule, opt.max_iter, opt.check_every, &it, &ist);
+      if (rc != PBGPU_OK) return rc;
+      if (ist == PBGPU_TIMEOUT) return c->fail(PBGPU_TIMEOUT, "solve: SpMV copy wait timed out");
+      // a correction not yet folded in (the run stopped in the FP32 recursion)
+      k_axpy_f32<<<grid_blocks(c, n_pad), kBlock, 0, c->stream>>>(n_pad, c->x.get(), c->x32.get());
+      PBGPU_LAUNCHED(c);
+      iters = it;
+      outer = 1;
+      status = ist;
+    }
+    for (outer = 1; !reliable && outer <= max_outer; ++outer) {
       // r = b - A x in fp64, handed to the inner solve in fp32
       launch_residual(c, A64, n, nullptr, c->b32.get());
       PBGPU_LAUNCHED(c);

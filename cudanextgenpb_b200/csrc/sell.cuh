@@ -40,10 +40,10 @@ struct V2<float> {
 // y_p = sum_j A(p, j) x_j for SELL row p, element j at sell_elem(): the
 // first W - W % G columns in groups of G (one vector load per group, a warp's
 // loads of one group contiguous), the remaining W % G columns one per lane.
-// (W and sb: width and first element of the row's slice)
+// (W and sb: width and first element of the row's slice, lane: the row's
+// position in it)
 template <typename T, int G>
-__device__ __forceinline__ T sell_row(const SellT<T>& A, int64_t p, const T* __restrict__ x, int W, int64_t sb) {
-  const int lane = (int)(p % A.C);
+__device__ __forceinline__ T sell_row(const SellT<T>& A, int lane, const T* __restrict__ x, int W, int64_t sb) {
   T acc = 0;
   if constexpr (G == 1) {
     const int64_t base = sb + lane;
@@ -100,8 +100,8 @@ __device__ __forceinline__ T sell_row(const SellT<T>& A, int64_t p, const T* __r
 
 template <typename T, int G>
 __device__ __forceinline__ T sell_row(const SellT<T>& A, int64_t p, const T* __restrict__ x) {
-  const int64_t s = p / A.C;
-  return sell_row<T, G>(A, p, x, A.slice_w[s], A.slice_ptr[s]);
+  const int64_t s = A.C == 32 ? (p >> 5) : p / A.C;  // the default slice height needs no division
+  return sell_row<T, G>(A, (int)(p - s * A.C), x, A.slice_w[s], A.slice_ptr[s]);
 }
 
 // fn(i, (A x)_i) for the rows of this thread (grid-stride loop).  (Loading
