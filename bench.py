@@ -373,6 +373,13 @@ def run_ours(args, rank, world, local):
                 "energy_kT": energies[-1],
                 "dof_iterations_per_s": world * info["n_nodes"] * float(np.median(iters)) / (ms / 1e3 / args.steps),
                 "stage_ms": stage,
+                "energy_pairs": {
+                    "points": cnt["energy_points"], "pairs_per_step": cnt["energy_pairs"] / max(args.steps, 1),
+                    # 12 FP64 flops per surface-point x atom pair (dx, dy, dz, r^2, 1/r, q/r, the
+                    # normal term), the count the roofline of the pair kernel uses
+                    "gflops": 12.0 * cnt["energy_pairs"] / max(args.steps, 1) / (stage["energy"] / 1e3) / 1e9
+                    if stage.get("energy") else None,
+                },
                 "l2": "inputs larger than L2 (126 MB): every step streams the mesh, matrix and vectors from HBM",
                 "parallelism": "replicas (one independent solve per GPU)",
             },

@@ -238,7 +238,7 @@ __global__ void k_cg_init(int64_t n, const T* __restrict__ b, const T* __restric
 }
 
 template <typename T, int G>
-__global__ void __launch_bounds__(kBlock, G == 1 ? kSpmvMinBlocks : kSpmvMinBlocksWide) k_cg_spmv(SellT<T> A, const T* __restrict__ p, T* __restrict__ q, KrylovScalars* ks, double* partials) {
+__global__ void __launch_bounds__(kBlock, kSpmvMinBlocks) k_cg_spmv(SellT<T> A, const T* __restrict__ p, T* __restrict__ q, KrylovScalars* ks, double* partials) {
   if (ks->done) return;
   double v[1] = {0.0};
   spmv_direct_rows<T, G>(A, p, [&](int64_t i, T y) {
@@ -510,7 +510,7 @@ __global__ void k_bicg_p(int64_t n, T* __restrict__ p, T* __restrict__ ph, const
 
 // v = A ph;  alpha = rho_new / (rh, v)
 template <typename T, int G>
-__global__ void __launch_bounds__(kBlock, G == 1 ? kSpmvMinBlocks : kSpmvMinBlocksWide) k_bicg_v(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh,
+__global__ void __launch_bounds__(kBlock, kSpmvMinBlocks) k_bicg_v(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh,
                          KrylovScalars* ks, double* partials) {
   if (ks->done) return;
   double s[1] = {0.0};

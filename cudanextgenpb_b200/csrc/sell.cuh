@@ -10,9 +10,10 @@ namespace pbgpu {
 
 constexpr int kBlock = 256;
 // resident blocks per SM the direct SpMV kernels are compiled for
-// (registers <= 65536 / (256 * blocks)): 4, i.e. 64 registers, which the
-// grouped loads and up to four fused reductions need without spills
-constexpr int kSpmvMinBlocks = 4;
+// (registers <= 65536 / (256 * blocks)): 5 (48 registers, 40 warps per SM:
+// the SpMV is latency-bound and gains more from resident warps than from
+// unrolling), 4 (64 registers) for kernels with three or more fused reductions
+constexpr int kSpmvMinBlocks = 5;
 constexpr int kSpmvMinBlocksWide = 4;
 
 template <typename T>
@@ -68,7 +69,6 @@ __device__ __forceinline__ T sell_row(const SellT<T>& A, int lane, const T* __re
   } else {
     const int64_t base = sb + 4 * lane;
     const int64_t stride = 4 * (int64_t)A.C;
-#pragma unroll 2
     for (int g = 0; g < (W >> 2); ++g) {
       const int64_t k = base + g * stride;
       const int4 c = __ldcs(reinterpret_cast<const int4*>(A.scol + k));
