@@ -61,6 +61,12 @@ class PbgpuCounters(C.Structure):
                 ("device_bytes", i64)]
 
 
+class PbgpuMeshBuild(C.Structure):
+    _fields_ = [("n_oct", i64), ("oct_xyz", P(i32)), ("oct_level", P(C.c_int8)), ("lo", dbl * 3), ("hi", dbl * 3),
+                ("locate_tol", dbl), ("refine", C.c_int), ("minlevel", C.c_int), ("maxlevel", C.c_int),
+                ("unilevel", C.c_int), ("n_spheres", i64), ("spheres", P(dbl))]
+
+
 class PbgpuRequest(C.Structure):
     _fields_ = [("mesh", P(PbgpuMesh)), ("rays", PbgpuRays * 3), ("n_atoms", i64), ("pos", P(dbl)),
                 ("charge", P(dbl)), ("model", P(PbgpuModel)), ("user_tag", i64)]
@@ -125,6 +131,8 @@ PBGPU_FUNCS = {
     "pbgpu_reset_counters": (C.c_int, [ctx_p]),
     "pbgpu_coulomb_energy_static": (C.c_int, [C.c_void_p, i64, dbl, dbl, C.c_void_p, C.c_void_p]),
     "pbgpu_autotune": (C.c_int, [ctx_p, C.c_int, P(PbgpuSellOpts), P(C.c_int), P(dbl)]),
+    "pbgpu_build_mesh": (C.c_int, [ctx_p, P(PbgpuMeshBuild)]),
+    "pbgpu_get_mesh_counts": (C.c_int, [ctx_p, P(i64), P(i64), P(i64), P(i64)]),
     "pbgpu_solve_charges": (C.c_int, [ctx_p, C.c_int, P(dbl), P(PbgpuSolverOpts), C.c_int, P(PbgpuEnergyOut),
                                       P(PbgpuSolveStats)]),
     "pbgpu_batch_create": (C.c_int, [P(C.c_void_p), C.c_int, C.c_void_p]),
@@ -161,6 +169,7 @@ PBHOST_FUNCS = {
     "pbhost_read_pqr": (C.c_int, [host_p, C.c_char_p]),
     "pbhost_set_atoms": (C.c_int, [host_p, i64, P(dbl), P(dbl), P(dbl)]),
     "pbhost_build_problem": (C.c_int, [host_p]),
+    "pbhost_build_on_gpu": (C.c_int, [host_p, C.c_void_p]),
     "pbhost_get_info": (C.c_int, [host_p, P(PbhostInfo)]),
     "pbhost_get_mesh": (C.c_int, [host_p, P(PbgpuMesh)]),
     "pbhost_get_rays": (C.c_int, [host_p, C.c_int, P(PbgpuRays)]),

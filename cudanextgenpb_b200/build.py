@@ -32,12 +32,12 @@ CXX = os.environ.get("PBGPU_CXX") or shutil.which("g++") or "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
            "-I" + os.path.join(ROOT, "include")]
-NO_FMA = {"k_markers.cu", "k_density.cu", "k_assemble.cu"}
+NO_FMA = {"k_markers.cu", "k_density.cu", "k_assemble.cu", "k_mesh.cu"}
 CXXFLAGS = ["-O3", "-std=c++17", "-fopenmp", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-function",
             "-I" + os.path.join(ROOT, "include")]
 
 GPU_SOURCES = ["pbgpu_api.cu", "k_markers.cu", "k_density.cu", "k_assemble.cu", "k_krylov.cu", "k_energy.cu",
-               "k_static.cu", "k_batch.cu", "pbgpu_server.cu", "k_multi.cu", "k_tune.cu"]
+               "k_static.cu", "k_batch.cu", "pbgpu_server.cu", "k_multi.cu", "k_tune.cu", "k_mesh.cu"]
 HOST_SOURCES = ["octree.cpp", "surface.cpp", "options.cpp", "pb_class.cpp", "pbhost_capi.cpp"]
 
 

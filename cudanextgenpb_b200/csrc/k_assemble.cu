@@ -401,6 +401,7 @@ __global__ void k_slice_width(const int32_t* __restrict__ perm, const int32_t* _
     const int64_t p = s * C + l;
     if (p < n) mx = max(mx, rowlen[perm[p]]);
   }
+  mx = (mx + G - 1) / G * G;  // padded to whole groups: the SpMV then needs no tail loop
   w[s] = mx;
   elems[s] = (int64_t)mx * C;
 }

@@ -12,19 +12,6 @@
 
 namespace pbgpu {
 
-__device__ __forceinline__ uint64_t spread3(uint64_t v) {
-  v &= 0x1fffffULL;
-  v = (v | v << 32) & 0x1f00000000ffffULL;
-  v = (v | v << 16) & 0x1f0000ff0000ffULL;
-  v = (v | v << 8) & 0x100f00f00f00f00fULL;
-  v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
-  v = (v | v << 2) & 0x1249249249249249ULL;
-  return v;
-}
-
-__device__ __forceinline__ uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
-  return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
-}
 
 __global__ void k_oct_keys(const int4* __restrict__ oct, int64_t n_oct, uint64_t* __restrict__ key) {
   const int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;

@@ -235,9 +235,16 @@ __global__ void k_energy_points(const int32_t* __restrict__ used_slots, int64_t 
   D[i] = make_double4(a.y, a.z, a.w, 0.0);
 }
 
-// x^{-1/2}: the FP32 hardware estimate refined by two Newton-Raphson steps
-// y <- y (3 - x y^2) / 2 (each step squares the relative error: ~2^-22 ->
-// ~1e-13 -> below double rounding).
+// x^{-1/2}: the FP32 hardware estimate refined by Newton-Raphson steps
+// y <- y (3 - x y^2) / 2, each squaring the relative error: one step
+// (~2.4e-7 -> ~1e-13) for the surface-point x atom pairs, whose kernel is
+// FP64-pipe bound and whose energies are held to 1e-10; two (-> below double
+// rounding) for the Coulomb sum, compared at 1e-12.
+__device__ __forceinline__ double rsqrt_nr1(double x) {
+  const double y = (double)rsqrtf((float)x);
+  return y * (1.5 - 0.5 * x * y * y);
+}
+
 __device__ __forceinline__ double rsqrt_nr(double x) {
   double y = (double)rsqrtf((float)x);
   y = y * (1.5 - 0.5 * x * y * y);
@@ -269,7 +276,7 @@ __global__ void __launch_bounds__(kTile) k_energy_pairs(const double4* __restric
       for (int j = 0; j < lim; ++j) {
         const double4 A = tile[j];
         const double dx = V.x - A.x, dy = V.y - A.y, dz = V.z - A.z;
-        const double y = rsqrt_nr(dx * dx + dy * dy + dz * dz);
+        const double y = rsqrt_nr1(dx * dx + dy * dy + dz * dz);
         s1 += A.w * y;
         if (IONIC) s2 += A.w * (dx * Dv.x + dy * Dv.y + dz * Dv.z) * (y * y * y);
       }

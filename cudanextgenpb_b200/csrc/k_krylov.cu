@@ -238,13 +238,14 @@ __global__ void k_cg_init(int64_t n, const T* __restrict__ b, const T* __restric
 }
 
 template <typename T, int G>
-__global__ void __launch_bounds__(kBlock, kSpmvMinBlocks) k_cg_spmv(SellT<T> A, const T* __restrict__ p, T* __restrict__ q, KrylovScalars* ks, double* partials) {
+__global__ void __launch_bounds__(kBlock, spmv_min_blocks<G>()) k_cg_spmv(SellT<T> A, const T* __restrict__ p, T* __restrict__ q, KrylovScalars* ks, double* partials) {
   if (ks->done) return;
   double v[1] = {0.0};
-  spmv_direct_rows<T, G>(A, p, [&](int64_t i, T y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x) {
+    const T y = sell_row<T, G>(A, i, p);
     q[i] = y;
     v[0] += (double)p[i] * (double)y;
-  });
+  }
   if (grid_sum<1>(v, partials, &ks->ticket[1]) && threadIdx.x == 0) {
     ks->pq = v[0];
     ks->alpha = ks->rz / v[0];
@@ -510,7 +511,7 @@ __global__ void k_bicg_p(int64_t n, T* __restrict__ p, T* __restrict__ ph, const
 
 // v = A ph;  alpha = rho_new / (rh, v)
 template <typename T, int G>
-__global__ void __launch_bounds__(kBlock, kSpmvMinBlocks) k_bicg_v(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh,
+__global__ void __launch_bounds__(kBlock, spmv_min_blocks<G>()) k_bicg_v(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh,
                          KrylovScalars* ks, double* partials) {
   if (ks->done) return;
   double s[1] = {0.0};
@@ -838,7 +839,7 @@ __device__ __forceinline__ bool spmv_rows(const SellT<T>& A, const T* __restrict
 
 // v = A ph;  alpha = rho / (rh, v)
 template <typename T, int G, int NC>
-__global__ void __launch_bounds__(kBlock, NC > 0 ? tma_min_blocks(NC) : G == 1 ? kSpmvMinBlocks : kSpmvMinBlocksWide)
+__global__ void __launch_bounds__(kBlock, NC > 0 ? tma_min_blocks(NC) : spmv_min_blocks<G>())
     k_cgs_v(SellT<T> A, const T* __restrict__ ph, T* __restrict__ v, const T* __restrict__ rh, KrylovScalars* ks,
             double* partials) {
   if (block_skip(ks, false)) return;

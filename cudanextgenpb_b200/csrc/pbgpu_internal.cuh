@@ -97,8 +97,8 @@ struct KrylovScalars {
 // `base` and has width W (columns), height C and column-group width G: the
 // first W - W % G columns are stored in groups of G lane-interleaved (a
 // thread loads a group with one vector load, a warp's loads of one group are
-// contiguous), the last W % G columns one per lane, so slice widths need no
-// padding to a multiple of G.
+// contiguous), the last W % G columns one per lane.  The assembly pads W to a
+// multiple of G, so the tail is empty for its matrices.
 __host__ __device__ __forceinline__ int64_t sell_elem(int64_t base, int W, int C, int G, int lane, int j) {
   const int Wg = W - W % G;
   if (j < Wg) return base + (int64_t)(j / G) * G * C + (int64_t)lane * G + j % G;
@@ -286,6 +286,21 @@ inline int cub_radix_launches(int64_t n, int bits) { return n <= 3584 ? 1 : 2 + 
 // lo + len * (i * 2^-19) with one rounding per operation, never contracted.
 __device__ __forceinline__ double coord(double lo, double len, int32_t i) {
   return __dadd_rn(lo, __dmul_rn(len, (double)i * 0x1p-19));
+}
+
+// Morton key of integer octree coordinates (x in the lowest bit).
+__device__ __forceinline__ uint64_t spread3(uint64_t v) {
+  v &= 0x1fffffULL;
+  v = (v | v << 32) & 0x1f00000000ffffULL;
+  v = (v | v << 16) & 0x1f0000ff0000ffULL;
+  v = (v | v << 8) & 0x100f00f00f00f00fULL;
+  v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+  v = (v | v << 2) & 0x1249249249249249ULL;
+  return v;
+}
+
+__device__ __forceinline__ uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
 }
 
 __device__ __forceinline__ uint64_t ray_key(int32_t a, int32_t b) {

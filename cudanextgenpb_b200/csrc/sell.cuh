@@ -15,6 +15,12 @@ constexpr int kBlock = 256;
 // unrolling), 4 (64 registers) for kernels with three or more fused reductions
 constexpr int kSpmvMinBlocks = 5;
 constexpr int kSpmvMinBlocksWide = 4;
+// the G = 4 row product (one group per iteration, no unrolling) fits in 40
+// registers: 6 blocks, 48 warps per SM, to keep more gathers in flight
+template <int G>
+__host__ __device__ constexpr int spmv_min_blocks() {
+  return G == 4 ? 6 : kSpmvMinBlocks;
+}
 
 template <typename T>
 struct SellT {
@@ -38,9 +44,11 @@ struct V2<float> {
   using t = float2;
 };
 
-// y_p = sum_j A(p, j) x_j for SELL row p, element j at sell_elem(): the
-// first W - W % G columns in groups of G (one vector load per group, a warp's
-// loads of one group contiguous), the remaining W % G columns one per lane.
+// y_p = sum_j A(p, j) x_j for SELL row p, element j at sell_elem(): columns
+// in groups of G (one vector load per group, a warp's loads of one group
+// contiguous).  The assembly pads slice widths to a multiple of G, so there
+// are no tail columns (a tail loop costs the registers that keep 40 warps per
+// SM resident; the padded layout measured faster despite its extra bytes).
 // (W and sb: width and first element of the row's slice, lane: the row's
 // position in it)
 template <typename T, int G>
@@ -69,6 +77,7 @@ __device__ __forceinline__ T sell_row(const SellT<T>& A, int lane, const T* __re
   } else {
     const int64_t base = sb + 4 * lane;
     const int64_t stride = 4 * (int64_t)A.C;
+#pragma unroll 1
     for (int g = 0; g < (W >> 2); ++g) {
       const int64_t k = base + g * stride;
       const int4 c = __ldcs(reinterpret_cast<const int4*>(A.scol + k));
@@ -87,13 +96,6 @@ __device__ __forceinline__ T sell_row(const SellT<T>& A, int lane, const T* __re
         acc += v.w * x[c.w];
       }
     }
-  }
-  // tail columns, one per lane
-  const int Wg = W - W % G;
-  const int64_t tb = sb + (int64_t)Wg * A.C + lane;
-  for (int j = Wg; j < W; ++j) {
-    const int64_t k = tb + (int64_t)(j - Wg) * A.C;
-    acc += __ldcs(A.sval + k) * x[__ldcs(A.scol + k)];
   }
   return acc;
 }

@@ -630,6 +630,58 @@ void poisson_boltzmann::build_problem() {
               << t3 - t2 << " s, " << tmsh.size() << " octants\n";
 }
 
+int poisson_boltzmann::build_problem_on_gpu(pbgpu_ctx* ctx) {
+  const double t0 = omp_get_wtime();
+  create_mesh();
+  if (mesh_shape == 0 || refine_box == 1 || mesh_shape == 4)
+    init_tmesh_with_refine_scale();
+  else if (mesh_shape == 3)
+    init_tmesh_with_refine_box_scale();
+  else
+    init_tmesh();
+  const int64_t no = tmsh.size();
+  std::vector<int32_t> xyz(3 * no);
+  std::vector<int8_t> lv(no);
+  for (int64_t i = 0; i < no; ++i) {
+    xyz[3 * i + 0] = tmsh.leaves[i].x;
+    xyz[3 * i + 1] = tmsh.leaves[i].y;
+    xyz[3 * i + 2] = tmsh.leaves[i].z;
+    lv[i] = (int8_t)tmsh.leaves[i].level;
+  }
+  std::vector<double> sph(4 * atoms.size());
+  for (size_t i = 0; i < atoms.size(); ++i) {
+    for (int k = 0; k < 3; ++k) sph[4 * i + k] = atoms[i].pos[k];
+    sph[4 * i + 3] = atoms[i].radius;
+  }
+  pbgpu_mesh_build b{};
+  b.n_oct = no;
+  b.oct_xyz = xyz.data();
+  b.oct_level = lv.data();
+  for (int a = 0; a < 3; ++a) {
+    b.lo[a] = dom.lo[a];
+    b.hi[a] = dom.hi[a];
+  }
+  b.locate_tol = locate_tol;
+  b.refine = (loc_refinement == 1 || mesh_shape == 4) ? 1 : 0;
+  b.minlevel = minlevel;
+  b.maxlevel = maxlevel;
+  b.unilevel = unilevel;
+  b.n_spheres = (int64_t)atoms.size();
+  b.spheres = sph.data();
+  gpu = ctx;
+  int st = check(pbgpu_build_mesh(ctx, &b));
+  if (st != PBGPU_OK) return st;
+  std::vector<double> pos(3 * pos_atoms.size());
+  for (size_t i = 0; i < pos_atoms.size(); ++i)
+    for (int k = 0; k < 3; ++k) pos[3 * i + k] = pos_atoms[i][k];
+  if ((st = check(pbgpu_set_atoms(ctx, (int64_t)pos_atoms.size(), pos.data(), charge_atoms.data()))) != PBGPU_OK)
+    return st;
+  const pbgpu_model md = model();
+  st = check(pbgpu_set_model(ctx, &md));
+  if (verbose) std::cerr << "build_problem_on_gpu: " << omp_get_wtime() - t0 << " s\n";
+  return st;
+}
+
 // ---------------------------------------------------------------------------
 // GPU path.
 pbgpu_model poisson_boltzmann::model() const {

@@ -95,6 +95,10 @@ struct poisson_boltzmann {
   void finalize_mesh();
   // Standard driver sequence up to finalize_mesh (src/poisson_boltzmann.cpp:112-188).
   void build_problem();
+  // The same problem with the surface refinement, nodes and ray tables built on
+  // the GPU (pbgpu_build_mesh) into `ctx`, which then also holds the atoms and
+  // the model: the domain and the initial octree are built here.
+  int build_problem_on_gpu(pbgpu_ctx* ctx);
 
   // ---- the GPU path (src/poisson_boltzmann.cpp:192-299)
   int upload();

@@ -117,6 +117,25 @@ int pbhost_build_problem(pbhost* h) {
   return PBGPU_OK;
 }
 
+int pbhost_build_on_gpu(pbhost* h, pbgpu_ctx* ctx) {
+  if (!h || !ctx) return PBGPU_ERR_ARG;
+  if (h->pb.atoms.empty()) {
+    h->err = "no atoms";
+    return PBGPU_ERR_STATE;
+  }
+  const char* v = std::getenv("PBHOST_VERBOSE");
+  h->pb.verbose = (v && *v && *v != '0') ? 1 : 0;
+  int st = PBGPU_OK;
+  try {
+    st = h->pb.build_problem_on_gpu(ctx);
+  } catch (const std::exception& ex) {
+    h->err = ex.what();
+    return PBGPU_ERR_ARG;
+  }
+  if (st != PBGPU_OK) h->err = h->pb.last_error;
+  return st;
+}
+
 int pbhost_get_info(const pbhost* h, pbhost_info* o) {
   if (!h || !o) return PBGPU_ERR_ARG;
   const pbh::poisson_boltzmann& p = h->pb;

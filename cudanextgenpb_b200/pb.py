@@ -86,6 +86,20 @@ class Problem:
             out[k] = list(v) if hasattr(v, "__len__") else v
         return out
 
+    def build_on_gpu(self, g: "GpuPath") -> "GpuPath":
+        """Domain and initial octree here, surface refinement, nodes and ray
+        tables on the GPU into g's context (which also gets the atoms and the
+        model); returns g, ready for create_markers."""
+        self._check(self._lib.pbhost_build_on_gpu(self._h, g._ctx))
+        no, nn, nh = C.c_int64(), C.c_int64(), C.c_int64()
+        nr = (C.c_int64 * 3)()
+        g._check(g._lib.pbgpu_get_mesh_counts(g._ctx, C.byref(no), C.byref(nn), C.byref(nh), nr))
+        g.n, g.n_oct, g.n_hang = nn.value, no.value, nh.value
+        g.n_rays = list(nr)
+        pos, q, _ = self.atoms()
+        g.n_atoms = len(q)
+        return g
+
     def mesh_struct(self) -> N.PbgpuMesh:
         m = N.PbgpuMesh()
         self._check(self._lib.pbhost_get_mesh(self._h, C.byref(m)))

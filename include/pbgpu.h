@@ -240,6 +240,30 @@ int pbgpu_reset_counters(pbgpu_ctx* ctx);
 int pbgpu_coulomb_energy_static(const double* atoms, int64_t n_atoms, double e_in, double T, double* out_energy,
                                 void* cuda_stream);
 
+/* ---- mesh construction on the GPU ----------------------------------------
+ * refine_surface (src/pb_class.cpp:1468-1745), the node numbering with hanging
+ * nodes (p8est_nodes / tmesh_3d) and the ray crossing tables of the three axes
+ * (NanoShaper's ray cache, src/raytracer.cpp:379-467; here the van der Waals
+ * union of the spheres), on the device.  Input: the initial octree that
+ * init_tmesh* builds (Morton order), the domain box, the refinement levels and
+ * the spheres (x, y, z, radius; radius <= 0 skipped).  Afterwards the context
+ * holds the mesh and rays as after pbgpu_set_mesh / pbgpu_set_rays, identical
+ * to the host build of the same problem. */
+typedef struct {
+  int64_t n_oct;
+  const int32_t* oct_xyz;    /* 3*n_oct */
+  const int8_t* oct_level;   /* n_oct */
+  double lo[3], hi[3];
+  double locate_tol;
+  int refine;                /* 1: run the surface refinement (loc_refinement == 1 or mesh_shape 4) */
+  int minlevel, maxlevel, unilevel;
+  int64_t n_spheres;
+  const double* spheres;     /* 4*n_spheres */
+} pbgpu_mesh_build;
+int pbgpu_build_mesh(pbgpu_ctx* ctx, const pbgpu_mesh_build* build);
+/* sizes of the context's mesh; n_rays: 3 entries (rays with crossings per axis) */
+int pbgpu_get_mesh_counts(pbgpu_ctx* ctx, int64_t* n_oct, int64_t* n_nodes, int64_t* n_hang, int64_t* n_rays);
+
 /* ---- SELL layout autotuner ----------------------------------------------
  * No counterpart in the reference.  Assembles the context's system (markers
  * and density map must be current) in each candidate layout (chunk 32 / 64,

@@ -47,6 +47,11 @@ int pbhost_set_atoms(pbhost* h, int64_t n, const double* pos, const double* char
 
 /* create_mesh + init_tmesh* + refine_surface + node/ray tables. */
 int pbhost_build_problem(pbhost* h);
+/* The domain and initial octree on the host, the surface refinement, nodes and
+ * ray tables on the GPU (pbgpu_build_mesh) into ctx, which also receives the
+ * atoms and the model; the host keeps no mesh (pbhost_get_mesh / _rays then
+ * describe nothing). */
+int pbhost_build_on_gpu(pbhost* h, pbgpu_ctx* ctx);
 /* Same with a caller-chosen domain (mesh_shape 2 box) and uniform/surface levels. */
 int pbhost_get_info(const pbhost* h, pbhost_info* out);
 int pbhost_get_mesh(const pbhost* h, pbgpu_mesh* out);

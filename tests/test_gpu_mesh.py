@@ -1,0 +1,48 @@
+"""Mesh construction on the GPU (pbgpu_build_mesh): surface refinement, nodes
+with hanging nodes and ray tables built on the device from the initial
+octree.  The host build of the same problem is the reference: identical
+sizes, identical markers, fractions, matrix and right-hand side, identical
+energies."""
+import numpy as np
+import pytest
+
+from cudanextgenpb_b200 import GpuPath, configs, solver_opts
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "born": lambda: configs.make_born_problem(5, 6),
+    "born_uniform": lambda: configs.make_born_problem(5, 5),
+    "mol60": lambda: configs.make_globular_problem(60, 7.0, -3.0, seed=60, levels=1),
+    "mol150": lambda: configs.make_globular_problem(150, 9.0, 2.0, seed=150, levels=2),
+    "mol300": lambda: configs.make_globular_problem(300, 11.0, -3.0, seed=300, levels=2),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_gpu_mesh_equals_host_mesh(name):
+    host = CASES[name]().build()
+    info = host.info()
+    g_host = GpuPath().load(host)
+    g_dev = CASES[name]().build_on_gpu(GpuPath())
+    assert (g_dev.n_oct, g_dev.n, g_dev.n_hang) == (info["n_oct"], info["n_nodes"], info["n_hang"])
+    assert g_dev.n_rays == list(info["n_rays"])
+    for g in (g_host, g_dev):
+        g.create_markers()
+        g.create_density_map()
+        g.assemble()
+    mh, bh = g_host.markers()
+    md, bd = g_dev.markers()
+    assert np.array_equal(mh, md) and np.array_equal(bh, bd)
+    assert np.array_equal(g_host.fractions(len(bh)), g_dev.fractions(len(bd)))
+    for a, b in zip(g_host.system(), g_dev.system()):
+        assert np.array_equal(a, b)
+    opts = solver_opts("cg", tol=1e-10)
+    g_host.solve(opts)
+    g_dev.solve(opts)
+    assert np.array_equal(g_host.phi(), g_dev.phi())
+    eh, ed = g_host.energy(), g_dev.energy()
+    for k in ("energy_pol", "energy_react", "energy_coul", "charge_flux"):
+        assert eh[k] == ed[k], k
+    g_host.close()
+    g_dev.close()
