@@ -55,6 +55,19 @@ class PbgpuEnergyOut(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class PbgpuPotFieldOut(C.Structure):
+    _fields_ = [("energy_pol", dbl), ("energy_react", dbl), ("energy_coul", dbl), ("charge_flux", dbl),
+                ("columns", C.c_int), ("reserved", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+# pot_field.dat column names in the order of the per-atom rows
+POT_FIELD_COLUMNS = ("phi_c", "phi_p", "phi_i", "Ex_c", "Ey_c", "Ez_c", "Ex_p", "Ey_p", "Ez_p",
+                     "Ex_i", "Ey_i", "Ez_i")
+
+
 class PbgpuCounters(C.Structure):
     _fields_ = [("launches", i64), ("spmv_launches", i64), ("spmv_ms", dbl), ("spmv_bytes", dbl),
                 ("krylov_iterations", i64), ("energy_points", i64), ("energy_pairs", i64),
@@ -117,6 +130,7 @@ PBGPU_FUNCS = {
     "pbgpu_solve": (C.c_int, [ctx_p, P(PbgpuSolverOpts), P(PbgpuSolveStats)]),
     "pbgpu_phi_on_atoms": (C.c_int, [ctx_p, P(dbl)]),
     "pbgpu_energy": (C.c_int, [ctx_p, C.c_int, P(PbgpuEnergyOut)]),
+    "pbgpu_pot_field": (C.c_int, [ctx_p, C.c_int, C.c_int, C.c_int, P(dbl), P(PbgpuPotFieldOut)]),
     "pbgpu_parse_lis_options": (C.c_int, [C.c_char_p, P(PbgpuSolverOpts)]),
     "pbgpu_default_solver_opts": (None, [P(PbgpuSolverOpts)]),
     "pbgpu_get_node_coeffs": (C.c_int, [ctx_p, P(dbl), P(dbl)]),

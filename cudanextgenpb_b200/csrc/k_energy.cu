@@ -235,23 +235,6 @@ __global__ void k_energy_points(const int32_t* __restrict__ used_slots, int64_t 
   D[i] = make_double4(a.y, a.z, a.w, 0.0);
 }
 
-// x^{-1/2}: the FP32 hardware estimate refined by Newton-Raphson steps
-// y <- y (3 - x y^2) / 2, each squaring the relative error: one step
-// (~2.4e-7 -> ~1e-13) for the surface-point x atom pairs, whose kernel is
-// FP64-pipe bound and whose energies are held to 1e-10; two (-> below double
-// rounding) for the Coulomb sum, compared at 1e-12.
-__device__ __forceinline__ double rsqrt_nr1(double x) {
-  const double y = (double)rsqrtf((float)x);
-  return y * (1.5 - 0.5 * x * y * y);
-}
-
-__device__ __forceinline__ double rsqrt_nr(double x) {
-  double y = (double)rsqrtf((float)x);
-  y = y * (1.5 - 0.5 * x * y * y);
-  y = y * (1.5 - 0.5 * x * y * y);
-  return y;
-}
-
 constexpr int kTile = 256;
 
 // (3) sum over points of F sum_a q_a / r  and  sum_a q_a (V - x_a).D / r^3
@@ -422,14 +405,22 @@ static int sum_partials(Context* c, const double* d, int nblk, int stride, doubl
   return PBGPU_OK;
 }
 
-int run_energy(Context* c, int fast, pbgpu_energy_out* out) {
-  if (!c->have_phi) return c->fail(PBGPU_ERR_STATE, "energy: solve has not run");
-  if (!c->have_markers) return c->fail(PBGPU_ERR_STATE, "energy: create_markers has not run");
+// The surface points of every border octant's elements, merged per crossing
+// (steps (1) and (2) above): P[i] = (V, F) and, with `ionic`, D[i] = sum of
+// coef * N of the triangle vertices on that crossing.  `fast` takes the
+// spacing of the first border octant for every octant, as energy_fast and
+// pot_field_fast do.  The lists live in the context's scratch slots.
+int surface_points(Context* c, int fast, bool ionic, SurfacePoints* out) {
+  out->P = nullptr;
+  out->D = nullptr;
+  out->n = 0;
   int st = ensure_tri(c);
   if (st != PBGPU_OK) return st;
   EnergyView E = energy_view(c, fast);
+  E.ionic = ionic;
   const int64_t nb = c->nb;
-  if (fast && nb > 0) {
+  if (nb == 0) return PBGPU_OK;
+  if (fast) {
     int32_t b0 = 0;
     int4 q;
     PBGPU_CUDA(c, cudaMemcpyAsync(&b0, c->border.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
@@ -444,10 +435,82 @@ int run_energy(Context* c, int fast, pbgpu_energy_out* out) {
       E.h0[a] = r - l;
     }
   }
+  const int64_t nslots = c->rays[0].nc + c->rays[1].nc + c->rays[2].nc;
+  const int64_t ns = nslots > 0 ? nslots : 1;
+  Scratch<double4> acc(c, kScEnAcc);
+  Scratch<uint8_t> used(c, kScEnUsed);
+  Scratch<int32_t> slot_ray(c, kScEnSlotRay), sel(c, kScEnSel);
+  Scratch<int64_t> nsel(c, kScEnNsel);
+  Scratch<unsigned long long> n_extra(c, kScEnNextra);
+  // elements whose edge carries no crossing (an epsilon jump seen through a
+  // hanging corner) keep their own point; their list starts at nb entries and
+  // is grown and the pass repeated if it overflows
+  int64_t extra_cap = nb + 1024;
+  Scratch<double4> xp(c, kScEnXp), xd(c, kScEnXd);
+  PBGPU_CUDA(c, acc.alloc(ns));
+  PBGPU_CUDA(c, used.alloc(ns));
+  PBGPU_CUDA(c, slot_ray.alloc(ns));
+  PBGPU_CUDA(c, sel.alloc(ns));
+  PBGPU_CUDA(c, nsel.alloc(1));
+  PBGPU_CUDA(c, n_extra.alloc(1));
+  E.acc = acc.get();
+  E.used = used.get();
+  E.slot_ray = slot_ray.get();
+  E.n_extra = n_extra.get();
+  unsigned long long nx = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    PBGPU_CUDA(c, xp.alloc(extra_cap));
+    PBGPU_CUDA(c, xd.alloc(extra_cap));
+    PBGPU_CUDA(c, cudaMemsetAsync(acc.get(), 0, ns * sizeof(double4), c->stream));
+    PBGPU_CUDA(c, cudaMemsetAsync(used.get(), 0, ns, c->stream));
+    PBGPU_CUDA(c, cudaMemsetAsync(n_extra.get(), 0, sizeof(unsigned long long), c->stream));
+    E.extra_p = xp.get();
+    E.extra_d = xd.get();
+    E.extra_cap = extra_cap;
+    k_energy_accumulate<<<grid_for(nb, 128), 128, 0, c->stream>>>(E);
+    PBGPU_LAUNCHED(c);
+    PBGPU_CUDA(c, cudaMemcpyAsync(&nx, n_extra.get(), sizeof(nx), cudaMemcpyDeviceToHost, c->stream));
+    PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    if ((int64_t)nx <= extra_cap) break;
+    extra_cap = (int64_t)nx;
+  }
+  if ((int64_t)nx > extra_cap) return c->fail(PBGPU_ERR_CAPACITY, "energy: surface element list overflow");
+  cub::CountingInputIterator<int32_t> idx(0);
+  size_t bytes = 0;
+  PBGPU_CUDA(c, cub::DeviceSelect::Flagged(nullptr, bytes, idx, used.get(), sel.get(), nsel.get(), ns, c->stream));
+  PBGPU_CUDA(c, ensure_tmp(c, bytes));
+  PBGPU_CUDA(c, cub::DeviceSelect::Flagged(c->tmp.get(), bytes, idx, used.get(), sel.get(), nsel.get(), ns, c->stream));
+  c->launches += kCubSelectLaunches;
+  int64_t np = 0;
+  PBGPU_CUDA(c, cudaMemcpyAsync(&np, nsel.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int64_t npts = np + (int64_t)nx;
+  Scratch<double4> P(c, kScEnP), D(c, kScEnD);
+  PBGPU_CUDA(c, P.alloc(npts > 0 ? npts : 1));
+  PBGPU_CUDA(c, D.alloc(npts > 0 ? npts : 1));
+  if (np) {
+    k_energy_points<<<grid_for(np, 256), 256, 0, c->stream>>>(sel.get(), np, E, P.get(), D.get());
+    PBGPU_LAUNCHED(c);
+  }
+  if (nx) {
+    PBGPU_CUDA(c, cudaMemcpyAsync(P.get() + np, xp.get(), nx * sizeof(double4), cudaMemcpyDeviceToDevice, c->stream));
+    PBGPU_CUDA(c, cudaMemcpyAsync(D.get() + np, xd.get(), nx * sizeof(double4), cudaMemcpyDeviceToDevice, c->stream));
+  }
+  out->P = P.get();
+  out->D = D.get();
+  out->n = npts;
+  return PBGPU_OK;
+}
+
+int run_energy(Context* c, int fast, pbgpu_energy_out* out) {
+  if (!c->have_phi) return c->fail(PBGPU_ERR_STATE, "energy: solve has not run");
+  if (!c->have_markers) return c->fail(PBGPU_ERR_STATE, "energy: create_markers has not run");
+  int st;
+  const int64_t nb = c->nb;
   const double inv_4pi = 1.0 / (4.0 * kPi);
   const double constant_pol = (1.0 / c->eps_out - 1.0 / c->eps_in) * inv_4pi;
   const double constant_react = (1.0 / c->eps_out) * inv_4pi;
-  const bool ionic = E.ionic;
+  const bool ionic = c->model.calc_energy == 2 && c->kappa > 1.e-5;
   const bool polar = c->model.calc_energy == 1 || (c->model.calc_energy == 2 && c->kappa < 1.e-5);
   // charged atoms (|q| > 1e-5, src/pb_class.cpp:2829-2834)
   std::vector<double4> ha(c->na);
@@ -469,75 +532,17 @@ int run_energy(Context* c, int fast, pbgpu_energy_out* out) {
   PBGPU_CUDA(c, c->energy_part.alloc(3 * nblk));
   double first_int = 0.0, second_int = 0.0, charge_pol = 0.0, coul = 0.0;
   if ((polar || ionic) && nb > 0) {
-    const int64_t nslots = c->rays[0].nc + c->rays[1].nc + c->rays[2].nc;
-    const int64_t ns = nslots > 0 ? nslots : 1;
-    Scratch<double4> acc(c, kScEnAcc);
-    Scratch<uint8_t> used(c, kScEnUsed);
-    Scratch<int32_t> slot_ray(c, kScEnSlotRay), sel(c, kScEnSel);
-    Scratch<int64_t> nsel(c, kScEnNsel);
-    Scratch<unsigned long long> n_extra(c, kScEnNextra);
-    // elements whose edge carries no crossing (an epsilon jump seen through a
-    // hanging corner) keep their own point; their list starts at nb entries and
-    // is grown and the pass repeated if it overflows
-    int64_t extra_cap = nb + 1024;
-    Scratch<double4> xp(c, kScEnXp), xd(c, kScEnXd);
-    PBGPU_CUDA(c, acc.alloc(ns));
-    PBGPU_CUDA(c, used.alloc(ns));
-    PBGPU_CUDA(c, slot_ray.alloc(ns));
-    PBGPU_CUDA(c, sel.alloc(ns));
-    PBGPU_CUDA(c, nsel.alloc(1));
-    PBGPU_CUDA(c, n_extra.alloc(1));
-    E.acc = acc.get();
-    E.used = used.get();
-    E.slot_ray = slot_ray.get();
-    E.n_extra = n_extra.get();
-    unsigned long long nx = 0;
-    for (int attempt = 0; attempt < 2; ++attempt) {
-      PBGPU_CUDA(c, xp.alloc(extra_cap));
-      PBGPU_CUDA(c, xd.alloc(extra_cap));
-      PBGPU_CUDA(c, cudaMemsetAsync(acc.get(), 0, ns * sizeof(double4), c->stream));
-      PBGPU_CUDA(c, cudaMemsetAsync(used.get(), 0, ns, c->stream));
-      PBGPU_CUDA(c, cudaMemsetAsync(n_extra.get(), 0, sizeof(unsigned long long), c->stream));
-      E.extra_p = xp.get();
-      E.extra_d = xd.get();
-      E.extra_cap = extra_cap;
-      k_energy_accumulate<<<grid_for(nb, 128), 128, 0, c->stream>>>(E);
-      PBGPU_LAUNCHED(c);
-      PBGPU_CUDA(c, cudaMemcpyAsync(&nx, n_extra.get(), sizeof(nx), cudaMemcpyDeviceToHost, c->stream));
-      PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
-      if ((int64_t)nx <= extra_cap) break;
-      extra_cap = (int64_t)nx;
-    }
-    if ((int64_t)nx > extra_cap) return c->fail(PBGPU_ERR_CAPACITY, "energy: surface element list overflow");
-    cub::CountingInputIterator<int32_t> idx(0);
-    size_t bytes = 0;
-    PBGPU_CUDA(c, cub::DeviceSelect::Flagged(nullptr, bytes, idx, used.get(), sel.get(), nsel.get(), ns, c->stream));
-    PBGPU_CUDA(c, ensure_tmp(c, bytes));
-    PBGPU_CUDA(c, cub::DeviceSelect::Flagged(c->tmp.get(), bytes, idx, used.get(), sel.get(), nsel.get(), ns, c->stream));
-    c->launches += kCubSelectLaunches;
-    int64_t np = 0;
-    PBGPU_CUDA(c, cudaMemcpyAsync(&np, nsel.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
-    PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
-    const int64_t npts = np + (int64_t)nx;
-    Scratch<double4> P(c, kScEnP), D(c, kScEnD);
-    PBGPU_CUDA(c, P.alloc(npts > 0 ? npts : 1));
-    PBGPU_CUDA(c, D.alloc(npts > 0 ? npts : 1));
-    if (np) {
-      k_energy_points<<<grid_for(np, 256), 256, 0, c->stream>>>(sel.get(), np, E, P.get(), D.get());
-      PBGPU_LAUNCHED(c);
-    }
-    if (nx) {
-      PBGPU_CUDA(c, cudaMemcpyAsync(P.get() + np, xp.get(), nx * sizeof(double4), cudaMemcpyDeviceToDevice, c->stream));
-      PBGPU_CUDA(c, cudaMemcpyAsync(D.get() + np, xd.get(), nx * sizeof(double4), cudaMemcpyDeviceToDevice, c->stream));
-    }
+    SurfacePoints sp;
+    if ((st = surface_points(c, fast, ionic, &sp)) != PBGPU_OK) return st;
+    const int64_t npts = sp.n;
     c->energy_points = npts;
     c->energy_pairs += npts * m;
     if (npts) {
       double s[3] = {0, 0, 0};
       if (ionic)
-        k_energy_pairs<true><<<nblk, kTile, 0, c->stream>>>(P.get(), D.get(), npts, dq.get(), m, c->energy_part.get());
+        k_energy_pairs<true><<<nblk, kTile, 0, c->stream>>>(sp.P, sp.D, npts, dq.get(), m, c->energy_part.get());
       else
-        k_energy_pairs<false><<<nblk, kTile, 0, c->stream>>>(P.get(), D.get(), npts, dq.get(), m, c->energy_part.get());
+        k_energy_pairs<false><<<nblk, kTile, 0, c->stream>>>(sp.P, sp.D, npts, dq.get(), m, c->energy_part.get());
       PBGPU_LAUNCHED(c);
       if ((st = sum_partials(c, c->energy_part.get(), nblk, 3, s)) != PBGPU_OK) return st;
       first_int = s[0];

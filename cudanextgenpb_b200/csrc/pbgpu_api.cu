@@ -404,6 +404,16 @@ int pbgpu_energy(pbgpu_ctx* h, int fast, pbgpu_energy_out* out) {
   return run_energy(c, fast, out);
 }
 
+// pot_field / pot_field_fast; its device time adds to the energy stage.
+int pbgpu_pot_field(pbgpu_ctx* h, int fast, int calc_potential_term, int calc_field_term, double* per_atom,
+                    pbgpu_pot_field_out* out) {
+  CTX_CHECK(h);
+  Context* c = &h->c;
+  SET_DEVICE(c);
+  StageTimer t(c, 5);
+  return run_pot_field(c, fast, calc_potential_term, calc_field_term, per_atom, out);
+}
+
 int pbgpu_solve_charges(pbgpu_ctx* h, int k, const double* charges, const pbgpu_solver_opts* o, int fast,
                         pbgpu_energy_out* energies, pbgpu_solve_stats* stats) {
   CTX_CHECK(h);

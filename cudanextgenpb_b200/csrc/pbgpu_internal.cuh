@@ -112,7 +112,7 @@ enum ScratchSlot {
   kScAsmOvf, kScAsmK0, kScAsmK1, kScAsmId0, kScAsmElems, kScAsmNnz, kScAsmCond, kScAsmKd, kScAsmFr,
   kScKrBad, kScKrRh32, kScKrV32, kScKrS32, kScKrT32, kScKrPh32, kScKrSh32,
   kScEnPhi, kScEnQ, kScEnAcc, kScEnUsed, kScEnSlotRay, kScEnSel, kScEnNsel, kScEnNextra, kScEnXp, kScEnXd,
-  kScEnP, kScEnD,
+  kScEnP, kScEnD, kScPfAtoms, kScPfPart, kScPfOut,
   kScInOctXyz, kScInOctLvl, kScInNodeXyz, kScInHangNp, kScInHangPar, kScInErr,
   kScratchSlots
 };
@@ -289,6 +289,23 @@ __device__ __forceinline__ double coord(double lo, double len, int32_t i) {
 }
 
 // Morton key of integer octree coordinates (x in the lowest bit).
+// x^{-1/2}: the FP32 hardware estimate refined by Newton-Raphson steps
+// y <- y (3 - x y^2) / 2, each squaring the relative error: one step
+// (~2.4e-7 -> ~1e-13) for the surface-point x atom pairs, whose kernel is
+// FP64-pipe bound and whose energies are held to 1e-10; two (-> below double
+// rounding) for the Coulomb sum, compared at 1e-12.
+__device__ __forceinline__ double rsqrt_nr1(double x) {
+  const double y = (double)rsqrtf((float)x);
+  return y * (1.5 - 0.5 * x * y * y);
+}
+
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  double y = (double)rsqrtf((float)x);
+  y = y * (1.5 - 0.5 * x * y * y);
+  y = y * (1.5 - 0.5 * x * y * y);
+  return y;
+}
+
 __device__ __forceinline__ uint64_t spread3(uint64_t v) {
   v &= 0x1fffffULL;
   v = (v | v << 32) & 0x1f00000000ffffULL;
@@ -380,6 +397,15 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o);
 int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st);
 int run_phi_atoms(Context* c, double* out);
 int run_energy(Context* c, int fast, pbgpu_energy_out* out);
+// surface points of the energy integrals, merged per crossing (k_energy.cu)
+struct SurfacePoints {
+  const double4* P;  // V, F
+  const double4* D;  // sum of coef * N (ionic)
+  int64_t n;
+};
+int surface_points(Context* c, int fast, bool ionic, SurfacePoints* out);
+int run_pot_field(Context* c, int fast, int calc_potential_term, int calc_field_term, double* per_atom,
+                  pbgpu_pot_field_out* out);
 int run_rhs(Context* c);
 bool tuned_layout(int64_t n, pbgpu_sell_opts* sell, int* cols);
 int run_solve_charges(Context* c, int k, const double* charges, const pbgpu_solver_opts* opts, int fast,

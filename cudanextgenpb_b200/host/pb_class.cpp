@@ -22,7 +22,7 @@ namespace pbh {
 static const double p4esttol = 1.0 / std::pow(2.0, kQMaxLevel);
 
 poisson_boltzmann::~poisson_boltzmann() {
-  if (gpu) pbgpu_ctx_destroy(gpu);
+  if (gpu && own_gpu) pbgpu_ctx_destroy(gpu);
 }
 
 // ---------------------------------------------------------------------------
@@ -82,6 +82,8 @@ void poisson_boltzmann::apply_options(const OptionFile& g) {
   T = g.get(md + "T", 298.15);
   calc_energy = g.get(md + "calc_energy", 2);
   calc_coulombic = g.get(md + "calc_coulombic", 0);
+  calc_potential_term = g.get(md + "calc_potential_terms", 0);
+  calc_field_term = g.get(md + "calc_field_terms", 0);
   atoms_write = g.get(md + "atoms_write", 0);
   const std::string s = "surface/";
   surf_type_num = g.get(s + "surface_type", 0);
@@ -668,7 +670,9 @@ int poisson_boltzmann::build_problem_on_gpu(pbgpu_ctx* ctx) {
   b.unilevel = unilevel;
   b.n_spheres = (int64_t)atoms.size();
   b.spheres = sph.data();
+  if (gpu && own_gpu && gpu != ctx) pbgpu_ctx_destroy(gpu);
   gpu = ctx;
+  own_gpu = false;
   int st = check(pbgpu_build_mesh(ctx, &b));
   if (st != PBGPU_OK) return st;
   std::vector<double> pos(3 * pos_atoms.size());
@@ -735,9 +739,12 @@ int poisson_boltzmann::check(int status) {
 
 int poisson_boltzmann::upload() {
   int st = PBGPU_OK;
-  if (!gpu && (st = pbgpu_ctx_create(&gpu, 0, nullptr)) != PBGPU_OK) {
-    last_error = "pbgpu_ctx_create failed";
-    return st;
+  if (!gpu) {
+    if ((st = pbgpu_ctx_create(&gpu, 0, nullptr)) != PBGPU_OK) {
+      last_error = "pbgpu_ctx_create failed";
+      return st;
+    }
+    own_gpu = true;
   }
   const pbgpu_mesh m = mesh_view();
   if ((st = check(pbgpu_set_mesh(gpu, &m))) != PBGPU_OK) return st;
@@ -834,6 +841,79 @@ static int run_energy(poisson_boltzmann& pb, int fast) {
 int poisson_boltzmann::energy() { return run_energy(*this, 0); }
 int poisson_boltzmann::energy_fast() { return run_energy(*this, 1); }
 
+// The heading line of pot_field.dat for each set of written columns
+// (src/pb_class.cpp:4279-4363; pot_field adds a space before the newline of the
+// phi_i-without-fields heading, :4982).
+static const char* pot_field_heading(int columns, int fast) {
+  const int kC = (1 << PBGPU_PF_PHI_C) | (7 << PBGPU_PF_EX_C);
+  const int kP = 1 << PBGPU_PF_PHI_P, kEP = 7 << PBGPU_PF_EX_P;
+  const int kI = 1 << PBGPU_PF_PHI_I, kEI = 7 << PBGPU_PF_EX_I;
+  if (columns == (kC | kP | kEP | kI | kEI))
+    return "phi_c    phi_p    phi_i    Ex_c    Ey_c    Ez_c   Ex_p    Ey_p    Ez_p   Ex_i    Ey_i    Ez_i\n";
+  if (columns == (kC | kP | kI))
+    return fast ? "phi_c    phi_p    phi_i    Ex_c    Ey_c    Ez_c\n" : "phi_c    phi_p    phi_i    Ex_c    Ey_c    Ez_c \n";
+  if (columns == (kC | kP | kEP | kI)) return "phi_c    phi_p    phi_i    Ex_c    Ey_c    Ez_c   Ex_p    Ey_p    Ez_p\n";
+  if (columns == (kC | kP)) return "phi_c    phi_p    Ex_c    Ey_c    Ez_c\n";
+  if (columns == (kC | kP | kEP)) return "phi_c    phi_p    Ex_c    Ey_c    Ez_c   Ex_p    Ey_p    Ez_p\n";
+  return "";
+}
+
+// pot_field / pot_field_fast: the GPU computes the rows; the energies and the
+// file follow the reference (:4252-4272 on stdout, :4277-4384 to the file,
+// setw(8) in the stream's default 6-significant-digit format).
+static int run_pot_field(poisson_boltzmann& pb, int fast, const std::string& path) {
+  const size_t na = pb.pos_atoms.size();
+  pb.pot_field_rows.assign(na * PBGPU_PF_COLUMNS, 0.0);
+  pbgpu_pot_field_out o{};
+  int st = pbgpu_pot_field(pb.gpu, fast, pb.calc_potential_term, pb.calc_field_term, pb.pot_field_rows.data(), &o);
+  if (st != PBGPU_OK) {
+    pb.last_error = pbgpu_last_error(pb.gpu);
+    return st;
+  }
+  pb.pot_field_columns = o.columns;
+  pb.energy_pol = o.energy_pol;
+  pb.energy_react = o.energy_react;
+  pb.coul_energy = o.energy_coul;
+  pb.charge_flux = o.charge_flux;
+  const int pt = pb.calc_potential_term, ft = pb.calc_field_term;
+  if (pb.verbose) {
+    const int w = 50;
+    std::cout << "\n================ [ Calculating Potential & Field Components ] =================\n";
+    if (pt == 1 || ft == 1 || pt == 2 || ft == 2)
+      std::cout << std::left << std::setw(w) << "  Polarization energy [kT]:" << std::setprecision(16) << o.energy_pol
+                << "\n";
+    if (pt == 2 || ft == 2)
+      std::cout << std::left << std::setw(w) << "  Direct ionic energy [kT]:" << std::setprecision(16)
+                << o.energy_react << "\n";
+    std::cout << std::left << std::setw(w) << "  Coulombic energy [kT]:" << std::setprecision(16) << o.energy_coul
+              << "\n";
+    std::cout << std::left << std::setw(w) << "  Sum of electrostatic energy contributions [kT]:"
+              << std::setprecision(16) << (o.energy_pol + o.energy_react + o.energy_coul) << "\n";
+    std::cout << "===========================================================\n";
+  }
+  if (path.empty()) return PBGPU_OK;
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) {
+    pb.last_error = "cannot write " + path;
+    return PBGPU_ERR_ARG;
+  }
+  std::fputs("# index    x    y    z    ", f);
+  std::fputs(pot_field_heading(o.columns, fast), f);
+  if (o.columns)
+    for (size_t i = 0; i < na; ++i) {
+      std::fprintf(f, "%5d  %8g  %8g  %8g  ", (int)(i + 1), pb.pos_atoms[i][0], pb.pos_atoms[i][1],
+                   pb.pos_atoms[i][2]);
+      for (int k = 0; k < PBGPU_PF_COLUMNS; ++k)
+        if ((o.columns >> k) & 1) std::fprintf(f, "%8g  ", pb.pot_field_rows[i * PBGPU_PF_COLUMNS + k]);
+      std::fputs("\n", f);
+    }
+  std::fclose(f);
+  return PBGPU_OK;
+}
+
+int poisson_boltzmann::pot_field(const std::string& path) { return run_pot_field(*this, 0, path); }
+int poisson_boltzmann::pot_field_fast(const std::string& path) { return run_pot_field(*this, 1, path); }
+
 // The driver's sequence from create_markers on (src/poisson_boltzmann.cpp:192-299).
 int poisson_boltzmann::run_gpu_path() {
   int st;
@@ -854,9 +934,18 @@ int poisson_boltzmann::run_gpu_path() {
     const int s2 = write_potential_on_atoms_fast();
     if (s2 != PBGPU_OK) return s2;
   }
-  if (calc_energy > 0) {
+  // :272-296
+  if (calc_potential_term > 0 || calc_field_term > 0 || calc_energy > 0) {
     const bool refined = (loc_refinement == 1 || mesh_shape > 2 || (mesh_shape == 2 && refine_box == 1));
-    const int s3 = refined ? energy() : energy_fast();
+    const bool pot_field_bool = (calc_potential_term > 0 || calc_field_term > 0);
+    int s3 = PBGPU_OK;
+    if (pot_field_bool) {
+      s3 = refined ? pot_field() : pot_field_fast();
+      if (s3 == PBGPU_OK && calc_energy > calc_potential_term && calc_energy > calc_field_term)
+        s3 = refined ? energy() : energy_fast();
+    } else {
+      s3 = refined ? energy() : energy_fast();
+    }
     if (s3 != PBGPU_OK) return s3;
   }
   return st;

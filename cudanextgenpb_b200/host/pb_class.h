@@ -47,6 +47,7 @@ struct poisson_boltzmann {
   double scale = 2.0, scale_min = 0.5, scale_max = 2.0, perfil1 = 0.8, perfil2 = 0.2;
   // [model]
   int linearized = 1, bc = 1, calc_energy = 2, calc_coulombic = 0, atoms_write = 0;
+  int calc_potential_term = 0, calc_field_term = 0;
   double e_in = 2.0, e_out = 80.0, ionic_strength = 0.145, T = 298.15;
   double net_charge = 0.0;
   // [surface]
@@ -58,6 +59,9 @@ struct poisson_boltzmann {
 
   // results (include/pb_class.h:126-128)
   double energy_pol = 0.0, energy_react = 0.0, coul_energy = 0.0, charge_flux = 0.0;
+  // pot_field results: one row of PBGPU_PF_COLUMNS values per atom
+  std::vector<double> pot_field_rows;
+  int pot_field_columns = 0;
   std::vector<double> phi_on_atoms;
   pbgpu_solve_stats solve_stats{};
 
@@ -73,8 +77,10 @@ struct poisson_boltzmann {
   double locate_tol = 0.0;
   int verbose = 0;
 
-  // GPU context of this problem
+  // GPU context of this problem; destroyed with the problem only when the
+  // problem created it (upload), not when a caller lent it (build_problem_on_gpu)
   pbgpu_ctx* gpu = nullptr;
+  bool own_gpu = false;
   std::string last_error;
 
   ~poisson_boltzmann();
@@ -110,6 +116,9 @@ struct poisson_boltzmann {
   int write_potential_on_atoms_fast(const std::string& path = "phi_on_atoms.txt");
   int energy();
   int energy_fast();
+  // per-atom potentials and fields, written to `path` (src/pb_class.cpp:3732-5060)
+  int pot_field(const std::string& path = "pot_field.dat");
+  int pot_field_fast(const std::string& path = "pot_field.dat");
   // Whole path in the reference's order; returns a pbgpu status.
   int run_gpu_path();
 

@@ -263,6 +263,16 @@ class GpuPath:
         self._check(self._lib.pbgpu_energy(self._ctx, 1 if fast else 0, C.byref(e)))
         return e.as_dict()
 
+    def pot_field(self, calc_potential_terms: int, calc_field_terms: int, fast=False):
+        """pot_field / pot_field_fast: (per-atom rows of the 12 columns in
+        N.POT_FIELD_COLUMNS order, dict of energies and the `columns` bitmask
+        of those the reference writes)."""
+        rows = np.zeros((self.n_atoms, len(N.POT_FIELD_COLUMNS)))
+        o = N.PbgpuPotFieldOut()
+        self._check(self._lib.pbgpu_pot_field(self._ctx, 1 if fast else 0, int(calc_potential_terms),
+                                              int(calc_field_terms), _dptr(rows), C.byref(o)))
+        return rows, o.as_dict()
+
     # ---- read-back
     def node_coeffs(self):
         eps, react = np.zeros(self.n), np.zeros(self.n)

@@ -15,6 +15,7 @@
  *                             poisson_boltzmann::mumps_compute_electric_potential :2200-2239
  *   pbgpu_phi_on_atoms        poisson_boltzmann::write_potential_on_atoms_fast    :2333-2417
  *   pbgpu_energy              poisson_boltzmann::energy / energy_fast              :2791-3338
+ *   pbgpu_pot_field           poisson_boltzmann::pot_field / pot_field_fast        :3732-5060
  *
  * Conventions (all plain C types; no framework types cross this boundary):
  *   - Every call returns an int status (PBGPU_OK = 0).  On failure
@@ -137,6 +138,26 @@ typedef struct {
   double sum;                /* energy_pol + energy_react + energy_coul */
 } pbgpu_energy_out;
 
+/* Per-atom columns of pbgpu_pot_field, in the order of the reference's
+ * pot_field.dat (src/pb_class.cpp:4282-4300): potentials phi_c (Coulomb),
+ * phi_p (polarisation), phi_i (ionic), then the field components of each. */
+enum {
+  PBGPU_PF_PHI_C = 0, PBGPU_PF_PHI_P = 1, PBGPU_PF_PHI_I = 2,
+  PBGPU_PF_EX_C = 3, PBGPU_PF_EY_C = 4, PBGPU_PF_EZ_C = 5,
+  PBGPU_PF_EX_P = 6, PBGPU_PF_EY_P = 7, PBGPU_PF_EZ_P = 8,
+  PBGPU_PF_EX_I = 9, PBGPU_PF_EY_I = 10, PBGPU_PF_EZ_I = 11,
+  PBGPU_PF_COLUMNS = 12
+};
+
+typedef struct {
+  double energy_pol;         /* polarisation energy [kT] (0 when the options compute none) */
+  double energy_react;       /* direct ionic energy [kT] (0 when the options compute none) */
+  double energy_coul;        /* Coulomb energy over all atom pairs [kT] */
+  double charge_flux;        /* sum of the flux elements / 4 pi [e] */
+  int columns;               /* bit k set: column k is written to pot_field.dat under these options */
+  int reserved;
+} pbgpu_pot_field_out;
+
 /* ---- context ---------------------------------------------------------- */
 int pbgpu_ctx_create(pbgpu_ctx** out, int device, void* cuda_stream /* NULL: own stream */);
 void pbgpu_ctx_destroy(pbgpu_ctx* ctx);
@@ -176,6 +197,15 @@ int pbgpu_solve(pbgpu_ctx* ctx, const pbgpu_solver_opts* opts, pbgpu_solve_stats
 int pbgpu_phi_on_atoms(pbgpu_ctx* ctx, double* phi_atoms /* n_atoms */);
 /* energy (fast = 0, src/pb_class.cpp:2791-3063) or energy_fast (fast = 1, :3066-3338). */
 int pbgpu_energy(pbgpu_ctx* ctx, int fast, pbgpu_energy_out* out);
+/* pot_field (fast = 0, src/pb_class.cpp:4390-5060) or pot_field_fast (fast = 1,
+ * :3732-4388): the potential and field at every atom, split into Coulomb,
+ * polarisation and ionic parts, for the model options calc_potential_terms and
+ * calc_field_terms (0, 1 or 2; src/pb_class.cpp:947-948).  per_atom (may be
+ * NULL) receives n_atoms rows of PBGPU_PF_COLUMNS doubles; columns that the
+ * options do not compute are 0, and out->columns names those the reference
+ * writes.  Every atom counts, charged or not, as in the reference. */
+int pbgpu_pot_field(pbgpu_ctx* ctx, int fast, int calc_potential_term, int calc_field_term, double* per_atom,
+                    pbgpu_pot_field_out* out);
 
 /* Parse a LIS option string ("-i bicgstab -p jacobi -tol 1.e-8 ...") into
  * solver options, the way lis_solver_set_option is fed at src/pb_class.cpp:2313.

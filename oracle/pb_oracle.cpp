@@ -1139,6 +1139,227 @@ int oracle_energy(oracle_state* s, int fast, pbgpu_energy_out* out) {
   return PBGPU_OK;
 }
 
+// pot_field / pot_field_fast (src/pb_class.cpp:3732-5060): the per-atom
+// Coulomb, polarisation and ionic potentials and fields.  The surface elements
+// are collected in the reference's order (border octants, then each octant's
+// flux edges, then its triangles' vertices) and every atom sums over them in
+// that order, with the reference's expressions; the Coulomb part is its i < j
+// pair loop (:3775-3814).  Same normal deviation as oracle_energy.
+int oracle_pot_field(oracle_state* s, int fast, int pt, int ft, double* per_atom, pbgpu_pot_field_out* out) {
+  if (!s->have_phi || !s->have_markers) return PBGPU_ERR_STATE;
+  if (pt < 0 || pt > 2 || ft < 0 || ft > 2 || !out) return PBGPU_ERR_ARG;
+  const double inv_4pi = 1.0 / (4.0 * kPi);
+  const double den_in = 1.0 / s->eps_in;
+  const double constant_pol = (1.0 / s->eps_out - 1.0 / s->eps_in) * inv_4pi;
+  const double constant_react = (1.0 / s->eps_out) * inv_4pi;
+  const double k = s->k;
+  const int64_t na = s->na;
+  const double* pos = s->pos.data();
+  const double* q = s->q.data();
+  std::vector<double> phi_c(na, 0.0), fcx(na, 0.0), fcy(na, 0.0), fcz(na, 0.0);
+  double coul = 0.0;
+  for (int64_t i = 0; i < na; ++i)
+    for (int64_t j = i + 1; j < na; ++j) {
+      const double dx = pos[3 * i] - pos[3 * j], dy = pos[3 * i + 1] - pos[3 * j + 1],
+                   dz = pos[3 * i + 2] - pos[3 * j + 2];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double r = std::sqrt(r2);
+      const double inv_r3 = 1.0 / (r2 * r);
+      coul += (q[i] * q[j]) / r * den_in;
+      phi_c[i] += q[j] / r * den_in;
+      phi_c[j] += q[i] / r * den_in;
+      fcx[i] += dx * inv_r3 * q[j] * den_in;
+      fcy[i] += dy * inv_r3 * q[j] * den_in;
+      fcz[i] += dz * inv_r3 * q[j] * den_in;
+      fcx[j] += -dx * inv_r3 * q[i] * den_in;
+      fcy[j] += -dy * inv_r3 * q[i] * den_in;
+      fcz[j] += -dz * inv_r3 * q[i] * den_in;
+    }
+  const bool a1 = (ft == 1 || (ft == 2 && k < 1.e-5)) && pt < 2;
+  const bool a2 = !a1 && (pt == 1 || (pt == 2 && k < 1.e-5)) && ft == 0;
+  const bool b1 = ft == 2 && k > 1.e-5;
+  const bool b2 = !b1 && (pt == 2 && k > 1.e-5) && ft == 0;
+  const bool b3 = !b1 && !b2 && (pt == 2 && k > 1.e-5) && ft == 1;
+  const bool surface = a1 || a2 || b1 || b2 || b3;
+  const bool ionic = b1 || b2 || b3;
+  // flux elements (V, F) and triangle vertices (V, N, phi_sup * area / 3 / 4 pi)
+  struct Flux {
+    double V[3], F;
+  };
+  struct Vert {
+    double V[3], N[3], ps, area;
+  };
+  std::vector<Flux> flux;
+  std::vector<Vert> verts;
+  double charge_pol = 0.0;
+  signed char tri[256][16];
+  pbmc::expand_tri_table(tri);
+  const int64_t nb = (int64_t)s->border.size();
+  double h0[3] = {0, 0, 0};
+  if (fast && nb) octant_h(s, s->border[0], h0);
+  if (surface)
+    for (int64_t b = 0; b < nb; ++b) {
+      const int64_t o = s->border[b];
+      double h[3];
+      if (fast)
+        for (int a = 0; a < 3; ++a) h[a] = h0[a];
+      else
+        octant_h(s, o, h);
+      const double area_h[3] = {h[1] * h[2] / h[0] * 0.25, h[0] * h[2] / h[1] * 0.25, h[0] * h[1] / h[2] * 0.25};
+      double te[8], tp[8];
+      for (int c = 0; c < 8; ++c) {
+        const int32_t nd = s->oct_nodes[8 * o + c];
+        te[c] = s->corner_val(s->eps, nd);
+        tp[c] = s->corner_val(s->phi, nd);
+      }
+      double N[3] = {0, 0, 0};
+      auto normal_intersection = [&](int e, double& fract) {
+        const int axis = EAX[e], i1 = E2N[2 * e], i2 = E2N[2 * e + 1];
+        const double x1 = s->corner_coord(o, i1, axis), x2 = s->corner_coord(o, i2, axis);
+        const double *I, *NN;
+        const int64_t mr = s->rays[axis].find(s->corner_ray(o, i1, axis), &I, &NN);
+        fract = 0.5;
+        for (int64_t t = 0; t < mr; ++t)
+          if (I[t] >= x1 && I[t] <= x2) {
+            N[0] = NN[3 * t];
+            N[1] = NN[3 * t + 1];
+            N[2] = NN[3 * t + 2];
+            fract = (I[t] - x1) / (x2 - x1);
+          }
+      };
+      auto vertex = [&](int e, double fract, double V[3]) {
+        const int axis = EAX[e], i1 = E2N[2 * e];
+        for (int a = 0; a < 3; ++a) V[a] = s->corner_coord(o, i1, a);
+        V[axis] += fract * h[axis];
+      };
+      int cube = 0;
+      if (ionic)
+        for (int v = 0; v < 8; ++v)
+          if (te[pbmc::kMcCorner[v]] < (s->eps_out - 1e-10)) cube |= 1 << v;
+      for (int e = 0; e < 12; ++e) {
+        const int i1 = E2N[2 * e], i2 = E2N[2 * e + 1];
+        double dir;
+        if (te[i1] < te[i2])
+          dir = 1;
+        else if (te[i1] > te[i2])
+          dir = -1;
+        else
+          continue;
+        double fract;
+        normal_intersection(e, fract);
+        Flux f;
+        vertex(e, fract, f.V);
+        f.F = -(tp[i2] - tp[i1]) * wha(te[i1], te[i2], fract) * dir * area_h[EAX[e]];
+        charge_pol += f.F;
+        flux.push_back(f);
+      }
+      if (!ionic || pbmc::cut_edges(cube) == 0) continue;
+      for (int t = 0; tri[cube][3 * t] != -1; ++t) {
+        Vert T[3];
+        for (int j = 0; j < 3; ++j) {
+          const int e = tri[cube][3 * t + j];
+          const int i1 = E2N[2 * e], i2 = E2N[2 * e + 1];
+          double fract;
+          normal_intersection(e, fract);
+          vertex(e, fract, T[j].V);
+          for (int a = 0; a < 3; ++a) T[j].N[a] = N[a];
+          T[j].ps = phi0(te[i1], te[i2], tp[i1], tp[i2], fract);
+        }
+        double ab[3], ac[3];
+        for (int a = 0; a < 3; ++a) {
+          ab[a] = T[0].V[a] - T[1].V[a];
+          ac[a] = T[0].V[a] - T[2].V[a];
+        }
+        const double area = 0.5 * std::hypot(ab[1] * ac[2] - ab[2] * ac[1], ab[0] * ac[2] - ab[2] * ac[0],
+                                             ab[1] * ac[0] - ab[0] * ac[1]);
+        for (int j = 0; j < 3; ++j) {
+          T[j].area = area;
+          verts.push_back(T[j]);
+        }
+      }
+    }
+  std::vector<double> pp(na, 0.0), fpx(na, 0.0), fpy(na, 0.0), fpz(na, 0.0);
+  std::vector<double> pi(na, 0.0), fix(na, 0.0), fiy(na, 0.0), fiz(na, 0.0);
+  std::vector<double> fi_a(na, 0.0), si_a(na, 0.0);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t ia = 0; ia < na; ++ia) {
+    const double* ra = &pos[3 * ia];
+    double first = 0.0, second = 0.0;
+    for (const Flux& f : flux) {
+      const double dx = ra[0] - f.V[0], dy = ra[1] - f.V[1], dz = ra[2] - f.V[2];
+      const double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+      const double inv_r3 = 1.0 / (r * r * r);
+      const double qflux = f.F / r;
+      first += q[ia] * qflux;
+      pp[ia] += qflux * constant_pol;
+      fpx[ia] += dx * inv_r3 * f.F * constant_pol;
+      fpy[ia] += dy * inv_r3 * f.F * constant_pol;
+      fpz[ia] += dz * inv_r3 * f.F * constant_pol;
+    }
+    for (const Vert& v : verts) {
+      const double d0 = v.V[0] - ra[0], d1 = v.V[1] - ra[1], d2 = v.V[2] - ra[2];
+      const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+      const double r = std::sqrt(r2);
+      const double inv_r3 = 1.0 / (r2 * r);
+      const double inv_r5 = inv_r3 / r2;
+      const double dot = d0 * v.N[0] + d1 * v.N[1] + d2 * v.N[2];
+      const double factor = v.ps * inv_4pi * v.area / 3.0;
+      second += q[ia] * v.ps * dot * inv_r3 * inv_4pi * v.area / 3.0;
+      pi[ia] += v.ps * dot * inv_r3 * inv_4pi * v.area / 3.0;
+      fix[ia] += factor * (-3 * d0 * inv_r5 * dot + v.N[0] * inv_r3);
+      fiy[ia] += factor * (-3 * d1 * inv_r5 * dot + v.N[1] * inv_r3);
+      fiz[ia] += factor * (-3 * d2 * inv_r5 * dot + v.N[2] * inv_r3);
+    }
+    fi_a[ia] = first;
+    si_a[ia] = second;
+  }
+  double first_int = 0.0, second_int = 0.0;
+  for (int64_t ia = 0; ia < na; ++ia) {
+    first_int += fi_a[ia];
+    second_int += si_a[ia];
+  }
+  // print-time correction (:4285-4288) and the written columns (:4281-4375)
+  const int kC = (1 << PBGPU_PF_PHI_C) | (7 << PBGPU_PF_EX_C);
+  const int kP = 1 << PBGPU_PF_PHI_P, kEP = 7 << PBGPU_PF_EX_P;
+  const int kI = 1 << PBGPU_PF_PHI_I, kEI = 7 << PBGPU_PF_EX_I;
+  int columns = 0;
+  if (b1)
+    columns = kC | kP | kEP | kI | kEI;
+  else if (b2)
+    columns = kC | kP | kI;
+  else if (b3)
+    columns = kC | kP | kEP | kI;
+  else if (a2)
+    columns = kC | kP;
+  else if (a1)
+    columns = kC | kP | kEP;
+  if (per_atom)
+    for (int64_t i = 0; i < na; ++i) {
+      double v[PBGPU_PF_COLUMNS];
+      v[PBGPU_PF_PHI_C] = phi_c[i];
+      v[PBGPU_PF_EX_C] = fcx[i];
+      v[PBGPU_PF_EY_C] = fcy[i];
+      v[PBGPU_PF_EZ_C] = fcz[i];
+      v[PBGPU_PF_PHI_P] = pp[i];
+      v[PBGPU_PF_EX_P] = fpx[i];
+      v[PBGPU_PF_EY_P] = fpy[i];
+      v[PBGPU_PF_EZ_P] = fpz[i];
+      v[PBGPU_PF_PHI_I] = pi[i] - pp[i] / constant_pol * constant_react;
+      v[PBGPU_PF_EX_I] = fix[i] - fpx[i] / constant_pol * constant_react;
+      v[PBGPU_PF_EY_I] = fiy[i] - fpy[i] / constant_pol * constant_react;
+      v[PBGPU_PF_EZ_I] = fiz[i] - fpz[i] / constant_pol * constant_react;
+      for (int c = 0; c < PBGPU_PF_COLUMNS; ++c) per_atom[PBGPU_PF_COLUMNS * i + c] = ((columns >> c) & 1) ? v[c] : 0.0;
+    }
+  pbgpu_pot_field_out o{};
+  o.energy_pol = surface ? 0.5 * constant_pol * first_int : 0.0;
+  o.energy_react = ionic ? 0.5 * (second_int - first_int * constant_react) : 0.0;
+  o.energy_coul = coul;
+  o.charge_flux = surface ? charge_pol / (4.0 * kPi) : 0.0;
+  o.columns = columns;
+  *out = o;
+  return PBGPU_OK;
+}
+
 int oracle_get_node_coeffs(const oracle_state* s, double* eps, double* react) {
   if (!s->have_markers) return PBGPU_ERR_STATE;
   if (eps) std::copy(s->eps.begin(), s->eps.end(), eps);

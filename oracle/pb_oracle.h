@@ -18,6 +18,7 @@
  *                      preconditioning), solved tight as MUMPS stand-in
  *   potential at atoms write_potential_on_atoms_fast :2333-2417
  *   energy             energy :2791-3063, energy_fast :3066-3338
+ *   per-atom phi / E   pot_field :4390-5060, pot_field_fast :3732-4388
  *
  * PARITY UNPINNED: the reference cannot be built here (bimpp, p4est, LIS, MUMPS
  * and NanoShaper are absent) and ships no tests or golden outputs.  The oracle
@@ -60,6 +61,10 @@ int oracle_solve_ex(oracle_state* s, int method, int precond, int conv_cond, dou
                     int threads, double* rel_residual);
 int oracle_phi_on_atoms(oracle_state* s, double* out);
 int oracle_energy(oracle_state* s, int fast, pbgpu_energy_out* out);
+/* pot_field (fast = 0) / pot_field_fast (fast = 1): per-atom rows of
+ * PBGPU_PF_COLUMNS values (may be NULL), energies and the written columns */
+int oracle_pot_field(oracle_state* s, int fast, int calc_potential_term, int calc_field_term, double* per_atom,
+                     pbgpu_pot_field_out* out);
 
 /* getters, same layouts as the pbgpu_get_* calls */
 int oracle_get_node_coeffs(const oracle_state* s, double* eps, double* react);

@@ -37,6 +37,7 @@ def load():
                                       P(C.c_double)]
         L.oracle_phi_on_atoms.argtypes = [sp, P(C.c_double)]
         L.oracle_energy.argtypes = [sp, C.c_int, P(N.PbgpuEnergyOut)]
+        L.oracle_pot_field.argtypes = [sp, C.c_int, C.c_int, C.c_int, P(C.c_double), P(N.PbgpuPotFieldOut)]
         L.oracle_get_node_coeffs.argtypes = [sp, P(C.c_double), P(C.c_double)]
         L.oracle_get_markers.argtypes = [sp, P(C.c_double), P(C.c_int64), P(C.c_int32)]
         L.oracle_get_fractions.argtypes = [sp, P(C.c_double)]
@@ -163,6 +164,13 @@ class Oracle:
         e = N.PbgpuEnergyOut()
         self._ok(self.L.oracle_energy(self.s, 1 if fast else 0, C.byref(e)))
         return e.as_dict()
+
+    def pot_field(self, calc_potential_terms, calc_field_terms, fast=False):
+        rows = np.zeros((self.na, len(N.POT_FIELD_COLUMNS)))
+        o = N.PbgpuPotFieldOut()
+        self._ok(self.L.oracle_pot_field(self.s, 1 if fast else 0, int(calc_potential_terms),
+                                         int(calc_field_terms), _d(rows), C.byref(o)))
+        return rows, o.as_dict()
 
     def spmv(self, x, threads=0):
         x = np.ascontiguousarray(x, dtype=np.float64)

@@ -9,7 +9,8 @@ import pytest
 import scipy.sparse as sp
 import scipy.sparse.linalg as spla
 
-from cudanextgenpb_b200 import configs
+from cudanextgenpb_b200 import Problem, configs
+from cudanextgenpb_b200._native import POT_FIELD_COLUMNS
 from oracle_lib import Oracle
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -174,3 +175,65 @@ def test_cgs_and_conv_cond(born):
     _, it4, _ = o.solve("cgs", 1e-4, precond="block_jacobi", conv_cond=2, tol_w=0.0)
     _, it6, _ = o.solve("cgs", 1e-6, precond="block_jacobi", conv_cond=2, tol_w=0.0)
     assert it4 < it6
+
+
+def _born_pair(salt=True):
+    text = configs.born_options(4, 5)
+    if not salt:
+        text = text.replace("ionic_strength = 0.145", "ionic_strength = 0")
+    prob = Problem(text)
+    prob.set_atoms(*configs.BORN_ATOM)
+    o = Oracle(prob.build())
+    o.markers()
+    o.density()
+    o.assemble()
+    o.solve("cg", 1e-12)
+    return o
+
+
+def test_pot_field_column_sets():
+    """pot_field writes the columns of the reference's print branches
+    (src/pb_class.cpp:4281-4375), which depend on the options and on salt."""
+    c = lambda *names: sum(1 << POT_FIELD_COLUMNS.index(n) for n in names)
+    base = c("phi_c", "Ex_c", "Ey_c", "Ez_c")
+    ep = c("Ex_p", "Ey_p", "Ez_p")
+    ei = c("Ex_i", "Ey_i", "Ez_i")
+    salt = {(0, 0): 0, (1, 0): base | c("phi_p"), (2, 0): base | c("phi_p", "phi_i"),
+            (0, 1): base | c("phi_p") | ep, (1, 1): base | c("phi_p") | ep,
+            (2, 1): base | c("phi_p", "phi_i") | ep,
+            (0, 2): base | c("phi_p", "phi_i") | ep | ei, (1, 2): base | c("phi_p", "phi_i") | ep | ei,
+            (2, 2): base | c("phi_p", "phi_i") | ep | ei}
+    no_salt = {(0, 0): 0, (1, 0): base | c("phi_p"), (2, 0): base | c("phi_p"),
+               (0, 1): base | c("phi_p") | ep, (1, 1): base | c("phi_p") | ep, (2, 1): 0,
+               (0, 2): base | c("phi_p") | ep, (1, 2): base | c("phi_p") | ep, (2, 2): 0}
+    for salty, table in ((True, salt), (False, no_salt)):
+        o = _born_pair(salty)
+        for (pt, ft), cols in table.items():
+            rows, e = o.pot_field(pt, ft)
+            assert e["columns"] == cols, (salty, pt, ft)
+            for k in range(len(POT_FIELD_COLUMNS)):
+                if not (cols >> k) & 1:
+                    assert np.all(rows[:, k] == 0.0)
+        o.close()
+
+
+def test_pot_field_consistent_with_energy():
+    """The per-atom decomposition carries the energy routine's energies: the
+    polarisation energy is 1/2 sum q phi_p, and by symmetry the reaction field
+    at the Born ion's centre vanishes next to its potential."""
+    o = _born_pair(True)
+    e = o.energy()
+    rows, pe = o.pot_field(2, 2)
+    for k in ("energy_pol", "energy_react", "charge_flux"):
+        assert pe[k] == pytest.approx(e[k], rel=1e-12), k
+    q = 1.0
+    assert 0.5 * q * rows[0, POT_FIELD_COLUMNS.index("phi_p")] == pytest.approx(e["energy_pol"], rel=1e-12)
+    # dummies at +-0.001 A carry the ion's Coulomb potential q / (eps_in r)
+    eps_in, _, _ = configs.scaled_constants()
+    assert rows[1:, 0] == pytest.approx(1.0 / (eps_in * 0.001), rel=1e-9)
+    phi_p = abs(rows[0, POT_FIELD_COLUMNS.index("phi_p")])
+    ex, ey, ez = np.abs(rows[0, [POT_FIELD_COLUMNS.index(n) for n in ("Ex_p", "Ey_p", "Ez_p")]])
+    # the mesh is mirror-symmetric in x and y; z, the axis of the in/out rays,
+    # keeps a discretisation-sized asymmetry
+    assert max(ex, ey) < 1e-9 * phi_p / 2.0 and ez < 1e-3 * phi_p / 2.0
+    o.close()
