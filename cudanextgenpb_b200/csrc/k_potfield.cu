@@ -23,6 +23,10 @@
 // and in coef * N).  The Coulomb part runs over all atom pairs j != i:
 //   phi_c = sum q_j / r / eps_in,   E_c = sum q_j (x_i - x_j) / r^3 / eps_in.
 // Every atom counts, charged or not, as in the reference's loops.
+//
+// The surface kernel is bound by the FP64 pipe; 1/r takes one Newton step
+// from the FP32 estimate (relative error ~1e-13 per term), the Coulomb kernel
+// two.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -70,7 +74,7 @@ __global__ void __launch_bounds__(kPfTile) k_pf_surface(const double4* __restric
     for (int j = 0; j < lim; ++j) {
       const double4 V = sP[j];
       const double dx = A.x - V.x, dy = A.y - V.y, dz = A.z - V.z;
-      const double y = rsqrt_nr(dx * dx + dy * dy + dz * dz);
+      const double y = rsqrt_nr1(dx * dx + dy * dy + dz * dz);
       sp += V.w * y;
       double y3 = 0.0;
       if (FIELD || IONIC) y3 = y * y * y;

@@ -4,8 +4,12 @@ of the reference's element loops (src/pb_class.cpp:3732-5060).
 Both sides use the same potential, so the only differences are the order of
 the sums (the GPU merges the elements on a crossing and sums per atom) and the
 last bits of the surface point coordinates.  Per-atom columns must agree to
-1e-9 of each column's largest magnitude; energies to 1e-10 relative; the set
-of written columns must be identical for every option pair."""
+1e-9 of the size of their summands: a potential column to 1e-9 of its
+largest magnitude, a field column to 1e-9 of the largest of its part's field
+and potential (per angstrom) -- a field that cancels to almost nothing, as
+the reaction field inside the Born sphere does, keeps only rounding noise of
+the terms.  Energies agree to 1e-10 relative, and the set of written columns
+is identical for every option pair."""
 import numpy as np
 import pytest
 
@@ -54,12 +58,19 @@ def solved(request):
     o.close()
 
 
+PART = {"c": (0, 3, 4, 5), "p": (1, 6, 7, 8), "i": (2, 9, 10, 11)}
+
+
 def _close_columns(gr, orows, columns):
     for k, name in enumerate(N.POT_FIELD_COLUMNS):
         if not (columns >> k) & 1:
             assert np.all(gr[:, k] == 0.0) and np.all(orows[:, k] == 0.0), name
             continue
-        scale = max(np.abs(orows[:, k]).max(), 1e-300)
+        scale = np.abs(orows[:, k]).max()
+        if name.startswith("E"):
+            cols = list(PART[name[-1]])
+            scale = max(scale, np.abs(orows[:, cols]).max())
+        scale = max(scale, 1e-300)
         err = np.abs(gr[:, k] - orows[:, k]).max()
         assert err <= 1e-9 * scale, (name, err, scale)
 
