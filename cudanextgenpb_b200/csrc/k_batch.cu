@@ -6,12 +6,16 @@
 //
 // Design:
 //  * Every member keeps its own SELL matrix and vectors; the kernel walks a
-//    table of member descriptors.  Rows are grouped in row-blocks of 256 rows,
-//    each row-block belongs to one member (rb_sys table), and the persistent
-//    blocks stride over all row-blocks.
+//    table of member descriptors.  Rows are grouped in row-blocks of 256 rows.
+//  * Every member owns a group of the resident CTAs, sized in proportion to
+//    its row-blocks (at least one); a CTA works for one member only and owns
+//    the same rows in every phase.  Members never wait for one another: the
+//    barriers between phases are per member, over its group alone, and a
+//    member that has converged lets its CTAs return.
 //  * Reductions are per member and deterministic: each row-block writes its
-//    partial sums, and after a grid barrier one warp per member sums that
-//    member's row-block partials in a fixed order and updates its scalars.
+//    partial sums, and the last CTA of the group to reach the barrier sums
+//    them with one warp in a fixed order and updates the member's scalars
+//    before it releases the others.
 //  * Each member runs Jacobi-preconditioned CG on A d = r in the inner type
 //    TI (float: FP32 matrix and vectors; double: plain FP64) with the
 //    solution accumulated in FP64.  In FP32 the CG uses reliable updates:
@@ -22,9 +26,9 @@
 //    convergence test.  Members move through these phases independently:
 //    one step of the kernel does one CG iteration for members in the inner
 //    phase and the residual / start / update work for the others.
-//  * A step has five row phases separated by a grid barrier (bounded spin:
-//    a barrier that times out sets an error flag and every block returns).
-//  * The kernel leaves early once every member is done.
+//  * A step has three row phases, each closed by the member's barrier
+//    (bounded spin: a barrier that times out sets an error flag and every
+//    CTA returns at its next barrier).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -76,46 +80,61 @@ struct BState {
   int phase, iters, inner_it, outer, status, max_iter, inner_cap, plain;
 };
 
-struct GridBar {
+// Barrier of one member's CTA group (count of arrivals, generation).
+struct MemBar {
   unsigned count;
   unsigned gen;
-  int err;
-  unsigned active[2];  // members not done, per step parity
 };
 
-// Generation barrier over all blocks of a cooperative launch; the wait is
-// bounded (about 2 s of wall time), after which err is set and every caller
-// returns false.
-__device__ __forceinline__ bool grid_barrier(GridBar* g) {
+// A CTA's assignment: the member slot it works for, its index in the
+// member's group and the group's size.
+struct CtaGroup {
+  int slot, k, size, pad;
+};
+
+// Barrier over the `size` CTAs of one member's group.  The last CTA to arrive
+// runs `last` (the member's reduction and scalar update) before it releases
+// the others.  The wait is bounded (about 2 s of wall time), after which the
+// shared error flag is set; every caller then returns false.
+template <class F>
+__device__ __forceinline__ bool member_barrier(MemBar* b, int size, int* err, F&& last) {
+  __shared__ int is_last;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* vgen = &g->gen;
+    volatile unsigned* vgen = &b->gen;
     const unsigned gen = *vgen;
     __threadfence();
-    if (atomicAdd(&g->count, 1u) == gridDim.x - 1) {
-      g->count = 0;
-      __threadfence();
-      atomicAdd(&g->gen, 1u);
-    } else {
+    is_last = atomicAdd(&b->count, 1u) == (unsigned)size - 1u;
+    if (!is_last) {
       const uint64_t t0 = global_ns();
       uint32_t it = 0;
       while (*vgen == gen) {
         if ((++it & 255u) == 0 && global_ns() - t0 > 2000000000ull) {
-          atomicExch(&g->err, 1);
+          atomicExch(err, 1);
           break;
         }
-        if (*reinterpret_cast<volatile int*>(&g->err)) break;
+        if (*reinterpret_cast<volatile int*>(err)) break;
       }
     }
     __threadfence();
   }
   __syncthreads();
-  return *reinterpret_cast<volatile int*>(&g->err) == 0;
+  if (is_last) {
+    last();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      b->count = 0;
+      __threadfence();
+      atomicAdd(&b->gen, 1u);
+    }
+  }
+  __syncthreads();
+  return *reinterpret_cast<volatile int*>(err) == 0;
 }
 
-// Member scalars and row-block partials, which other blocks of the running
+// Member scalars and row-block partials, which other CTAs of the running
 // kernel write, are read through L2 only (ld.global.cg).  The gathered vector
-// entries are plain loads (L1-cached): they are read only after a grid
+// entries are plain loads (L1-cached): they are read only after a member
 // barrier whose acquire fence (fence.sc.gpu) orders them after the writers'
 // release, never through the read-only path.  Every row is owned by the same
 // thread in every phase, so a thread's own rows need no care.
@@ -182,23 +201,109 @@ __device__ __forceinline__ void member_sum(const double* part, int64_t rb0, int 
     for (int o = 16; o > 0; o >>= 1) out[k] += __shfl_xor_sync(0xffffffffu, out[k], o);
 }
 
+// Member decisions after the first phase (warp 0 of the group's last CTA):
+// the FP64 residual norm of an outer step, or alpha of a CG iteration.
+template <typename TI>
+__device__ __forceinline__ void member_after_spmv(BState& S, const BMember<TI>& M, const double* part) {
+  const int lane = threadIdx.x & 31;
+  const int ph = ldcg(&S.phase);
+  if (ph == kPhDone || ph == kPhStart || ph == kPhResume) return;
+  double a[2];
+  member_sum<2>(part, M.rb0, M.nrb, a);
+  if (lane != 0) return;
+  if (ph == kPhOuter || ph == kPhApply || ph == kPhReliable) {
+    if (S.outer == 0) {
+      S.bb = a[1];
+      S.tol2 = S.tol2 * a[1];  // tol^2 was stored; scale by ||b||^2
+    }
+    S.rr64 = a[0];
+    S.outer += 1;
+    if (!isfinite(a[0])) {
+      S.status = PBGPU_BREAKDOWN;
+      S.phase = kPhDone;
+    } else if (a[0] <= S.tol2) {
+      S.phase = kPhDone;
+    } else if (S.iters >= S.max_iter) {
+      S.status = PBGPU_NOT_CONVERGED;
+      S.phase = kPhDone;
+    } else {
+      // the TI recursion aims at the final target; with reliable updates
+      // (mixed precision) its residual is refreshed from FP64 on the way
+      S.rr_ref = a[0];
+      S.tol2i = S.tol2;
+      S.phase = ph == kPhOuter ? kPhStart : kPhResume;
+      S.inner_it = 0;
+    }
+  } else {  // inner
+    const double alpha = S.rz / a[0];
+    if (!(a[0] > 0.0) || !isfinite(alpha)) {
+      S.status = PBGPU_BREAKDOWN;
+      S.phase = kPhDone;
+    } else {
+      S.alpha = alpha;
+    }
+  }
+}
+
+// Member decisions after the second phase: rz of a (re)start, or beta and the
+// stopping tests of a CG iteration.
+template <typename TI>
+__device__ __forceinline__ void member_after_update(BState& S, const BMember<TI>& M, const double* part) {
+  const int lane = threadIdx.x & 31;
+  const int ph = ldcg(&S.phase);
+  if (ph != kPhStart && ph != kPhResume && ph != kPhInner) return;
+  double a[2];
+  member_sum<2>(part, M.rb0, M.nrb, a);
+  if (lane != 0) return;
+  if (ph == kPhStart) {
+    S.rz = a[0];
+    S.phase = kPhInner;
+  } else if (ph == kPhResume) {
+    // CG continues from the fresh residual: p = z + beta p in the third phase
+    S.beta = a[0] / S.rz;
+    S.rz = a[0];
+    S.phase = isfinite(S.beta) ? kPhInner : kPhDone;
+    if (S.phase == kPhDone) S.status = PBGPU_BREAKDOWN;
+  } else {
+    S.iters += 1;
+    S.inner_it += 1;
+    S.rri = a[1];
+    if (!isfinite(a[0]) || !isfinite(a[1])) {
+      S.status = PBGPU_BREAKDOWN;
+      S.phase = kPhDone;
+    } else if (a[1] <= S.tol2i || S.inner_it >= S.inner_cap || S.iters >= S.max_iter) {
+      S.phase = kPhApply;
+    } else if (a[1] <= S.delta2 * S.rr_ref) {
+      S.phase = kPhReliable;
+    } else {
+      S.beta = a[0] / S.rz;
+      S.rz = a[0];
+    }
+  }
+}
+
 template <typename TI>
 __global__ void __launch_bounds__(kBlock, kBatchMinBlocks)
-    k_batch_cg(const BMember<TI>* __restrict__ mem, int n_mem, const int32_t* __restrict__ rb_sys, int64_t n_rb,
-               BState* st, double* part, GridBar* bar, int steps) {
-  const int lane = threadIdx.x & 31;
-  const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    k_batch_cg(const BMember<TI>* __restrict__ mem, const CtaGroup* __restrict__ groups, BState* st, double* part,
+               MemBar* bars, int* err, int steps) {
+  const CtaGroup G = groups[blockIdx.x];
+  const BMember<TI>& M = mem[G.slot];
+  BState& S = st[G.slot];
+  MemBar* mb = bars + G.slot;
+  const int warp = threadIdx.x >> 5;
   __shared__ int ph_s;
+  auto read_phase = [&]() {
+    __syncthreads();
+    if (threadIdx.x == 0) ph_s = ldcg(&S.phase);
+    __syncthreads();
+    return ph_s;
+  };
   for (int step = 0; step < steps; ++step) {
-    // ---- P1: outer residual (outer / apply) or q = A p (inner)
-    for (int64_t rb = blockIdx.x; rb < n_rb; rb += gridDim.x) {
-      const int s = rb_sys[rb];
-      if (threadIdx.x == 0) ph_s = ldcg(&st[s].phase);
-      __syncthreads();
-      const int ph = ph_s;
-      const BMember<TI>& M = mem[s];
-      const int64_t i = (rb - M.rb0) * kRowBlock + threadIdx.x;
+    // ---- phase 1: outer residual (outer / apply / reliable) or q = A p (inner)
+    int ph = read_phase();
+    if (ph == kPhDone) return;
+    for (int rb = G.k; rb < M.nrb; rb += G.size) {
+      const int64_t i = (int64_t)rb * kRowBlock + threadIdx.x;
       double v[2] = {0.0, 0.0};
       if ((ph == kPhOuter || ph == kPhApply || ph == kPhReliable) && i < M.A.n_pad) {
         const double ri = M.b[i] - batch_row<double>(M.A, i, M.x);
@@ -212,62 +317,19 @@ __global__ void __launch_bounds__(kBlock, kBatchMinBlocks)
       }
       block_sum<2>(v);
       if (threadIdx.x == 0) {
-        part[rb * 2] = v[0];
-        part[rb * 2 + 1] = v[1];
+        part[(M.rb0 + rb) * 2] = v[0];
+        part[(M.rb0 + rb) * 2 + 1] = v[1];
       }
     }
-    if (!grid_barrier(bar)) return;
-    // ---- P2: per-member decisions
-    if (blockIdx.x == 0 && threadIdx.x == 0) bar->active[(step + 1) & 1] = 0;
-    for (int64_t s = gwarp; s < n_mem; s += nwarps) {
-      BState& S = st[s];
-      const int ph = ldcg(&S.phase);
-      if (ph == kPhDone || ph == kPhStart || ph == kPhResume) continue;
-      double a[2];
-      member_sum<2>(part, mem[s].rb0, mem[s].nrb, a);
-      if (lane != 0) continue;
-      if (ph == kPhOuter || ph == kPhApply || ph == kPhReliable) {
-        if (S.outer == 0) {
-          S.bb = a[1];
-          S.tol2 = S.tol2 * a[1];  // tol^2 was stored; scale by ||b||^2
-        }
-        S.rr64 = a[0];
-        S.outer += 1;
-        if (!isfinite(a[0])) {
-          S.status = PBGPU_BREAKDOWN;
-          S.phase = kPhDone;
-        } else if (a[0] <= S.tol2) {
-          S.phase = kPhDone;
-        } else if (S.iters >= S.max_iter) {
-          S.status = PBGPU_NOT_CONVERGED;
-          S.phase = kPhDone;
-        } else {
-          // the TI recursion aims at the final target; with reliable updates
-          // (mixed precision) its residual is refreshed from FP64 on the way
-          S.rr_ref = a[0];
-          S.tol2i = S.tol2;
-          S.phase = ph == kPhOuter ? kPhStart : kPhResume;
-          S.inner_it = 0;
-        }
-      } else {  // inner
-        const double alpha = S.rz / a[0];
-        if (!(a[0] > 0.0) || !isfinite(alpha)) {
-          S.status = PBGPU_BREAKDOWN;
-          S.phase = kPhDone;
-        } else {
-          S.alpha = alpha;
-        }
-      }
-    }
-    if (!grid_barrier(bar)) return;
-    // ---- P3: inner start (xi = 0, r = bi, p = z) or inner update
-    for (int64_t rb = blockIdx.x; rb < n_rb; rb += gridDim.x) {
-      const int s = rb_sys[rb];
-      if (threadIdx.x == 0) ph_s = ldcg(&st[s].phase);
-      __syncthreads();
-      const int ph = ph_s;
-      const BMember<TI>& M = mem[s];
-      const int64_t i = (rb - M.rb0) * kRowBlock + threadIdx.x;
+    if (!member_barrier(mb, G.size, err, [&] {
+          if (warp == 0) member_after_spmv<TI>(S, M, part);
+        }))
+      return;
+    // ---- phase 2: inner start (xi = 0, r = bi, p = z) or inner update
+    ph = read_phase();
+    if (ph == kPhDone) return;
+    for (int rb = G.k; rb < M.nrb; rb += G.size) {
+      const int64_t i = (int64_t)rb * kRowBlock + threadIdx.x;
       double v[2] = {0.0, 0.0};
       if ((ph == kPhStart || ph == kPhResume) && i < M.A.n_pad) {
         const TI ri = M.bi[i];
@@ -277,7 +339,7 @@ __global__ void __launch_bounds__(kBlock, kBatchMinBlocks)
         if (ph == kPhStart) M.p[i] = zi;
         v[0] = (double)ri * (double)zi;
       } else if (ph == kPhInner && i < M.A.n_pad) {
-        const TI alpha = (TI)ldcg(&st[s].alpha);
+        const TI alpha = (TI)ldcg(&S.alpha);
         M.xi[i] += alpha * M.p[i];
         const TI ri = M.r[i] - alpha * M.q[i];
         M.r[i] = ri;
@@ -286,68 +348,29 @@ __global__ void __launch_bounds__(kBlock, kBatchMinBlocks)
       }
       block_sum<2>(v);
       if (threadIdx.x == 0) {
-        part[rb * 2] = v[0];
-        part[rb * 2 + 1] = v[1];
+        part[(M.rb0 + rb) * 2] = v[0];
+        part[(M.rb0 + rb) * 2 + 1] = v[1];
       }
     }
-    if (!grid_barrier(bar)) return;
-    // ---- P4: per-member inner bookkeeping
-    for (int64_t s = gwarp; s < n_mem; s += nwarps) {
-      BState& S = st[s];
-      const int ph = ldcg(&S.phase);
-      if (ph == kPhStart || ph == kPhResume || ph == kPhInner) {
-        double a[2];
-        member_sum<2>(part, mem[s].rb0, mem[s].nrb, a);
-        if (lane == 0) {
-          if (ph == kPhStart) {
-            S.rz = a[0];
-            S.phase = kPhInner;
-          } else if (ph == kPhResume) {
-            // CG continues from the fresh residual: p = z + beta p in P5
-            S.beta = a[0] / S.rz;
-            S.rz = a[0];
-            S.phase = isfinite(S.beta) ? kPhInner : kPhDone;
-            if (S.phase == kPhDone) S.status = PBGPU_BREAKDOWN;
-          } else {
-            S.iters += 1;
-            S.inner_it += 1;
-            S.rri = a[1];
-            if (!isfinite(a[0]) || !isfinite(a[1])) {
-              S.status = PBGPU_BREAKDOWN;
-              S.phase = kPhDone;
-            } else if (a[1] <= S.tol2i || S.inner_it >= S.inner_cap || S.iters >= S.max_iter) {
-              S.phase = kPhApply;
-            } else if (a[1] <= S.delta2 * S.rr_ref) {
-              S.phase = kPhReliable;
-            } else {
-              S.beta = a[0] / S.rz;
-              S.rz = a[0];
-            }
-          }
-        }
+    if (!member_barrier(mb, G.size, err, [&] {
+          if (warp == 0) member_after_update<TI>(S, M, part);
+        }))
+      return;
+    // ---- phase 3: p = z + beta p (inner) or x += xi (apply / reliable)
+    ph = read_phase();
+    if (ph == kPhDone) return;
+    if (ph == kPhInner || ph == kPhApply || ph == kPhReliable) {
+      const TI beta = ph == kPhInner ? (TI)ldcg(&S.beta) : (TI)0;
+      for (int rb = G.k; rb < M.nrb; rb += G.size) {
+        const int64_t i = (int64_t)rb * kRowBlock + threadIdx.x;
+        if (i >= M.A.n_pad) continue;
+        if (ph == kPhInner)
+          M.p[i] = M.dinv[i] * M.r[i] + beta * M.p[i];
+        else
+          M.x[i] += (double)M.xi[i];
       }
-      if (lane == 0 && S.phase != kPhDone) atomicAdd(&bar->active[step & 1], 1u);
     }
-    if (!grid_barrier(bar)) return;
-    // ---- P5: p = z + beta p (inner) or x += xi (apply)
-    for (int64_t rb = blockIdx.x; rb < n_rb; rb += gridDim.x) {
-      const int s = rb_sys[rb];
-      if (threadIdx.x == 0) ph_s = ldcg(&st[s].phase);
-      __syncthreads();
-      const int ph = ph_s;
-      const BMember<TI>& M = mem[s];
-      const int64_t i = (rb - M.rb0) * kRowBlock + threadIdx.x;
-      if (ph == kPhInner && i < M.A.n_pad) {
-        const TI beta = (TI)ldcg(&st[s].beta);
-        M.p[i] = M.dinv[i] * M.r[i] + beta * M.p[i];
-      } else if ((ph == kPhApply || ph == kPhReliable) && i < M.A.n_pad) {
-        M.x[i] += (double)M.xi[i];
-      }
-      __syncthreads();
-    }
-    const unsigned active = *reinterpret_cast<volatile unsigned*>(&bar->active[step & 1]);
-    if (!grid_barrier(bar)) return;
-    if (active == 0) return;
+    if (!member_barrier(mb, G.size, err, [] {})) return;
   }
 }
 
@@ -388,13 +411,16 @@ struct pbgpu_batch {
   DBuf<BMember<float>> m32;
   std::vector<BMember<double>> h64;
   std::vector<BMember<float>> h32;
-  DBuf<int32_t> rb_sys;
+  DBuf<CtaGroup> groups;
+  std::vector<CtaGroup> h_groups;
   DBuf<double> part;
   DBuf<BState> st;
-  DBuf<GridBar> bar;
+  DBuf<MemBar> bars;          // one per slot
+  DBuf<int> errf;             // barrier timeout flag
+  bool bars_reset = true;     // clear the member barriers before the next launch
   BState* st_host = nullptr;
   size_t st_cap = 0;
-  GridBar* bar_host = nullptr;      // pinned copy of the barrier state
+  int* err_host = nullptr;          // pinned copy of the timeout flag
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool in_flight = false;           // a launch whose states are not yet read
   bool kernel_in_flight = false;
@@ -524,7 +550,7 @@ int prepare_member(pbgpu_batch* B, int slot) {
   return PBGPU_OK;
 }
 
-// Descriptors and the row-block -> slot table of the current members.
+// Descriptors of the current members and their row-block ranges.
 template <typename TI>
 int upload_tables(pbgpu_batch* B) {
   std::vector<BMember<TI>>& hm = *[&]() {
@@ -551,10 +577,6 @@ int upload_tables(pbgpu_batch* B) {
     dm = B->m64.get();
   BATCH_CUDA(B, cudaMemcpyAsync(dm, hm.data(), B->slots.size() * sizeof(BMember<TI>), cudaMemcpyHostToDevice,
                                 B->stream));
-  BATCH_CUDA(B, B->rb_sys.alloc(std::max<int64_t>(B->n_rb, 1)));
-  if (B->n_rb)
-    BATCH_CUDA(B, cudaMemcpyAsync(B->rb_sys.get(), rbs.data(), B->n_rb * sizeof(int32_t), cudaMemcpyHostToDevice,
-                                  B->stream));
   BATCH_CUDA(B, B->part.alloc(2 * std::max<int64_t>(B->n_rb, 1)));
   B->dirty = false;
   return PBGPU_OK;
@@ -575,39 +597,84 @@ int batch_launch(pbgpu_batch* B, int steps) {
   if (!B->ev0) {
     BATCH_CUDA(B, cudaEventCreate(&B->ev0));
     BATCH_CUDA(B, cudaEventCreate(&B->ev1));
-    BATCH_CUDA(B, cudaMallocHost(&B->bar_host, sizeof(GridBar)));
+    BATCH_CUDA(B, cudaMallocHost(&B->err_host, sizeof(int)));
   }
-  B->bar_host->err = 0;
+  *B->err_host = 0;
   B->kernel_in_flight = false;
-  if (B->n_rb > 0 && steps > 0) {
-    if (!B->bar.get()) {
-      BATCH_CUDA(B, B->bar.alloc(1));
-      BATCH_CUDA(B, cudaMemsetAsync(B->bar.get(), 0, sizeof(GridBar), B->stream));
-    }
+  // members that take part: set up and not finished
+  const std::vector<BMember<TI>>& hm = *[&]() {
+    if constexpr (std::is_same<TI, float>::value)
+      return &B->h32;
+    else
+      return &B->h64;
+  }();
+  std::vector<int> act;
+  for (int k = 0; k < nm; ++k)
+    if (B->slots[k] && !B->pending[k] && B->st_host[k].phase != kPhDone && hm[k].nrb > 0) act.push_back(k);
+  if (!act.empty() && steps > 0) {
     int occ = 0;
     BATCH_CUDA(B, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_cg<TI>, kBlock, 0));
     if (occ <= 0) return B->fail(PBGPU_ERR_CUDA, "batch: kernel cannot be resident");
     if (B->blocks_per_sm > 0) occ = std::min(occ, B->blocks_per_sm);
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)occ * B->sm_count, B->n_rb));
+    const int64_t cap = (int64_t)occ * B->sm_count;
+    if ((int64_t)act.size() > cap)
+      return B->fail(PBGPU_ERR_CAPACITY, "batch: more unfinished members than resident CTAs (" + std::to_string(cap) + ")");
+    // CTA groups: one CTA each, then one more at a time to the member with
+    // the most row-blocks per CTA, up to the resident CTAs or one CTA per
+    // row-block
+    std::vector<int> g(act.size(), 1);
+    int64_t left = cap - (int64_t)act.size();
+    while (left > 0) {
+      int best = -1;
+      double bw = 0.0;
+      for (size_t j = 0; j < act.size(); ++j) {
+        const int nrb = hm[act[j]].nrb;
+        if (g[j] >= nrb) continue;
+        const double w = (double)nrb / g[j];
+        if (w > bw) {
+          bw = w;
+          best = (int)j;
+        }
+      }
+      if (best < 0) break;
+      ++g[best];
+      --left;
+    }
+    B->h_groups.clear();
+    for (size_t j = 0; j < act.size(); ++j)
+      for (int k = 0; k < g[j]; ++k) B->h_groups.push_back(CtaGroup{act[j], k, g[j], 0});
+    const int grid = (int)B->h_groups.size();
+    BATCH_CUDA(B, B->groups.alloc(grid));
+    BATCH_CUDA(B, cudaMemcpyAsync(B->groups.get(), B->h_groups.data(), grid * sizeof(CtaGroup),
+                                  cudaMemcpyHostToDevice, B->stream));
+    if (B->bars.n < B->st_cap || !B->bars.get()) {
+      BATCH_CUDA(B, B->bars.alloc(B->st_cap));
+      B->bars_reset = true;
+    }
+    if (B->bars_reset) {
+      BATCH_CUDA(B, cudaMemsetAsync(B->bars.get(), 0, B->bars.n * sizeof(MemBar), B->stream));
+      B->bars_reset = false;
+    }
+    BATCH_CUDA(B, B->errf.alloc(1));
+    BATCH_CUDA(B, cudaMemsetAsync(B->errf.get(), 0, sizeof(int), B->stream));
     const BMember<TI>* a_mem;
     if constexpr (std::is_same<TI, float>::value)
       a_mem = B->m32.get();
     else
       a_mem = B->m64.get();
-    int a_nm = nm;
-    const int32_t* a_rb = B->rb_sys.get();
-    int64_t a_nrb = B->n_rb;
+    const CtaGroup* a_groups = B->groups.get();
     BState* a_st = B->st.get();
     double* a_part = B->part.get();
-    GridBar* a_bar = B->bar.get();
+    MemBar* a_bars = B->bars.get();
+    int* a_err = B->errf.get();
     int a_steps = steps;
-    void* args[] = {&a_mem, &a_nm, &a_rb, &a_nrb, &a_st, &a_part, &a_bar, &a_steps};
+    void* args[] = {&a_mem, &a_groups, &a_st, &a_part, &a_bars, &a_err, &a_steps};
     BATCH_CUDA(B, cudaEventRecord(B->ev0, B->stream));
     BATCH_CUDA(B, cudaLaunchCooperativeKernel((const void*)k_batch_cg<TI>, dim3(grid), dim3(kBlock), args, 0,
                                               B->stream));
     B->launches += 1;
     BATCH_CUDA(B, cudaEventRecord(B->ev1, B->stream));
-    BATCH_CUDA(B, cudaMemcpyAsync(B->bar_host, B->bar.get(), sizeof(GridBar), cudaMemcpyDeviceToHost, B->stream));
+    BATCH_CUDA(B, cudaMemcpyAsync(B->err_host, B->errf.get(), sizeof(int), cudaMemcpyDeviceToHost, B->stream));
     B->kernel_in_flight = true;
   }
   BATCH_CUDA(B, cudaMemcpyAsync(B->st_host, B->st.get(), nm * sizeof(BState), cudaMemcpyDeviceToHost, B->stream));
@@ -623,7 +690,10 @@ int batch_wait(pbgpu_batch* B, int* n_active) {
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, B->ev0, B->ev1) == cudaSuccess) B->last_ms += ms;
       B->kernel_in_flight = false;
-      if (B->bar_host->err) return B->fail(PBGPU_TIMEOUT, "batch: grid barrier wait timed out");
+      if (*B->err_host) {
+        B->bars_reset = true;
+        return B->fail(PBGPU_TIMEOUT, "batch: member barrier wait timed out");
+      }
     }
   }
   int active = 0;
@@ -709,7 +779,7 @@ void pbgpu_batch_destroy(pbgpu_batch* b) {
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->st_host) cudaFreeHost(b->st_host);
-  if (b->bar_host) cudaFreeHost(b->bar_host);
+  if (b->err_host) cudaFreeHost(b->err_host);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   cudaStream_t s = b->stream;
