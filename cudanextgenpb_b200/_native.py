@@ -147,6 +147,8 @@ PBGPU_FUNCS = {
     "pbgpu_autotune": (C.c_int, [ctx_p, C.c_int, P(PbgpuSellOpts), P(C.c_int), P(dbl)]),
     "pbgpu_build_mesh": (C.c_int, [ctx_p, P(PbgpuMeshBuild)]),
     "pbgpu_get_mesh_counts": (C.c_int, [ctx_p, P(i64), P(i64), P(i64), P(i64)]),
+    "pbgpu_get_mesh": (C.c_int, [ctx_p, P(C.c_int32), P(C.c_int8), P(C.c_int32), P(C.c_int32), P(C.c_int8),
+                                 P(C.c_int32), P(dbl)]),
     "pbgpu_solve_charges": (C.c_int, [ctx_p, C.c_int, P(dbl), P(PbgpuSolverOpts), C.c_int, P(PbgpuEnergyOut),
                                       P(PbgpuSolveStats)]),
     "pbgpu_batch_create": (C.c_int, [P(C.c_void_p), C.c_int, C.c_void_p]),
@@ -184,6 +186,7 @@ PBHOST_FUNCS = {
     "pbhost_set_atoms": (C.c_int, [host_p, i64, P(dbl), P(dbl), P(dbl)]),
     "pbhost_build_problem": (C.c_int, [host_p]),
     "pbhost_build_on_gpu": (C.c_int, [host_p, C.c_void_p]),
+    "pbhost_write_vtu": (C.c_int, [host_p, C.c_char_p, C.c_char_p, P(dbl)]),
     "pbhost_get_info": (C.c_int, [host_p, P(PbhostInfo)]),
     "pbhost_get_mesh": (C.c_int, [host_p, P(PbgpuMesh)]),
     "pbhost_get_rays": (C.c_int, [host_p, C.c_int, P(PbgpuRays)]),

@@ -39,7 +39,7 @@ CXXFLAGS = ["-O3", "-std=c++17", "-fopenmp", "-fPIC", "-ffp-contract=off", "-Wal
 GPU_SOURCES = ["pbgpu_api.cu", "k_markers.cu", "k_density.cu", "k_assemble.cu", "k_krylov.cu", "k_energy.cu",
                "k_static.cu", "k_batch.cu", "pbgpu_server.cu", "k_multi.cu", "k_tune.cu", "k_mesh.cu",
                "k_potfield.cu"]
-HOST_SOURCES = ["octree.cpp", "surface.cpp", "options.cpp", "pb_class.cpp", "pbhost_capi.cpp"]
+HOST_SOURCES = ["octree.cpp", "surface.cpp", "options.cpp", "pb_class.cpp", "pbhost_capi.cpp", "vtu.cpp"]
 
 
 def _run(cmd, verbose=False):

@@ -1212,3 +1212,59 @@ extern "C" int pbgpu_get_mesh_counts(pbgpu_ctx* h, int64_t* n_oct, int64_t* n_no
     for (int a = 0; a < 3; ++a) n_rays[a] = c.rays[a].n;
   return PBGPU_OK;
 }
+
+// The context's mesh copied back to host arrays (any may be NULL), sized by
+// pbgpu_get_mesh_counts; box receives lo[3] and the extent hi - lo [3] the
+// node coordinates are computed from.
+extern "C" int pbgpu_get_mesh(pbgpu_ctx* h, int32_t* oct_xyz, int8_t* oct_level, int32_t* oct_nodes,
+                              int32_t* node_xyz, int8_t* hang_np, int32_t* hang_par, double* box) {
+  if (!h) return PBGPU_ERR_ARG;
+  Context* c = &h->c;
+  if (!c->have_mesh) return c->fail(PBGPU_ERR_STATE, "get_mesh: no mesh");
+  if (cudaSetDevice(c->device) != cudaSuccess) return c->fail(PBGPU_ERR_CUDA, "get_mesh: cudaSetDevice");
+  std::vector<int4> v;
+  if (oct_xyz || oct_level) {
+    v.resize(c->n_oct);
+    PBGPU_CUDA(c, cudaMemcpyAsync(v.data(), c->oct.get(), c->n_oct * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+    PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int64_t i = 0; i < c->n_oct; ++i) {
+      if (oct_xyz) {
+        oct_xyz[3 * i] = v[i].x;
+        oct_xyz[3 * i + 1] = v[i].y;
+        oct_xyz[3 * i + 2] = v[i].z;
+      }
+      if (oct_level) oct_level[i] = (int8_t)v[i].w;
+    }
+  }
+  if (oct_nodes)
+    PBGPU_CUDA(c, cudaMemcpyAsync(oct_nodes, c->oct_nodes.get(), 8 * c->n_oct * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                  c->stream));
+  std::vector<int8_t> np;
+  if ((hang_np || hang_par) && c->nh) {
+    np.resize(c->nh);
+    PBGPU_CUDA(c, cudaMemcpyAsync(np.data(), c->hang_np.get(), c->nh, cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (hang_par && c->nh)
+    PBGPU_CUDA(c, cudaMemcpyAsync(hang_par, c->hang_par.get(), c->nh * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (hang_np && c->nh) std::memcpy(hang_np, np.data(), c->nh);
+  if (hang_par)  // the device pads unused parent slots; the host layout marks them -1
+    for (int64_t i = 0; i < c->nh; ++i)
+      for (int j = np[i]; j < 4; ++j) hang_par[4 * i + j] = -1;
+  if (node_xyz) {
+    v.resize(c->n);
+    PBGPU_CUDA(c, cudaMemcpyAsync(v.data(), c->node_xyz.get(), c->n * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+    PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int64_t i = 0; i < c->n; ++i) {
+      node_xyz[3 * i] = v[i].x;
+      node_xyz[3 * i + 1] = v[i].y;
+      node_xyz[3 * i + 2] = v[i].z;
+    }
+  }
+  if (box)
+    for (int a = 0; a < 3; ++a) {
+      box[a] = c->lo[a];
+      box[3 + a] = c->len[a];
+    }
+  return PBGPU_OK;
+}

@@ -1,6 +1,7 @@
 // Host-side poisson_boltzmann: configuration, atoms, domain box, octree
 // refinement, surface rays, and the GPU path through the pbgpu C ABI.
 #include "pb_class.h"
+#include "vtu.h"
 
 #include <omp.h>
 
@@ -84,6 +85,9 @@ void poisson_boltzmann::apply_options(const OptionFile& g) {
   calc_coulombic = g.get(md + "calc_coulombic", 0);
   calc_potential_term = g.get(md + "calc_potential_terms", 0);
   calc_field_term = g.get(md + "calc_field_terms", 0);
+  map_type = g.get(md + "map_type", std::string("vtu"));
+  potential_map = g.get(md + "potential_map", 0);
+  eps_map = g.get(md + "eps_map", 0);
   atoms_write = g.get(md + "atoms_write", 0);
   const std::string s = "surface/";
   surf_type_num = g.get(s + "surface_type", 0);
@@ -914,6 +918,95 @@ static int run_pot_field(poisson_boltzmann& pb, int fast, const std::string& pat
 int poisson_boltzmann::pot_field(const std::string& path) { return run_pot_field(*this, 0, path); }
 int poisson_boltzmann::pot_field_fast(const std::string& path) { return run_pot_field(*this, 1, path); }
 
+// The mesh of a field: the host's own tables when the host built the mesh,
+// else the context's (built on the GPU), copied back.
+int poisson_boltzmann::write_vtu(const std::string& basename, const std::string& fieldname, const double* values) {
+  VtuMesh vm;
+  std::vector<int32_t> oxyz, onodes, nxyz, hpar;
+  std::vector<int8_t> olvl, hnp;
+  if (!oct_level.empty()) {
+    const pbgpu_mesh m = mesh_view();
+    vm.n_oct = m.n_oct;
+    vm.oct_xyz = m.oct_xyz;
+    vm.oct_level = m.oct_level;
+    vm.oct_nodes = m.oct_nodes;
+    vm.n_nodes = m.n_nodes;
+    vm.node_xyz = m.node_xyz;
+    vm.n_hang = m.n_hang;
+    vm.hang_np = m.hang_np;
+    vm.hang_par = m.hang_par;
+    for (int a = 0; a < 3; ++a) {
+      vm.lo[a] = m.lo[a];
+      vm.extent[a] = m.hi[a] - m.lo[a];
+    }
+  } else if (gpu) {
+    int64_t no = 0, nn = 0, nh = 0, nr[3];
+    int st = check(pbgpu_get_mesh_counts(gpu, &no, &nn, &nh, nr));
+    if (st != PBGPU_OK) return st;
+    oxyz.resize(3 * no);
+    olvl.resize(no);
+    onodes.resize(8 * no);
+    nxyz.resize(3 * nn);
+    hnp.resize(nh);
+    hpar.resize(4 * nh);
+    double box[6];
+    st = check(pbgpu_get_mesh(gpu, oxyz.data(), olvl.data(), onodes.data(), nxyz.data(), hnp.data(), hpar.data(), box));
+    if (st != PBGPU_OK) return st;
+    vm.n_oct = no;
+    vm.oct_xyz = oxyz.data();
+    vm.oct_level = olvl.data();
+    vm.oct_nodes = onodes.data();
+    vm.n_nodes = nn;
+    vm.node_xyz = nxyz.data();
+    vm.n_hang = nh;
+    vm.hang_np = hnp.data();
+    vm.hang_par = hpar.data();
+    for (int a = 0; a < 3; ++a) {
+      vm.lo[a] = box[a];
+      vm.extent[a] = box[3 + a];
+    }
+  } else {
+    last_error = "write_vtu: no mesh";
+    return PBGPU_ERR_STATE;
+  }
+  if (!pbh::write_vtu(basename, fieldname, vm, values, &last_error)) return PBGPU_ERR_ARG;
+  return PBGPU_OK;
+}
+
+// map_type = vtu: potential_map_0000.vtu (phi), eps_map_0000.vtu (epsilon at
+// the nodes) and their total_*.pvtu.  The octbin format of map_type = oct is
+// p4est's own and is not written here.
+int poisson_boltzmann::export_maps() {
+  if (!potential_map && !eps_map) return PBGPU_OK;
+  if (map_type == "oct") {
+    last_error = "map_type = oct (p4est octbin) is not supported; use map_type = vtu";
+    return PBGPU_ERR_ARG;
+  }
+  if (map_type != "vtu") {
+    last_error = "Wrong type of map output: " + map_type;
+    return PBGPU_ERR_ARG;
+  }
+  int64_t no = 0, nn = 0, nh = 0, nr[3];
+  int st = check(pbgpu_get_mesh_counts(gpu, &no, &nn, &nh, nr));
+  if (st != PBGPU_OK) return st;
+  std::vector<std::string> fields, bases;
+  std::vector<double> v(nn);
+  if (potential_map) {
+    if ((st = check(pbgpu_get_phi(gpu, v.data()))) != PBGPU_OK) return st;
+    if ((st = write_vtu("potential_map", "phi", v.data())) != PBGPU_OK) return st;
+    fields.push_back("phi");
+    bases.push_back("potential_map");
+  }
+  if (eps_map) {
+    if ((st = check(pbgpu_get_node_coeffs(gpu, v.data(), nullptr))) != PBGPU_OK) return st;
+    if ((st = write_vtu("eps_map", "eps", v.data())) != PBGPU_OK) return st;
+    fields.push_back("eps");
+    bases.push_back("eps_map");
+  }
+  if (!pbh::write_pvtu(fields, bases, 1, &last_error)) return PBGPU_ERR_ARG;
+  return PBGPU_OK;
+}
+
 // The driver's sequence from create_markers on (src/poisson_boltzmann.cpp:192-299).
 int poisson_boltzmann::run_gpu_path() {
   int st;
@@ -948,6 +1041,9 @@ int poisson_boltzmann::run_gpu_path() {
     }
     if (s3 != PBGPU_OK) return s3;
   }
+  // :305-351
+  const int s4 = export_maps();
+  if (s4 != PBGPU_OK) return s4;
   return st;
 }
 

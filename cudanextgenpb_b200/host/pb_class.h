@@ -48,6 +48,8 @@ struct poisson_boltzmann {
   // [model]
   int linearized = 1, bc = 1, calc_energy = 2, calc_coulombic = 0, atoms_write = 0;
   int calc_potential_term = 0, calc_field_term = 0;
+  std::string map_type = "vtu";
+  int potential_map = 0, eps_map = 0;
   double e_in = 2.0, e_out = 80.0, ionic_strength = 0.145, T = 298.15;
   double net_charge = 0.0;
   // [surface]
@@ -119,6 +121,10 @@ struct poisson_boltzmann {
   // per-atom potentials and fields, written to `path` (src/pb_class.cpp:3732-5060)
   int pot_field(const std::string& path = "pot_field.dat");
   int pot_field_fast(const std::string& path = "pot_field.dat");
+  // potential_map / eps_map output for map_type = vtu (src/poisson_boltzmann.cpp:319-351)
+  int export_maps();
+  // one node field (values in node order) on the context's mesh to <basename>_0000.vtu
+  int write_vtu(const std::string& basename, const std::string& fieldname, const double* values);
   // Whole path in the reference's order; returns a pbgpu status.
   int run_gpu_path();
 

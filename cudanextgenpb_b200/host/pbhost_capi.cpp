@@ -136,6 +136,19 @@ int pbhost_build_on_gpu(pbhost* h, pbgpu_ctx* ctx) {
   return st;
 }
 
+int pbhost_write_vtu(pbhost* h, const char* basename, const char* fieldname, const double* values) {
+  if (!h || !basename || !fieldname || !values) return PBGPU_ERR_ARG;
+  int st;
+  try {
+    st = h->pb.write_vtu(basename, fieldname, values);
+  } catch (const std::exception& ex) {
+    h->err = ex.what();
+    return PBGPU_ERR_ARG;
+  }
+  if (st != PBGPU_OK) h->err = h->pb.last_error;
+  return st;
+}
+
 int pbhost_get_info(const pbhost* h, pbhost_info* o) {
   if (!h || !o) return PBGPU_ERR_ARG;
   const pbh::poisson_boltzmann& p = h->pb;

@@ -100,6 +100,13 @@ class Problem:
         g.n_atoms = len(q)
         return g
 
+    def write_vtu(self, basename: str, fieldname: str, values) -> str:
+        """One node field on this problem's mesh to <basename>_0000.vtu (the
+        reference's VTU layout); returns the file name."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self._check(self._lib.pbhost_write_vtu(self._h, basename.encode(), fieldname.encode(), _dptr(v)))
+        return "%s_0000.vtu" % basename
+
     def mesh_struct(self) -> N.PbgpuMesh:
         m = N.PbgpuMesh()
         self._check(self._lib.pbhost_get_mesh(self._h, C.byref(m)))
@@ -274,6 +281,25 @@ class GpuPath:
         return rows, o.as_dict()
 
     # ---- read-back
+    def mesh_arrays(self) -> dict:
+        """The context's mesh (set or built on the GPU) as numpy arrays in the
+        layout of Problem.mesh()."""
+        no, nn, nh = C.c_int64(), C.c_int64(), C.c_int64()
+        nr = (C.c_int64 * 3)()
+        self._check(self._lib.pbgpu_get_mesh_counts(self._ctx, C.byref(no), C.byref(nn), C.byref(nh), nr))
+        no, nn, nh = no.value, nn.value, nh.value
+        d = {"oct_xyz": np.zeros((no, 3), np.int32), "oct_level": np.zeros(no, np.int8),
+             "oct_nodes": np.zeros((no, 8), np.int32), "node_xyz": np.zeros((nn, 3), np.int32),
+             "hang_np": np.zeros(nh, np.int8), "hang_par": np.zeros((nh, 4), np.int32)}
+        box = np.zeros(6)
+        P = C.POINTER
+        i32 = lambda a: a.ctypes.data_as(P(C.c_int32))
+        i8 = lambda a: a.ctypes.data_as(P(C.c_int8))
+        self._check(self._lib.pbgpu_get_mesh(self._ctx, i32(d["oct_xyz"]), i8(d["oct_level"]), i32(d["oct_nodes"]),
+                                             i32(d["node_xyz"]), i8(d["hang_np"]), i32(d["hang_par"]), _dptr(box)))
+        d["lo"], d["extent"] = box[:3].copy(), box[3:].copy()
+        return d
+
     def node_coeffs(self):
         eps, react = np.zeros(self.n), np.zeros(self.n)
         self._check(self._lib.pbgpu_get_node_coeffs(self._ctx, _dptr(eps), _dptr(react)))

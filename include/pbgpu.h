@@ -293,6 +293,13 @@ typedef struct {
 int pbgpu_build_mesh(pbgpu_ctx* ctx, const pbgpu_mesh_build* build);
 /* sizes of the context's mesh; n_rays: 3 entries (rays with crossings per axis) */
 int pbgpu_get_mesh_counts(pbgpu_ctx* ctx, int64_t* n_oct, int64_t* n_nodes, int64_t* n_hang, int64_t* n_rays);
+/* The context's mesh (set or built) copied to host arrays in the layout of
+ * pbgpu_mesh, any of them NULL to skip, sized by pbgpu_get_mesh_counts;
+ * hang_par takes 4 per hanging node.  box (may be NULL) receives lo[3] and the
+ * extents hi - lo [3]: a corner at integer coordinate i sits at
+ * lo + extent * (i * 2^-19).  No reference counterpart (tmesh accessors). */
+int pbgpu_get_mesh(pbgpu_ctx* ctx, int32_t* oct_xyz, int8_t* oct_level, int32_t* oct_nodes, int32_t* node_xyz,
+                   int8_t* hang_np, int32_t* hang_par, double* box);
 
 /* ---- SELL layout autotuner ----------------------------------------------
  * No counterpart in the reference.  Assembles the context's system (markers

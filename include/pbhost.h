@@ -52,6 +52,11 @@ int pbhost_build_problem(pbhost* h);
  * atoms and the model; the host keeps no mesh (pbhost_get_mesh / _rays then
  * describe nothing). */
 int pbhost_build_on_gpu(pbhost* h, pbgpu_ctx* ctx);
+/* One node field (values in node order, n_nodes) on the problem's mesh to
+ * <basename>_0000.vtu in the layout of the reference's VTKWriter
+ * (src/vtk_class.cpp:20-429): the host's mesh, or the GPU context's when the
+ * mesh was built there. */
+int pbhost_write_vtu(pbhost* h, const char* basename, const char* fieldname, const double* values);
 /* Same with a caller-chosen domain (mesh_shape 2 box) and uniform/surface levels. */
 int pbhost_get_info(const pbhost* h, pbhost_info* out);
 int pbhost_get_mesh(const pbhost* h, pbgpu_mesh* out);

@@ -28,6 +28,13 @@ def test_gpu_mesh_equals_host_mesh(name):
     g_dev = CASES[name]().build_on_gpu(GpuPath())
     assert (g_dev.n_oct, g_dev.n, g_dev.n_hang) == (info["n_oct"], info["n_nodes"], info["n_hang"])
     assert g_dev.n_rays == list(info["n_rays"])
+    # the arrays themselves, read back from both contexts
+    hm = host.mesh()
+    for g in (g_host, g_dev):
+        d = g.mesh_arrays()
+        for k in ("oct_xyz", "oct_level", "oct_nodes", "node_xyz", "hang_np", "hang_par"):
+            assert np.array_equal(d[k], hm[k]), k
+        np.testing.assert_array_equal(d["lo"], hm["lo"])
     for g in (g_host, g_dev):
         g.create_markers()
         g.create_density_map()

@@ -154,3 +154,44 @@ def test_host_driver_writes_pot_field(tmp_path, monkeypatch):
     assert e["energy_pol"] == pytest.approx(pe["energy_pol"], rel=1e-6)
     assert e["energy_react"] == pytest.approx(pe["energy_react"], rel=1e-6)
     g.close()
+
+
+def test_host_driver_writes_vtu_maps(tmp_path, monkeypatch):
+    """potential_map / eps_map with map_type = vtu: the driver writes
+    potential_map_0000.vtu (phi), eps_map_0000.vtu (epsilon at the nodes) and
+    their total_*.pvtu, from the context's own potential; with the mesh built
+    on the GPU the same files come from the context's mesh."""
+    from vtu_reader import read_vtu
+    text = configs.born_options(5, 6).replace(
+        "calc_coulombic = 1", "calc_coulombic = 1\npotential_map = 1\neps_map = 1\nmap_type = vtu")
+    prob = Problem(text)
+    prob.set_atoms(*configs.BORN_ATOM)
+    prob.build()
+    monkeypatch.chdir(tmp_path)
+    prob.run_gpu()
+    g = GpuPath().load(prob)
+    g.create_markers()
+    g.create_density_map()
+    g.assemble()
+    g.solve(prob.solver_opts())
+    n = g.n
+    phi = read_vtu("potential_map_0000.vtu")["arrays"]["phi"]
+    eps = read_vtu("eps_map_0000.vtu")["arrays"]["eps"]
+    np.testing.assert_array_equal(phi[:n], g.phi())
+    np.testing.assert_array_equal(eps[:n], g.node_coeffs()[0])
+    for base, field in (("potential_map", "phi"), ("eps_map", "eps")):
+        t = (tmp_path / ("total_%s.pvtu" % base)).read_text()
+        assert 'Name="%s"' % field in t and '<Piece Source="%s_0000.vtu"/>' % base in t
+    g.close()
+    # mesh built on the GPU: same file
+    os_mesh = (tmp_path / "potential_map_0000.vtu").read_bytes()
+    p2 = Problem(text)
+    p2.set_atoms(*configs.BORN_ATOM)
+    g2 = p2.build_on_gpu(GpuPath())
+    g2.create_markers()
+    g2.create_density_map()
+    g2.assemble()
+    g2.solve(prob.solver_opts())
+    p2.write_vtu(str(tmp_path / "gpu_map"), "phi", g2.phi())
+    assert (tmp_path / "gpu_map_0000.vtu").read_bytes() == os_mesh
+    g2.close()
