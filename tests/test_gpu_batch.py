@@ -1,7 +1,7 @@
 """The multi-system persistent solve (pbgpu_batch_*): each member's result in
 the batch equals its own single-system solve within the solve tolerance, and
-the energies agree to 1e-6 relative (the north_star's "same alone and in the
-mix" check)."""
+the energies agree to 1e-6 relative: a molecule gives the same result alone
+and in the mix."""
 import numpy as np
 import pytest
 
