@@ -669,7 +669,9 @@ def run_batch(args, rank, world, local):
 SERVES = {
     # name: (pool size, min atoms, max atoms, seed, surface levels, arrivals per s, seconds)
     "serve": (24, 200, 3000, 5, 1, 200.0, 10.0),
-    "serve_small": (8, 50, 400, 5, 1, 100.0, 3.0),
+    # small molecules, offered faster than either path serves them, so the
+    # value is each path's capacity
+    "serve_small": (8, 50, 400, 5, 1, 2000.0, 1.0),
 }
 
 

@@ -58,6 +58,14 @@ struct Running {
 
 int64_t ctx_bytes(pbgpu_ctx* c) { return c ? c->c.dev_bytes : 0; }
 
+// A converged member out of the batch whose energy is still to compute.
+struct Retire {
+  Running r;
+  pbgpu_solve_stats stats;
+  pbgpu_energy_out energy;
+  int st;
+};
+
 }  // namespace
 
 struct pbgpu_server {
@@ -75,6 +83,7 @@ struct pbgpu_server {
   bool stop = false;
   std::deque<Pending> queue;
   std::vector<Running> running;
+  std::vector<Retire> finishing;  // batched mode: energies of the next tick
   std::vector<pbgpu_ctx*> idle;
   int64_t next_id = 1;
   bool in_session = false;
@@ -217,6 +226,7 @@ void pbgpu_server_destroy(pbgpu_server* s) {
   }
   if (s->batch) pbgpu_batch_destroy(s->batch);
   for (Running& r : s->running) pbgpu_ctx_destroy(r.ctx);
+  for (Retire& x : s->finishing) pbgpu_ctx_destroy(x.r.ctx);
   for (pbgpu_ctx* c : s->idle) pbgpu_ctx_destroy(c);
   delete s;
 }
@@ -247,10 +257,11 @@ int pbgpu_server_pending(const pbgpu_server* sc, int* queued, int* running, int6
     return PBGPU_OK;
   }
   if (queued) *queued = (int)s->queue.size();
-  if (running) *running = (int)s->running.size();
+  if (running) *running = (int)(s->running.size() + s->finishing.size());
   if (device_bytes) {
     int64_t b = 0;
     for (const Running& r : s->running) b += ctx_bytes(r.ctx);
+    for (const Retire& x : s->finishing) b += ctx_bytes(x.r.ctx);
     for (pbgpu_ctx* c : s->idle) b += ctx_bytes(c);
     *device_bytes = b;
   }
@@ -261,6 +272,7 @@ int pbgpu_server_pending(const pbgpu_server* sc, int* queued, int* running, int6
 static int64_t held_bytes(const pbgpu_server* s) {
   int64_t b = 0;
   for (const Running& r : s->running) b += ctx_bytes(r.ctx);
+  for (const Retire& x : s->finishing) b += ctx_bytes(x.r.ctx);
   for (pbgpu_ctx* c : s->idle) b += ctx_bytes(c);
   return b;
 }
@@ -369,21 +381,46 @@ int pbgpu_server_progress(pbgpu_server* s, pbgpu_result* out, int cap, int* n_ou
     adm.push_back(Admit{p, ctx, Clock::now(), PBGPU_OK});
     s->queue.pop_front();
   }
-  if (adm.size() == 1) {
-    adm[0].st = setup_request(s, adm[0].ctx, adm[0].p.req);
-  } else if (!adm.empty()) {
+  //    and the members that converged last tick compute their energies (as
+  //    many as the output array holds), also one host thread each
+  const size_t n_fin = std::min(s->finishing.size(), (size_t)std::max(cap, 0));
+  auto energy_of = [s](Retire& x) {
+    if (x.st == PBGPU_OK) x.st = pbgpu_energy(x.r.ctx, s->opts.energy_fast, &x.energy);
+  };
+  if (adm.size() + n_fin == 1) {
+    if (n_fin)
+      energy_of(s->finishing[0]);
+    else
+      adm[0].st = setup_request(s, adm[0].ctx, adm[0].p.req);
+  } else if (adm.size() + n_fin > 1) {
     std::vector<std::thread> th;
-    th.reserve(adm.size());
+    th.reserve(adm.size() + n_fin);
     for (Admit& a : adm) th.emplace_back([s, &a] { a.st = setup_request(s, a.ctx, a.p.req); });
+    for (size_t k = 0; k < n_fin; ++k) th.emplace_back([&energy_of, s, k] { energy_of(s->finishing[k]); });
     for (std::thread& t : th) t.join();
   }
+  for (size_t k = 0; k < n_fin; ++k) {
+    Retire& x = s->finishing[k];
+    pbgpu_result& o = out[(*n_out)++];
+    std::memset(&o, 0, sizeof(o));
+    o.id = x.r.id;
+    o.user_tag = x.r.tag;
+    o.status = x.st;
+    o.stats = x.stats;
+    o.energy = x.energy;
+    o.latency_ms = ms_since(x.r.t_submit);
+    o.queue_ms = std::chrono::duration<double, std::milli>(x.r.t_admit - x.r.t_submit).count();
+    s->idle.push_back(x.r.ctx);
+    ++s->completed;
+  }
+  s->finishing.erase(s->finishing.begin(), s->finishing.begin() + n_fin);
   // 3. the batch launch completes
   int active = 0;
   if (launched && (st = pbgpu_batch_wait(s->batch, &active)) != PBGPU_OK)
     return s->fail(st, std::string("server: ") + pbgpu_batch_last_error(s->batch));
-  // 4. retire converged members (as many as the output array holds)
+  // 4. converged members leave the batch with their potentials; their
+  //    energies run during the next tick
   for (size_t k = 0; k < s->running.size();) {
-    if (n_out && *n_out >= cap) break;
     Running& r = s->running[k];
     int done = 0;
     pbgpu_solve_stats stats{};
@@ -393,19 +430,9 @@ int pbgpu_server_progress(pbgpu_server* s, pbgpu_result* out, int cap, int* n_ou
       ++k;
       continue;
     }
-    pbgpu_result& o = out[(*n_out)++];
-    std::memset(&o, 0, sizeof(o));
-    o.id = r.id;
-    o.user_tag = r.tag;
-    o.status = stats.status;
-    o.stats = stats;
-    if (stats.status == PBGPU_OK) o.status = pbgpu_energy(r.ctx, s->opts.energy_fast, &o.energy);
-    o.latency_ms = ms_since(r.t_submit);
-    o.queue_ms = std::chrono::duration<double, std::milli>(r.t_admit - r.t_submit).count();
+    s->finishing.push_back(Retire{r, stats, pbgpu_energy_out{}, stats.status});
     pbgpu_batch_remove(s->batch, r.slot);
-    s->idle.push_back(r.ctx);
     s->running.erase(s->running.begin() + k);
-    ++s->completed;
   }
   // 5. the newly set-up requests join the batch (they start next tick)
   for (Admit& a : adm) {
