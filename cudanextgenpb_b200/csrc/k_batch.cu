@@ -470,8 +470,7 @@ int ensure_capacity(pbgpu_batch* B) {
     BATCH_CUDA(B, cudaMemcpyAsync(nst.get(), B->st.get(), B->st_cap * sizeof(BState), cudaMemcpyDeviceToDevice,
                                   B->stream));
   BATCH_CUDA(B, cudaStreamSynchronize(B->stream));
-  std::swap(B->st.p, nst.p);
-  std::swap(B->st.n, nst.n);
+  B->st.swap(nst);
   B->h64.resize(cap);
   B->h32.resize(cap);
   BATCH_CUDA(B, B->m64.alloc(cap));
@@ -486,6 +485,7 @@ template <typename TI>
 int prepare_member(pbgpu_batch* B, int slot) {
   Context* c = &B->slots[slot]->c;
   AcctScope acct(&c->dev_bytes);
+  StreamScope sscope(c->stream);  // pool allocations on the member's own stream
   BATCH_CUDA(B, cudaStreamSynchronize(c->stream));  // the member's assembly is complete
   if (c->G != 4 || c->C != 32) return B->fail(PBGPU_ERR_ARG, "batch: members must be assembled with chunk 32, group 4");
   const int64_t n_pad = c->n_slices * c->C;
@@ -501,6 +501,7 @@ int prepare_member(pbgpu_batch* B, int slot) {
     if (e == cudaSuccess) e = c->sval32.alloc(c->sell_len);
   }
   if (e != cudaSuccess) return bfail(B, e, "batch: member vectors");
+  BATCH_CUDA(B, cudaStreamSynchronize(c->stream));  // the allocations are ordered on that stream
   BATCH_CUDA(B, cudaMemsetAsync(c->x.get(), 0, n_pad * sizeof(double), B->stream));
   if (mixed) {
     const int g = (int)std::min<int64_t>((c->sell_len + kBlock - 1) / kBlock, (int64_t)B->sm_count * 8);
@@ -709,8 +710,10 @@ template <typename TI>
 int finish_member(pbgpu_batch* B, int slot, pbgpu_solve_stats* stats) {
   Context* c = &B->slots[slot]->c;
   AcctScope acct(&c->dev_bytes);
+  StreamScope sscope(c->stream);  // pool allocations on the member's own stream
   const BState& S = B->st_host[slot];
   BATCH_CUDA(B, c->phi.alloc(c->n));
+  BATCH_CUDA(B, cudaStreamSynchronize(c->stream));
   const BMember<TI>* dm;
   if constexpr (std::is_same<TI, float>::value)
     dm = B->m32.get();

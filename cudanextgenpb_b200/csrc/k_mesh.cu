@@ -917,8 +917,7 @@ struct Builder {
     k_split_fill<<<grid_for(n, 256), 256, 0, st()>>>(leaves.get(), marks.get(), n, off.get(), leaves2.get());
     PBGPU_LAUNCHED(c);
     PBGPU_CUDA(c, cudaStreamSynchronize(st()));
-    std::swap(leaves.p, leaves2.p);
-    std::swap(leaves.n, leaves2.n);
+    leaves.swap(leaves2);
     std::swap(leaves.acct, leaves2.acct);
     n = nn;
     return rekey();
@@ -1025,6 +1024,7 @@ extern "C" int pbgpu_build_mesh(pbgpu_ctx* h, const pbgpu_mesh_build* in) {
   for (int a = 0; a < 3; ++a)
     if (!(in->hi[a] > in->lo[a])) return c->fail(PBGPU_ERR_ARG, "build_mesh: empty domain box");
   AcctScope acct(&c->dev_bytes);
+  StreamScope sscope(c->stream);
   if (cudaSetDevice(c->device) != cudaSuccess) return c->fail(PBGPU_ERR_CUDA, "build_mesh: cudaSetDevice");
   cudaGetLastError();
   c->have_mesh = c->have_markers = c->have_incidence = c->have_density = c->have_system = c->have_phi = false;

@@ -54,6 +54,7 @@ int pbgpu_autotune(pbgpu_ctx* h, int iterations, pbgpu_sell_opts* best, int* bes
   if (!c->have_markers || !c->have_density) return c->fail(PBGPU_ERR_STATE, "autotune: density map required");
   if (iterations <= 0) iterations = 24;
   AcctScope acct(&c->dev_bytes);
+  StreamScope sscope(c->stream);
   if (cudaSetDevice(c->device) != cudaSuccess) return c->fail(PBGPU_ERR_CUDA, "autotune: cudaSetDevice");
   struct Cand {
     pbgpu_sell_opts s;

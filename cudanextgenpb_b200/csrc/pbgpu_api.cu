@@ -5,6 +5,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <sstream>
 #include <string>
@@ -21,6 +23,60 @@ int cuda_fail(Context* c, cudaError_t e, const char* what) {
 }
 
 cudaError_t ensure_tmp(Context* c, size_t bytes) { return c->tmp.alloc(bytes > 0 ? bytes : 1); }
+
+// One pool per device, kept for the life of the process.  Its release
+// threshold is unlimited, so memory that a context frees stays cached for the
+// next allocation on that device instead of going back at every
+// synchronisation; pool_trim hands the unused part back (when a context is
+// destroyed).
+static std::mutex g_pool_mu;
+static std::map<int, cudaMemPool_t> g_pools;
+
+cudaMemPool_t device_pool() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto it = g_pools.find(dev);
+  if (it != g_pools.end()) return it->second;
+  cudaMemPool_t pool = nullptr;
+  int supported = 0;
+  if (cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, dev) == cudaSuccess && supported) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    if (cudaMemPoolCreate(&pool, &props) == cudaSuccess) {
+      uint64_t threshold = UINT64_MAX;
+      if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold) != cudaSuccess) {
+        cudaMemPoolDestroy(pool);
+        pool = nullptr;
+      }
+    } else {
+      pool = nullptr;
+    }
+  }
+  cudaGetLastError();
+  g_pools[dev] = pool;
+  return pool;
+}
+
+void pool_trim() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    auto it = g_pools.find(dev);
+    if (it != g_pools.end()) pool = it->second;
+  }
+  if (pool && cudaMemPoolTrimTo(pool, 0) != cudaSuccess) cudaGetLastError();
+}
 
 template <typename T>
 static int upload(Context* c, DBuf<T>& d, const T* h, size_t count) {
@@ -69,6 +125,7 @@ using namespace pbgpu;
 // is set), so it is not blamed on this call's launches.
 #define SET_DEVICE(C)                                                                         \
   AcctScope _acct(&(C)->dev_bytes);                                                           \
+  StreamScope _sscope((C)->stream);                                                           \
   do {                                                                                        \
     cudaError_t _e = cudaSetDevice((C)->device);                                              \
     if (_e != cudaSuccess) return cuda_fail((C), _e, "cudaSetDevice");                        \
@@ -122,12 +179,16 @@ void pbgpu_ctx_destroy(pbgpu_ctx* h) {
   if (!h) return;
   Context* c = &h->c;
   cudaSetDevice(c->device);
-  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaStream_t st = c->stream;
+  const bool own = c->own_stream;
+  if (st) cudaStreamSynchronize(st);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ks_host) cudaFreeHost(c->ks_host);
-  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
-  delete h;  // DBuf destructors free device memory
+  delete h;  // DBuf destructors free device memory (pool buffers on the stream)
+  if (st) cudaStreamSynchronize(st);
+  if (own && st) cudaStreamDestroy(st);
+  pool_trim();
 }
 
 const char* pbgpu_last_error(const pbgpu_ctx* h) { return h ? h->c.err.c_str() : "null context"; }

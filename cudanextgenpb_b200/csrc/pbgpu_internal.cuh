@@ -2,6 +2,8 @@
 // device-side helpers shared by the kernels.  B200 (sm_100a) only.
 #pragma once
 #include <cuda_runtime.h>
+
+#include <utility>
 #include <stdint.h>
 
 #include <cstdio>
@@ -30,40 +32,110 @@ struct AcctScope {
   ~AcctScope() { tl_acct = prev; }
 };
 
+// Stream-ordered allocation.  Inside an API call on a context (StreamScope,
+// set with the accounting scope) buffers come from a per-device pool on the
+// stream the call works on, and go back to the pool on that stream: growing
+// a buffer then waits for nothing but that stream.  A cudaFree would wait for
+// the whole device -- every other context's work and a running batch kernel
+// -- which serialised contexts that are reused for systems of varying sizes.
+// Outside such a scope, and while the stream is being captured into a graph,
+// buffers use cudaMalloc / cudaFree.
+inline thread_local cudaStream_t tl_stream = nullptr;
+inline thread_local bool tl_pooled = false;
+
+struct StreamScope {
+  cudaStream_t prev;
+  bool prev_pooled;
+  explicit StreamScope(cudaStream_t s) : prev(tl_stream), prev_pooled(tl_pooled) {
+    tl_stream = s;
+    tl_pooled = true;
+  }
+  ~StreamScope() {
+    tl_stream = prev;
+    tl_pooled = prev_pooled;
+  }
+};
+
+// The library's memory pool on the current device (created on first use;
+// freed memory stays in it for reuse until pool_trim); null if the device has
+// no memory pools.
+cudaMemPool_t device_pool();
+// Returns the unused memory of the current device's pool to the device.
+void pool_trim();
+
+inline bool stream_capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+    cudaGetLastError();
+    return true;  // unknown: take the plain path
+  }
+  return st != cudaStreamCaptureStatusNone;
+}
+
 // Device buffer owned by a context.
 template <typename T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0;
   int64_t* acct = nullptr;
+  cudaStream_t s = nullptr;  // stream of a pool allocation
+  bool pooled = false;
   DBuf() = default;
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
   ~DBuf() { release(); }
   void release() {
     if (p) {
-      cudaFree(p);
+      if (pooled)
+        cudaFreeAsync(p, s);
+      else
+        cudaFree(p);
       if (acct) *acct -= (int64_t)(n * sizeof(T));
     }
     p = nullptr;
     n = 0;
     acct = nullptr;
+    s = nullptr;
+    pooled = false;
   }
   cudaError_t alloc(size_t count) {
     if (count <= n && p) return cudaSuccess;
     release();
     if (count == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    const size_t bytes = count * sizeof(T);
+    cudaError_t e;
+    cudaMemPool_t pool = (tl_pooled && !stream_capturing(tl_stream)) ? device_pool() : nullptr;
+    if (pool) {
+      e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), bytes, pool, tl_stream);
+      if (e == cudaSuccess) {
+        pooled = true;
+        s = tl_stream;
+      }
+    } else {
+      e = cudaMalloc(&p, bytes);
+      if (e == cudaErrorMemoryAllocation) {  // memory cached in the pool is not cudaMalloc's
+        cudaGetLastError();
+        pool_trim();
+        e = cudaMalloc(&p, bytes);
+      }
+    }
     if (e == cudaSuccess) {
       n = count;
       acct = tl_acct;
-      if (acct) *acct += (int64_t)(count * sizeof(T));
+      if (acct) *acct += (int64_t)bytes;
     } else {
       p = nullptr;
     }
     return e;
   }
   T* get() const { return p; }
+  void swap(DBuf& o) {
+    std::swap(p, o.p);
+    std::swap(n, o.n);
+    std::swap(acct, o.acct);
+    std::swap(s, o.s);
+    std::swap(pooled, o.pooled);
+  }
 };
 
 struct Rays {
