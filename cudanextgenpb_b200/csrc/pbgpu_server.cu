@@ -22,11 +22,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
-#include <mutex>
 #include <cstring>
 #include <deque>
+#include <functional>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -387,16 +389,22 @@ int pbgpu_server_progress(pbgpu_server* s, pbgpu_result* out, int cap, int* n_ou
   auto energy_of = [s](Retire& x) {
     if (x.st == PBGPU_OK) x.st = pbgpu_energy(x.r.ctx, s->opts.energy_fast, &x.energy);
   };
-  if (adm.size() + n_fin == 1) {
-    if (n_fin)
-      energy_of(s->finishing[0]);
-    else
-      adm[0].st = setup_request(s, adm[0].ctx, adm[0].p.req);
-  } else if (adm.size() + n_fin > 1) {
+  // at most `workers` host threads: a thread waiting in a stream
+  // synchronisation spins, and one thread per job oversubscribes the host
+  std::vector<std::function<void()>> jobs;
+  jobs.reserve(adm.size() + n_fin);
+  for (Admit& a : adm) jobs.emplace_back([s, &a] { a.st = setup_request(s, a.ctx, a.p.req); });
+  for (size_t k = 0; k < n_fin; ++k) jobs.emplace_back([&energy_of, s, k] { energy_of(s->finishing[k]); });
+  if (!jobs.empty()) {
+    std::atomic<size_t> next{0};
+    auto run = [&jobs, &next] {
+      for (size_t k; (k = next.fetch_add(1)) < jobs.size();) jobs[k]();
+    };
+    const size_t nth = std::min(jobs.size(), (size_t)std::max(1, s->opts.workers));
     std::vector<std::thread> th;
-    th.reserve(adm.size() + n_fin);
-    for (Admit& a : adm) th.emplace_back([s, &a] { a.st = setup_request(s, a.ctx, a.p.req); });
-    for (size_t k = 0; k < n_fin; ++k) th.emplace_back([&energy_of, s, k] { energy_of(s->finishing[k]); });
+    th.reserve(nth - 1);
+    for (size_t t = 1; t < nth; ++t) th.emplace_back(run);
+    run();
     for (std::thread& t : th) t.join();
   }
   for (size_t k = 0; k < n_fin; ++k) {
