@@ -444,6 +444,8 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   c->C = C;
   c->sigma = sigma;
   c->G = G;
+  c->have_system = false;  // a failed re-assembly leaves no stale system behind
+  c->have_phi = false;
   const int64_t n = c->n;
   const double3 lo = make_double3(c->lo[0], c->lo[1], c->lo[2]);
   const double3 len = make_double3(c->len[0], c->len[1], c->len[2]);
@@ -459,12 +461,10 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   Scratch<int> ovf(c, kScAsmOvf);
   PBGPU_CUDA(c, ovf.alloc(1));
   PBGPU_CUDA(c, cudaMemsetAsync(ovf.get(), 0, sizeof(int), c->stream));
+  // a row longer than kMaxRow keeps kMaxRow in rowlen and raises the flag,
+  // which is read with the matrix size below, before any row is filled
   k_row_len<<<grid_for(n, 128), 128, 0, c->stream>>>(A, c->rowlen.get(), ovf.get());
   PBGPU_LAUNCHED(c);
-  int h_ovf = 0;
-  PBGPU_CUDA(c, cudaMemcpyAsync(&h_ovf, ovf.get(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
-  if (h_ovf) return c->fail(PBGPU_ERR_CAPACITY, "assemble: a matrix row has more than kMaxRow columns");
 
   // SELL-C-sigma permutation
   const int64_t n_slices = (n + C - 1) / C, n_pad = n_slices * C;
@@ -485,7 +485,6 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
     PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(c->tmp.get(), bytes, k0.get(), k1.get(), id0.get(), c->perm.get(),
                                                   (int)n, 0, 64, c->stream));
     c->launches += cub_radix_launches(n, 64);
-    PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   } else {
     k_identity<<<grid_for(n, 256), 256, 0, c->stream>>>(c->perm.get(), n);
     PBGPU_LAUNCHED(c);
@@ -516,8 +515,11 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   k_sum_rowlen<<<grid_for(n, 256), 256, 0, c->stream>>>(c->rowlen.get(), n, nnz_d.get());
   PBGPU_LAUNCHED(c);
   int64_t nnz = 0;
+  int h_ovf = 0;
   PBGPU_CUDA(c, cudaMemcpyAsync(&nnz, nnz_d.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, cudaMemcpyAsync(&h_ovf, ovf.get(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (h_ovf) return c->fail(PBGPU_ERR_CAPACITY, "assemble: a matrix row has more than kMaxRow columns");
   c->n_slices = n_slices;
   c->sell_len = total;
   c->nnz = nnz;
