@@ -60,11 +60,15 @@ def _d(a):
 class Oracle:
     """The CPU restatement of the reference path on one problem's inputs."""
 
-    def __init__(self, prob):
+    def __init__(self, prob, atoms=None):
+        """atoms: (pos, q) to use instead of the problem's own."""
         self.L = load()
         m = prob.mesh_struct()
         rays = (N.PbgpuRays * 3)(*[prob.rays_struct(a) for a in range(3)])
-        pos, q, _ = prob.atoms()
+        if atoms is None:
+            pos, q, _ = prob.atoms()
+        else:
+            pos, q = np.asarray(atoms[0], dtype=np.float64).reshape(-1, 3), np.asarray(atoms[1], dtype=np.float64)
         self.pos, self.q = np.ascontiguousarray(pos), np.ascontiguousarray(q)
         md = prob.model()
         self.s = self.L.oracle_create(C.byref(m), rays, len(q), _d(self.pos), _d(self.q), C.byref(md))
