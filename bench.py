@@ -779,7 +779,7 @@ def main():
     ap.add_argument("--via-batch", action="store_true", help="solve through the persistent multi-system kernel")
     ap.add_argument("--server-mode", default="concurrent", choices=["concurrent", "batched"])
     ap.add_argument("--compare-fp64", action="store_true", help="mixed precision: error against a plain FP64 solve")
-    ap.add_argument("--workers", type=int, default=4)
+    ap.add_argument("--workers", type=int, default=8)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--chunk", type=int, default=32)

@@ -167,7 +167,7 @@ void pbgpu_default_server_opts(pbgpu_server_opts* o) {
   o->blocks_per_sm = 2;
   o->admit_per_tick = 16;
   o->mode = 0;
-  o->workers = 4;
+  o->workers = 8;
   pbgpu_default_solver_opts(&o->solver);
   o->solver.method = PBGPU_CG;
   o->solver.precond = PBGPU_PRECOND_JACOBI;
@@ -192,7 +192,7 @@ int pbgpu_server_create(pbgpu_server** out, int device, const pbgpu_server_opts*
   if (s->opts.steps_per_tick <= 0) s->opts.steps_per_tick = 32;
   if (!(s->opts.hbm_budget_bytes > 0)) s->opts.hbm_budget_bytes = 160e9;
   if (s->opts.mode == 1) {
-    const int nw = s->opts.workers > 0 ? s->opts.workers : 4;
+    const int nw = s->opts.workers > 0 ? s->opts.workers : 8;
     for (int w = 0; w < nw; ++w) {
       pbgpu_ctx* c = nullptr;
       const int st = pbgpu_ctx_create(&c, device, nullptr);

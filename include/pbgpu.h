@@ -404,7 +404,7 @@ typedef struct {
   int mode;                  /* 0: members advance together in the persistent multi-system kernel;
                                 1: `workers` host threads each run whole requests on their own
                                 context and stream, overlapping on the device */
-  int workers;               /* host threads (default 4): mode 1 runs whole requests on them; mode 0
+  int workers;               /* host threads (default 8): mode 1 runs whole requests on them; mode 0
                                 sets up admitted requests and computes energies on them */
 } pbgpu_server_opts;
 
