@@ -1,19 +1,29 @@
-"""Benchmark of the PB assemble/solve/energy path (one JSON line on rank 0).
+"""Benchmark of the PB path (one JSON line on rank 0).
 
-A step is one complete PB solve of one molecule through the GPU path:
-create_markers -> create_density_map -> assemble (SELL-C-sigma) -> Krylov solve
--> potential at atoms -> energy.  Default workload (the plain-FP64 2,000-atom
-configuration): a seeded synthetic globular molecule, 2,000 atoms on a lattice
-subset inside an 18 A sphere, net charge -3 e, mesh_shape 0 at scale 2/A with 3
-surface refinement levels, Jacobi-CG to a relative residual of 1e-8.
+Default workload (`serve`): a seeded stream of PB requests, each a synthetic
+molecule (atoms log-uniform in 200-2,000, scale 2/A, 1 or 2 surface levels).
+A request is served whole on the GPU: the mesh (initial octree, surface
+refinement, nodes, hanging nodes, ray tables), create_markers,
+create_density_map, assembly (SELL-C-sigma), the Krylov solve and the energy.
+The same requests run twice in one process:
 
-value   solves/s with mesh, rays and atoms already resident in HBM.
-e2e     the same, through the C ABI from pinned host buffers: every step uploads
-        the inputs (pbgpu_set_mesh / set_rays / set_atoms / set_model) and reads
-        back the potential at the atoms and the energies.
-Multi-GPU (torchrun): one process per GPU, each solving its own copy of the
-molecule (independent solves, no data-path collective); timing is the max over
-ranks.  --impl reference times the CPU restatement of the reference path.
+  served  the continuous-batching server, worker contexts each serving whole
+          requests on their own stream, FP32-inner / FP64-refined CG;
+  plain   one request at a time through the plain FP64 path.
+
+value            served solves/s (all timed requests offered at once);
+latency_ms       p50/p95/p99 from arrival to result under Poisson arrivals at
+                 70 % of that capacity;
+speedup_vs_plain_fp64, and the energy error of every served request against
+the plain FP64 result and, on three molecules, against the CPU oracle.
+roofline         the CG SpMV of the plain FP64 path on the 2,000-atom molecule.
+
+Single-molecule workloads (`mol2000`, `mol2000l2`, `mol25k`, ...) time one
+molecule's whole path per step (value: inputs resident in HBM; e2e: through
+the C ABI from pinned host buffers).  Multi-GPU (torchrun, or --gpus N which
+starts it): replicas, one process per GPU, timing the max over ranks.
+--impl reference times the CPU oracle, whole solves, with inputs prepared in a
+separate process.
 """
 from __future__ import annotations
 
@@ -46,11 +56,6 @@ WORKLOADS = {
     # host mesh build stays within a minute
     "mol25k": (25000, 45.0, 7.0, 25000, 2.0, 2),
 }
-# Jacobi-CG iterations to ||r|| <= 1e-8 ||b|| on the large workloads (the same
-# count on the GPU and on the CPU oracle: one algorithm, differing only in
-# rounding); the CPU arm times a sample of iterations and scales to this count.
-# Smaller workloads are solved to convergence on the CPU to find it.
-CG_ITERS_1E8 = {"mol2000": 1405, "mol2000l2": 889}
 
 
 def log(*a):
@@ -457,7 +462,7 @@ def run_ours(args, rank, world, local):
                 "bytes_per_iteration_fp32_inner": 8 * nnz + 52 * n,
             }
         if world == 1 and not args.no_cpu_baseline:
-            result["cpu_baseline"] = cpu_baseline(prob, g, int(np.median(iters)), args)
+            result["cpu_baseline"] = cpu_baseline(prob, args)
     g.close()
     if dist:
         dist.barrier()
@@ -479,68 +484,124 @@ def workload_desc(name, info):
             (na, rad, net, seed, scale, levels, info["n_nodes"]))
 
 
-def cpu_baseline(prob, g, gpu_iters, args):
-    """The oracle's Jacobi-CG on the same assembled system, all host cores: a
-    bounded sample of iterations, scaled to solves/s with the GPU's iteration
-    count.  Assembly and energy are not timed on the CPU side."""
+def cpu_baseline(prob, args):
+    """The oracle's whole path on the same molecule (markers, density,
+    assembly, Jacobi-CG to the tolerance, potential at the atoms, energy), one
+    solve on all host cores, timed."""
     from oracle_lib import Oracle
     o = Oracle(prob)
-    rp, col, val, rhs = g.system()
-    o.set_system(rp, col, val, rhs)
-    threads = os.cpu_count() or 1
-    it = args.cpu_iters
-    t = o.time_cg(it, threads)
-    per_iter = t / it
+    t0 = time.perf_counter()
+    e, _, it, _ = o.run("cg", args.tol)
+    o.phi_on_atoms()
+    dt = time.perf_counter() - t0
     o.close()
-    return {"value": 1.0 / (per_iter * gpu_iters), "unit": "solves/s", "cores": threads, "kind": "port",
-            "sample": "%d Jacobi-CG iterations of the CPU oracle on the same %d-DoF system (%.2f s, %.1f ms/iter), "
-                      "scaled by the GPU's %d iterations per solve; assembly and energy excluded"
-                      % (it, g.n, t, 1e3 * per_iter, gpu_iters)}
+    return {"value": 1.0 / dt, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": "one whole solve of the same molecule by the CPU oracle: markers, density, assembly, "
+                      "Jacobi-CG to %g (%d iterations), potential at the atoms, energy (%.1f s)" % (args.tol, it, dt),
+            "energy_kT": e["sum"]}
+
+
+def molecule_spec(args):
+    """(n_atoms, radius, net charge, seed, levels, scale) of a single-molecule workload."""
+    na, rad, net, seed, scale, levels = WORKLOADS[args.workload]
+    return (na, rad, net, seed, levels, scale)
+
+
+def prepare_inputs(specs, outdir, threads=8):
+    """Host builds (libpbhost) of the given molecules, saved as numpy arrays,
+    one file per molecule: the inputs of the reference arm, made in a process
+    of their own so the timed process loads no library of this package."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from cudanextgenpb_b200 import configs
+    from oracle_lib import problem_arrays
+
+    def one(item):
+        key, (na, rad, net, seed, lv, scale) = item
+        prob = configs.make_globular_problem(na, rad, net, seed, scale=scale, levels=lv).build()
+        np.savez(os.path.join(outdir, "%s.npz" % key), **problem_arrays(prob))
+        prob.close()
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(one, specs.items()))
+
+
+def reference_inputs(specs, outdir):
+    """Runs prepare_inputs for `specs` ({key: spec}) in a subprocess."""
+    spec_file = os.path.join(outdir, "specs.json")
+    json.dump({k: list(v) for k, v in specs.items()}, open(spec_file, "w"))
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--prepare-inputs", outdir],
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("input preparation failed: " + r.stderr[-2000:])
+
+
+def oracle_request(path, tol):
+    """The oracle's whole path on one saved molecule: markers, density,
+    assembly, Jacobi-CG to tol, potential at the atoms, energy.  Returns
+    (seconds, iterations, energy)."""
+    from oracle_lib import ArrayProblem, Oracle
+    d = dict(np.load(path))
+    t0 = time.perf_counter()
+    o = Oracle(ArrayProblem(d))
+    e, _, it, _ = o.run("cg", tol)
+    o.phi_on_atoms()
+    dt = time.perf_counter() - t0
+    o.close()
+    return dt, it, e["sum"]
 
 
 def run_reference(args, rank, world):
-    """CPU restatement of the reference path (oracle port), rank 0 only."""
+    """The reference arm: the CPU oracle (this package's C++ restatement of
+    the reference path; the reference itself cannot be built here) timed on
+    the host cores, whole solves with CG run to the tolerance.  Rank 0 alone
+    runs; its inputs come from a separate process (prepare_inputs)."""
     if rank != 0:
         return None
-    from oracle_lib import Oracle
-    prob = build_problem(args.workload)
-    info = prob.info()
-    o = Oracle(prob)
-    t0 = time.time()
-    o.markers()
-    o.density()
-    o.assemble("rows")
-    t_setup = time.time() - t0
-    # the energy post-process (its cost does not depend on the potential's values)
-    o.set_phi(np.zeros(o.n))
-    t0 = time.time()
-    o.energy()
-    t_setup += time.time() - t0
-    # iterations the full solve needs
-    if args.ref_iters:
-        iters = args.ref_iters
-    elif args.tol == 1e-8 and args.workload in CG_ITERS_1E8:
-        iters = CG_ITERS_1E8[args.workload]
-    else:
-        _, iters, _ = o.solve("cg", args.tol)
+    import tempfile
+    serve = args.workload in SERVES
+    with tempfile.TemporaryDirectory() as tmp:
+        if serve:
+            per_step = SERVES[args.workload][5]
+            specs = serve_specs(args.workload)
+            # a step is one request: the first K requests of the timed stream
+            picks = serve_picks(args.workload, (args.warmup + args.steps) * per_step)[args.warmup * per_step:]
+            timed = [int(k) for k in picks[:args.steps]]
+            small = min(range(len(specs)), key=lambda k: specs[k][0])
+            warm = [small] * args.warmup
+            need = {"m%d" % k: tuple(specs[k]) + (2.0,) for k in set(timed + warm)}
+            files = lambda ks: [os.path.join(tmp, "m%d.npz" % k) for k in ks]
+            desc = ("the first %d requests of the timed stream, one at a time (pool molecules %s); warm-up: %d "
+                    "solves of the smallest pool molecule" % (args.steps, timed, args.warmup))
+        else:
+            need = {"w": molecule_spec(args), "s": (60, 7.0, -3.0, 60, 1, 2.0)}
+            files = lambda ks: [os.path.join(tmp, "%s.npz" % k) for k in ks]
+            timed, warm = ["w"] * args.steps, ["s"] * args.warmup
+            desc = ("%d whole solves of the molecule; warm-up: %d solves of a 60-atom molecule"
+                    % (args.steps, args.warmup))
+        t0 = time.time()
+        reference_inputs(need, tmp)
+        prep_s = time.time() - t0
+        for f in files(warm):
+            oracle_request(f, args.tol)
+        secs, its = [], []
+        for f in files(timed):
+            dt, it, _ = oracle_request(f, args.tol)
+            secs.append(dt)
+            its.append(it)
     threads = os.cpu_count() or 1
-    samples = []
-    for _ in range(args.warmup):
-        o.time_cg(args.cpu_iters, threads)
-    for _ in range(args.steps):
-        samples.append(o.time_cg(args.cpu_iters, threads) / args.cpu_iters)
-    per_iter = float(np.median(samples))
-    need = iters
-    sec = t_setup + per_iter * need
-    v = 1.0 / sec
+    total = float(sum(secs))
+    v = len(secs) / total
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_desc(args.workload, info), "n_dof": info["n_nodes"]},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(secs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "cg_iterations": its, "tol": args.tol,
+                       "input_preparation_s": prep_s,
+                       "what": "CPU oracle (C++ restatement of the reference path, OpenMP on all host cores): "
+                               "markers, density, assembly, Jacobi-CG to tol, potential at the atoms, energy; "
+                               "meshes built beforehand in a separate process and not timed"},
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port",
-                             "sample": "CPU oracle: markers+density+assembly+energy timed once (%.2f s), %d Jacobi-CG "
-                                       "iterations per step timed, scaled to %d iterations per solve"
-                                       % (t_setup, args.cpu_iters, need)},
+                             "sample": desc + " (%.1f s timed)" % total},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -667,105 +728,325 @@ def run_batch(args, rank, world, local):
 
 
 SERVES = {
-    # name: (pool size, min atoms, max atoms, seed, surface levels, arrivals per s, seconds)
-    "serve": (24, 200, 3000, 5, 1, 200.0, 10.0),
-    # small molecules, offered faster than either path serves them, so the
-    # value is each path's capacity
-    "serve_small": (8, 50, 400, 5, 1, 2000.0, 1.0),
+    # name: (pool size, min atoms, max atoms, seed, surface levels drawn from, requests per step)
+    # the request stream: seeded synthetic molecules (atoms log-uniform in
+    # [min, max], integer net charges), scale 2/A, each request's mesh built on
+    # the GPU as part of serving it
+    "serve": (24, 200, 2000, 5, (1, 2), 8),
+    # small molecules, one surface level
+    "serve_small": (8, 50, 400, 5, (1,), 16),
 }
 
 
+def serve_specs(name):
+    """(n_atoms, radius, net charge, seed, surface levels) of the pool's molecules."""
+    from cudanextgenpb_b200 import configs
+    npool, lo, hi, seed, levels, _ = SERVES[name]
+    specs = configs.molecule_specs(npool, lo, hi, seed)
+    lv = np.random.default_rng(seed + 1).choice(np.array(levels), size=npool)
+    return [(na, rad, net, s, int(l)) for (na, rad, net, s), l in zip(specs, lv)]
+
+
+def serve_picks(name, n):
+    """The pool molecule of each of the first n requests of the stream."""
+    npool, _, _, seed = SERVES[name][:4]
+    return np.random.default_rng(seed + 2).integers(0, npool, size=n)
+
+
+class PoolMolecule:
+    """A request's payload: the molecule (atoms, charges, radii) and its
+    options; the host part of the mesh set-up is only the domain box
+    (create_mesh), the rest is built on the GPU (Problem.mesh_build)."""
+
+    def __init__(self, spec):
+        from cudanextgenpb_b200 import configs
+        na, rad, net, seed, lv = spec
+        self.spec = spec
+        self.prob = configs.make_globular_problem(na, rad, net, seed, scale=2.0, levels=lv)
+        self.build = self.prob.mesh_build()
+        self.pos, self.q, self.radius = self.prob.atoms()
+        self.model = self.prob.model()
+        self.upload_bytes = int(self.pos.nbytes + self.q.nbytes + self.radius.nbytes + 4 * 8 * len(self.q))
+
+
+def plain_request(g, m, opts):
+    """One request through the plain path, one call per reference stage:
+    mesh build, markers, density, assembly, FP64 solve, energy."""
+    g.build_mesh(m.build)
+    g.set_atoms(m.pos, m.q)
+    g.set_model(m.model)
+    g.create_markers()
+    g.create_density_map()
+    g.assemble()
+    st = g.solve(opts)
+    return g.energy(False), st
+
+
+def serve_stream(srv, reqs, arrivals=None):
+    """Submits reqs (all at once, or at `arrivals` seconds after the start) and
+    drains the server; returns (seconds, {tag: result}, {tag: latency ms})."""
+    t0 = time.perf_counter()
+    res, lat = {}, {}
+    nxt, n = 0, len(reqs)
+    if arrivals is None:
+        for r in reqs:
+            srv.submit(r)
+        nxt = n
+    while len(res) < n:
+        now = time.perf_counter() - t0
+        while nxt < n and arrivals[nxt] <= now:
+            srv.submit(reqs[nxt])
+            nxt += 1
+        for r in srv.progress():
+            res[r["tag"]] = r
+            lat[r["tag"]] = 1e3 * (time.perf_counter() - t0 - (arrivals[r["tag"]] if arrivals is not None else 0.0))
+        if nxt < n and not srv.pending()[0] and not srv.pending()[1]:
+            time.sleep(max(0.0, min(arrivals[nxt] - (time.perf_counter() - t0), 0.002)))
+    return time.perf_counter() - t0, res, lat
+
+
+def spmv_roofline(local):
+    """The SpMV roofline on the 2,000-atom molecule at 2 surface levels (3.3 M
+    DoF, matrix > L2), plain FP64 CG solves with CUDA events around every SpMV
+    launch on the context's stream."""
+    from cudanextgenpb_b200 import GpuPath, configs, solver_opts
+    na, rad, net, seed, scale, levels = WORKLOADS["mol2000l2"]
+    prob = configs.make_globular_problem(na, rad, net, seed, scale=scale, levels=levels)
+    g = prob.build_on_gpu(GpuPath(local))
+    g.create_markers()
+    g.create_density_map()
+    g.assemble(32, 2048, 4)
+    opts = solver_opts("cg", tol=1e-8, max_iter=50000)
+    g.solve(opts)
+    g.set_profiling(True)
+    g.reset_counters()
+    for _ in range(3):
+        st = g.solve(opts)
+    cnt = g.counters()
+    nnz = info_nnz(g)
+    g.close()
+    avg = cnt["spmv_ms"] / max(cnt["spmv_launches"], 1)
+    peak, kind = measured_peak()
+    achieved = cnt["spmv_bytes"] / (avg / 1e3) / 1e9
+    tr = spmv_traffic()
+    kname = "k_cg_spmv<double, 4>"
+    traffic = None
+    if tr and kname in tr.get("kernels", {}):
+        traffic = tr["kernels"][kname]["dram_bytes_per_launch"] * (nnz / tr["nnz"])
+    return {"kernel": kname + " (SELL-C-sigma SpMV fused with p.Ap)", "bound": "hbm", "achieved": achieved,
+            "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind_text(kind),
+            "traffic": traffic, "algorithmic_bytes_per_launch": cnt["spmv_bytes"], "avg_launch_ms": avg,
+            "launches_timed": cnt["spmv_launches"],
+            "workload": "2,000-atom molecule, 2 surface levels (%d DoF, nnz %d), plain FP64 Jacobi-CG, %d iterations "
+                        "per solve, 3 solves" % (g.n, nnz, st.iterations)}
+
+
+def peak_kind_text(kind):
+    return "of measured (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else "of fallback"
+
+
+def oracle_serve_parity(pool, ids, e_plain, e_served):
+    """Energies of pool molecules `ids` from the CPU oracle (host-built mesh,
+    tight CG) against the plain FP64 and served energies of the same molecules."""
+    from oracle_lib import Oracle
+    from cudanextgenpb_b200 import configs
+    out = {"molecules": [], "max_rel_err_plain": 0.0, "max_rel_err_served": 0.0}
+    for k in ids:
+        na, rad, net, seed, lv = pool[k].spec
+        prob = configs.make_globular_problem(na, rad, net, seed, scale=2.0, levels=lv).build()
+        o = Oracle(prob)
+        oe, _, it, rel = o.run("cg", 1e-12)
+        o.close()
+        prob.close()
+        ep = abs(e_plain[k] - oe["sum"]) / abs(oe["sum"])
+        es = abs(e_served[k] - oe["sum"]) / abs(oe["sum"])
+        out["molecules"].append({"atoms": na, "levels": lv, "oracle_kT": oe["sum"], "plain_kT": e_plain[k],
+                                 "served_kT": e_served[k], "rel_err_plain": ep, "rel_err_served": es})
+        out["max_rel_err_plain"] = max(out["max_rel_err_plain"], ep)
+        out["max_rel_err_served"] = max(out["max_rel_err_served"], es)
+    return out
+
+
+def serve_cpu_baseline(pool, picks, tol, budget_s=20.0):
+    """The oracle's whole path (markers .. energy, CG to tol) on the stream's
+    first requests, one at a time on all host cores, until budget_s of CPU
+    time: solves/s of that bounded sample."""
+    from oracle_lib import Oracle
+    from cudanextgenpb_b200 import configs
+    done, t_total, ids = 0, 0.0, []
+    for k in picks:
+        na, rad, net, seed, lv = pool[k].spec
+        prob = configs.make_globular_problem(na, rad, net, seed, scale=2.0, levels=lv).build()
+        o = Oracle(prob)
+        t0 = time.perf_counter()
+        o.run("cg", tol)
+        t_total += time.perf_counter() - t0
+        o.close()
+        prob.close()
+        done += 1
+        ids.append(int(k))
+        if t_total >= budget_s:
+            break
+    return {"value": done / t_total, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": "the CPU oracle's markers, density, assembly, Jacobi-CG to %g and energy on the stream's first "
+                      "%d requests (pool molecules %s), one at a time, %.1f s; meshes built on the host beforehand "
+                      "(not timed)" % (tol, done, ids, t_total)}
+
+
 def run_serve(args, rank, world, local):
-    """Serving workload: a seeded Poisson request stream over a pool of
-    synthetic molecules, served by the continuous-batching server, against the
-    plain FP64 path taking the same requests one at a time.  Latency is from
-    each request's arrival time to its result (queueing included)."""
+    """The headline: a seeded request stream of synthetic molecules served by
+    the continuous-batching server (FP32-inner / FP64-refined solves, whole
+    requests on concurrent worker contexts), against the plain FP64 path taking
+    the same requests one at a time.  Every request's mesh (initial octree,
+    surface refinement, nodes, hanging nodes, ray tables) is built on the GPU
+    inside the request.  Replicas under torchrun: every rank serves its own copy
+    of the stream on its own GPU."""
     import torch
 
-    from cudanextgenpb_b200 import GpuPath, Server, configs, solver_opts
+    from cudanextgenpb_b200 import GpuPath, Server, solver_opts
 
-    if rank != 0 and world > 1:
-        return None
     torch.cuda.set_device(local)
-    npool, lo, hi, seed, levels, rate, seconds = SERVES[args.workload]
-    specs = configs.molecule_specs(npool, lo, hi, seed)
-    probs = build_pool(specs, levels)
-    rng = np.random.default_rng(seed)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * seconds * 1.5)))
-    arrivals = arrivals[arrivals < seconds]
-    picks = rng.integers(0, npool, size=len(arrivals))
-    n_req = len(arrivals)
+    dist = None
+    if world > 1:
+        import datetime
 
-    # served
-    srv = Server(local, tol=args.tol, precision=args.precision, max_members=args.max_members,
-                 steps_per_tick=32, inner_tol=1e-4, mode=1 if args.server_mode == "concurrent" else 0,
-                 workers=args.workers)
-    reqs = [srv.request(p) for p in probs]
-    # warm-up: one request of each molecule
-    for r in reqs:
-        srv.submit(r)
-    got = 0
-    while got < npool:
-        got += len(srv.progress())
-    lat_s, e_served = {}, {}
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    nxt = 0
-    while len(lat_s) < n_req:
-        now = time.perf_counter() - t0
-        while nxt < n_req and arrivals[nxt] <= now:
-            r = srv.request(probs[picks[nxt]], tag=nxt)
-            srv.submit(r)
-            nxt += 1
-        for res in srv.progress():
-            k = res["tag"]
-            lat_s[k] = 1e3 * (time.perf_counter() - t0 - arrivals[k])
-            e_served[k] = res["energy"]["sum"]
-        if nxt < n_req and not srv.pending()[0] and not srv.pending()[1]:
-            time.sleep(max(0.0, min(arrivals[nxt] - (time.perf_counter() - t0), 0.002)))
-    t_served = time.perf_counter() - t0
-    srv.close()
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    npool, lo, hi, seed, levels, per_step = SERVES[args.workload]
+    specs = serve_specs(args.workload)
+    pool = [PoolMolecule(s) for s in specs]
+    n_warm, n_req = args.warmup * per_step, args.steps * per_step
+    picks = serve_picks(args.workload, n_warm + n_req)
+    warm, timed = picks[:n_warm], picks[n_warm:]
+    opts64 = solver_opts("cg", tol=args.tol, max_iter=50000)
 
-    # plain FP64, one at a time, same stream
+    def sync_all():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    # ---- plain FP64, one request at a time
     g = GpuPath(local)
-    plain_opts = solver_opts("cg", tol=args.tol, max_iter=50000)
-    e_plain = {}
-    for k in range(npool):
-        g.load(probs[k])
-        g.run(plain_opts)
-    lat_p = {}
-    torch.cuda.synchronize()
+    for k in warm:
+        plain_request(g, pool[k], opts64)
+    g.reset_counters()
+    sync_all()
+    clocks = Clocks(local)
+    clocks.start()
+    e_plain, lat_p, it_p = {}, [], []
     t0 = time.perf_counter()
-    for k in range(n_req):
-        now = time.perf_counter() - t0
-        if arrivals[k] > now:
-            time.sleep(arrivals[k] - now)
-        g.load(probs[picks[k]])
-        e, _ = g.run(plain_opts)
-        e_plain[k] = e["sum"]
-        lat_p[k] = 1e3 * (time.perf_counter() - t0 - arrivals[k])
-    t_plain = time.perf_counter() - t0
+    for k in timed:
+        a = time.perf_counter()
+        e, st = plain_request(g, pool[k], opts64)
+        lat_p.append(1e3 * (time.perf_counter() - a))
+        e_plain[int(k)] = e["sum"]
+        it_p.append(st.iterations)
+    torch.cuda.synchronize()
+    t_plain = max_over_ranks(time.perf_counter() - t0, dist)
+    plain_launches = g.counters()["launches"]
     g.close()
-    err = max(abs(e_served[k] - e_plain[k]) / max(abs(e_plain[k]), 1e-300) for k in range(n_req))
-    ls = np.array([lat_s[k] for k in range(n_req)])
-    lp = np.array([lat_p[k] for k in range(n_req)])
-    value = n_req / t_served
-    plain = n_req / t_plain
-    pct = lambda a: {"p50": float(np.percentile(a, 50)), "p95": float(np.percentile(a, 95)),
-                     "p99": float(np.percentile(a, 99))}
-    return {
-        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": n_req, "warmup": npool,
-        "ms_per_step": 1e3 * t_served / n_req, "latency_ms": pct(ls), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32-inner/f64", "data": "synthetic",
-        "config": {"workload": "Poisson stream %.0f req/s for %.0f s (seed %d) over %d synthetic molecules, atoms "
-                               "log-uniform in %d-%d, scale 2/A, %d surface level(s); continuous-batching server"
-                               % (rate, seconds, seed, npool, lo, hi, levels),
-                   "requests": n_req, "tol": args.tol, "precision": args.precision,
-                   "max_members": args.max_members, "server_mode": args.server_mode, "workers": args.workers,
-                   "plain_solves_per_s": plain, "plain_latency_ms": pct(lp), "speedup_vs_plain": value / plain,
-                   "max_rel_energy_err_vs_plain": err,
-                   "wall_clock": "host perf_counter; latency from each request's scheduled arrival"},
-    }
+
+    # ---- served: continuous batching of whole requests, FP32-inner solves
+    srv = Server(local, tol=args.tol, precision=args.precision, mode=1 if args.server_mode == "concurrent" else 0,
+                 workers=args.workers, max_members=args.max_members, steps_per_tick=32, inner_tol=1e-4)
+
+    def requests(ks):
+        return [srv.request(pool[k].prob, tag=j, build=pool[k].build) for j, k in enumerate(ks)]
+
+    serve_stream(srv, requests(warm))
+    sync_all()
+    l0 = srv.stats()["launches"]
+    t_served, res, _ = serve_stream(srv, requests(timed))
+    torch.cuda.synchronize()
+    t_served = max_over_ranks(t_served, dist)
+    served_launches = srv.stats()["launches"] - l0
+    # latency at an offered load the server sustains: Poisson arrivals at 70 %
+    # of the capacity just measured
+    rate = 0.7 * len(timed) / t_served
+    arrivals = np.cumsum(np.random.default_rng(seed + 3).exponential(1.0 / rate, size=len(timed)))
+    sync_all()
+    t_lat, res_lat, lat_s = serve_stream(srv, requests(timed), arrivals)
+    srv.close()
+    ck = clocks.stop()
+
+    bad = [r for r in list(res.values()) + list(res_lat.values()) if r["status"] != 0]
+    e_served = {}
+    err_plain = 0.0
+    for j, k in enumerate(timed):
+        for r in (res[j], res_lat[j]):
+            e_served[int(k)] = r["energy"]["sum"]
+            err_plain = max(err_plain, abs(r["energy"]["sum"] - e_plain[int(k)]) / abs(e_plain[int(k)]))
+    result = None
+    if rank == 0:
+        value = world * len(timed) / t_served
+        plain = world * len(timed) / t_plain
+        pct = lambda a: {"p50": float(np.percentile(a, 50)), "p95": float(np.percentile(a, 95)),
+                         "p99": float(np.percentile(a, 99))}
+        h2d = sum(pool[k].upload_bytes for k in timed)
+        # the oracle on the three smallest molecules the stream served (tight solve)
+        served_ids = sorted(set(int(k) for k in timed), key=lambda k: pool[k].spec[0])[:3]
+        parity = oracle_serve_parity(pool, served_ids, e_plain, e_served)
+        roof = spmv_roofline(local)
+        n_dof = [0]
+        result = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_served / args.steps,
+            "latency_ms": pct(list(lat_s.values())), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32-inner/f64" if args.precision == "mixed" else "f64",
+            "data": "synthetic",
+            "config": {
+                "workload": "PB request stream: %d requests per step (%d timed) drawn from %d synthetic molecules "
+                            "(atoms log-uniform in %d-%d, FCC-lattice subsets, net charge in [-5, 5], seed %d), "
+                            "scale 2/A, %s surface level(s); every request's mesh built on the GPU inside it; served "
+                            "by %d concurrent worker contexts with %s solves to rel. residual %g, against the plain "
+                            "FP64 path one request at a time" % (per_step, len(timed), npool, lo, hi, seed,
+                                                                  "/".join(map(str, levels)), args.workers,
+                                                                  "FP32-inner/FP64-refined" if args.precision ==
+                                                                  "mixed" else "FP64", args.tol),
+                "speedup_vs_plain_fp64": value / plain,
+                "plain_fp64_solves_per_s": plain,
+                "plain_fp64_latency_ms": pct(lat_p),
+                "latency_load": "Poisson arrivals at %.1f req/s (70%% of the measured capacity), %d requests; "
+                                "latency from arrival to result" % (rate, len(timed)),
+                "max_rel_energy_err_served_vs_plain_fp64": err_plain,
+                "oracle_parity": parity,
+                "failed_requests": len(bad),
+                "plain_cg_iterations_median": float(np.median(it_p)),
+                "served_iterations_median": float(np.median([r["iterations"] for r in res.values()])),
+                "tol": args.tol, "precision": args.precision, "server_mode": args.server_mode,
+                "workers": args.workers,
+                "plain_gpu_launches": plain_launches,
+                "l2": "each request's matrix and vectors are smaller than L2 for most of the pool; requests run "
+                      "back to back with no L2 flush, as a server would run them",
+                "wall_clock": "host perf_counter around each stream after a device synchronize",
+                "parallelism": "replicas (one server per GPU)" if world > 1 else "one GPU",
+            },
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": h2d // args.steps,
+                    "d2h_bytes_per_step": 96 * per_step,
+                    "note": "the same measurement as value: a request is a host-side molecule that the server "
+                            "uploads, meshes and solves on the GPU and answers to the host"},
+            "roofline": roof,
+            "gpu_launches": served_launches,
+            "clocks": ck,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = serve_cpu_baseline(pool, timed, args.tol)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def spawn_replicas(n):
+    """Re-run this command as n ranks under torchrun on this node (127.0.0.1
+    rendezvous on a free port); returns its exit status."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(n),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
 
 
 def main():
@@ -774,35 +1055,43 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mol2000", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(SERVES))
+    ap.add_argument("--workload", default="serve", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(SERVES))
     ap.add_argument("--max-members", type=int, default=64)
     ap.add_argument("--via-batch", action="store_true", help="solve through the persistent multi-system kernel")
     ap.add_argument("--server-mode", default="concurrent", choices=["concurrent", "batched"])
     ap.add_argument("--compare-fp64", action="store_true", help="mixed precision: error against a plain FP64 solve")
     ap.add_argument("--workers", type=int, default=8)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="default: mixed for the served stream, fp64 otherwise")
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--chunk", type=int, default=32)
     ap.add_argument("--sigma", type=int, default=2048)
     ap.add_argument("--group", type=int, default=4)
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "block_jacobi", "none"])
-    ap.add_argument("--cpu-iters", type=int, default=30)
-    ap.add_argument("--ref-iters", type=int, default=0)
+    ap.add_argument("--prepare-inputs", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.prepare_inputs:
+        specs = json.load(open(os.path.join(args.prepare_inputs, "specs.json")))
+        prepare_inputs({k: tuple(v) for k, v in specs.items()}, args.prepare_inputs)
+        return
     args.warmup = max(args.warmup, 3)
+    if args.precision is None:
+        args.precision = "mixed" if args.workload in SERVES else "fp64"
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: start the replicas under torchrun (rank 0 prints the line)
+        sys.exit(spawn_replicas(args.gpus))
     rank, world, local = dist_env()
     from cudanextgenpb_b200 import build as b
     if rank == 0:
         b.build_all()
-    if args.workload in SERVES:
-        res = run_serve(args, rank, world, local) if args.impl == "ours" else {
-            "impl": "reference", "unavailable": "the serving workload is measured against the plain GPU path"}
+    if args.impl == "reference" and args.workload not in BATCHES:
+        res = run_reference(args, rank, world)
+    elif args.workload in SERVES:
+        res = run_serve(args, rank, world, local)
     elif args.workload in BATCHES:
         res = run_batch(args, rank, world, local) if args.impl == "ours" else {
             "impl": "reference", "unavailable": "batched workloads are measured against the plain GPU path"}
-    elif args.impl == "reference":
-        res = run_reference(args, rank, world)
     else:
         res = run_ours(args, rank, world, local)
     if rank == 0 and res is not None:

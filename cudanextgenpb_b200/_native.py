@@ -77,12 +77,13 @@ class PbgpuCounters(C.Structure):
 class PbgpuMeshBuild(C.Structure):
     _fields_ = [("n_oct", i64), ("oct_xyz", P(i32)), ("oct_level", P(C.c_int8)), ("lo", dbl * 3), ("hi", dbl * 3),
                 ("locate_tol", dbl), ("refine", C.c_int), ("minlevel", C.c_int), ("maxlevel", C.c_int),
-                ("unilevel", C.c_int), ("n_spheres", i64), ("spheres", P(dbl))]
+                ("unilevel", C.c_int), ("n_spheres", i64), ("spheres", P(dbl)), ("init_level", C.c_int),
+                ("box_level", C.c_int), ("box_lo", dbl * 3), ("box_hi", dbl * 3)]
 
 
 class PbgpuRequest(C.Structure):
     _fields_ = [("mesh", P(PbgpuMesh)), ("rays", PbgpuRays * 3), ("n_atoms", i64), ("pos", P(dbl)),
-                ("charge", P(dbl)), ("model", P(PbgpuModel)), ("user_tag", i64)]
+                ("charge", P(dbl)), ("model", P(PbgpuModel)), ("user_tag", i64), ("build", P(PbgpuMeshBuild))]
 
 
 class PbgpuResult(C.Structure):
@@ -106,7 +107,7 @@ class PbhostInfo(C.Structure):
 
 PBGPU_OK = 0
 PBGPU_ERR_ARG, PBGPU_ERR_CUDA, PBGPU_ERR_OOM, PBGPU_ERR_STATE, PBGPU_ERR_CAPACITY = 1, 2, 3, 4, 5
-PBGPU_NOT_CONVERGED, PBGPU_BREAKDOWN, PBGPU_TIMEOUT = 10, 11, 12
+PBGPU_NOT_CONVERGED, PBGPU_BREAKDOWN, PBGPU_TIMEOUT, PBGPU_REJECTED = 10, 11, 12, 13
 PBGPU_CG, PBGPU_BICGSTAB, PBGPU_CGS = 0, 1, 2
 PBGPU_PRECOND_NONE, PBGPU_PRECOND_JACOBI, PBGPU_PRECOND_BLOCK_JACOBI = 0, 1, 2
 PBGPU_FP64, PBGPU_MIXED = 0, 1
@@ -141,6 +142,7 @@ PBGPU_FUNCS = {
     "pbgpu_get_phi": (C.c_int, [ctx_p, P(dbl)]),
     "pbgpu_get_stage_ms": (C.c_int, [ctx_p, P(dbl)]),
     "pbgpu_set_profiling": (C.c_int, [ctx_p, C.c_int]),
+    "pbgpu_set_wait_limit": (C.c_int, [ctx_p, dbl]),
     "pbgpu_get_counters": (C.c_int, [ctx_p, P(PbgpuCounters)]),
     "pbgpu_reset_counters": (C.c_int, [ctx_p]),
     "pbgpu_coulomb_energy_static": (C.c_int, [C.c_void_p, i64, dbl, dbl, C.c_void_p, C.c_void_p]),
@@ -162,6 +164,7 @@ PBGPU_FUNCS = {
     "pbgpu_batch_step": (C.c_int, [C.c_void_p, C.c_int, P(C.c_int)]),
     "pbgpu_batch_member": (C.c_int, [C.c_void_p, C.c_int, P(C.c_int), P(PbgpuSolveStats)]),
     "pbgpu_batch_set_blocks_per_sm": (C.c_int, [C.c_void_p, C.c_int]),
+    "pbgpu_batch_set_wait_limit": (C.c_int, [C.c_void_p, dbl]),
     "pbgpu_batch_launch": (C.c_int, [C.c_void_p, C.c_int]),
     "pbgpu_batch_wait": (C.c_int, [C.c_void_p, P(C.c_int)]),
     "pbgpu_default_server_opts": (None, [P(PbgpuServerOpts)]),
@@ -171,6 +174,7 @@ PBGPU_FUNCS = {
     "pbgpu_server_submit": (C.c_int, [C.c_void_p, P(PbgpuRequest), P(i64)]),
     "pbgpu_server_progress": (C.c_int, [C.c_void_p, P(PbgpuResult), C.c_int, P(C.c_int)]),
     "pbgpu_server_pending": (C.c_int, [C.c_void_p, P(C.c_int), P(C.c_int), P(i64)]),
+    "pbgpu_server_stats": (C.c_int, [C.c_void_p, P(i64), P(i64), P(i64), P(i64)]),
     "pbgpu_request_bytes_estimate": (i64, [P(PbgpuRequest)]),
 }
 
@@ -186,6 +190,7 @@ PBHOST_FUNCS = {
     "pbhost_set_atoms": (C.c_int, [host_p, i64, P(dbl), P(dbl), P(dbl)]),
     "pbhost_build_problem": (C.c_int, [host_p]),
     "pbhost_build_on_gpu": (C.c_int, [host_p, C.c_void_p]),
+    "pbhost_initial_octree": (C.c_int, [host_p, C.c_int, P(PbgpuMeshBuild)]),
     "pbhost_write_vtu": (C.c_int, [host_p, C.c_char_p, C.c_char_p, P(dbl)]),
     "pbhost_get_info": (C.c_int, [host_p, P(PbhostInfo)]),
     "pbhost_get_mesh": (C.c_int, [host_p, P(PbgpuMesh)]),

@@ -116,7 +116,7 @@ def build_oracle(verbose=False):
     os.makedirs(out, exist_ok=True)
     so = os.path.join(out, "liboracle.so")
     src = os.path.join(ORACLE, "pb_oracle.cpp")
-    deps = [src, os.path.join(ORACLE, "pb_oracle.h"), os.path.join(CSRC, "mc_tables.h"),
+    deps = [src, os.path.join(ORACLE, "pb_oracle.h"), os.path.join(ORACLE, "mc_tri_table.h"),
             os.path.join(ROOT, "include", "pbgpu.h")]
     if _stale(so, deps):
         _run([CXX] + CXXFLAGS + ["-shared", src, "-o", so], verbose)

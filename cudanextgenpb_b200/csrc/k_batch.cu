@@ -94,10 +94,12 @@ struct CtaGroup {
 
 // Barrier over the `size` CTAs of one member's group.  The last CTA to arrive
 // runs `last` (the member's reduction and scalar update) before it releases
-// the others.  The wait is bounded (about 2 s of wall time), after which the
-// shared error flag is set; every caller then returns false.
+// the others.  The wait is bounded (wait_ns of wall time, 2 s unless the
+// batch's wait limit says otherwise), after which the shared error flag is
+// set; every caller then returns false.  A zero limit gives up at once without
+// polling (tests drive the timeout path with it).
 template <class F>
-__device__ __forceinline__ bool member_barrier(MemBar* b, int size, int* err, F&& last) {
+__device__ __forceinline__ bool member_barrier(MemBar* b, int size, int* err, uint64_t wait_ns, F&& last) {
   __shared__ int is_last;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -105,11 +107,13 @@ __device__ __forceinline__ bool member_barrier(MemBar* b, int size, int* err, F&
     const unsigned gen = *vgen;
     __threadfence();
     is_last = atomicAdd(&b->count, 1u) == (unsigned)size - 1u;
-    if (!is_last) {
+    if (!is_last && wait_ns == 0) {
+      atomicExch(err, 1);
+    } else if (!is_last) {
       const uint64_t t0 = global_ns();
       uint32_t it = 0;
       while (*vgen == gen) {
-        if ((++it & 255u) == 0 && global_ns() - t0 > 2000000000ull) {
+        if ((++it & 255u) == 0 && global_ns() - t0 > wait_ns) {
           atomicExch(err, 1);
           break;
         }
@@ -285,7 +289,7 @@ __device__ __forceinline__ void member_after_update(BState& S, const BMember<TI>
 template <typename TI>
 __global__ void __launch_bounds__(kBlock, kBatchMinBlocks)
     k_batch_cg(const BMember<TI>* __restrict__ mem, const CtaGroup* __restrict__ groups, BState* st, double* part,
-               MemBar* bars, int* err, int steps) {
+               MemBar* bars, int* err, int steps, unsigned long long wait_ns) {
   const CtaGroup G = groups[blockIdx.x];
   const BMember<TI>& M = mem[G.slot];
   BState& S = st[G.slot];
@@ -321,7 +325,7 @@ __global__ void __launch_bounds__(kBlock, kBatchMinBlocks)
         part[(M.rb0 + rb) * 2 + 1] = v[1];
       }
     }
-    if (!member_barrier(mb, G.size, err, [&] {
+    if (!member_barrier(mb, G.size, err, wait_ns, [&] {
           if (warp == 0) member_after_spmv<TI>(S, M, part);
         }))
       return;
@@ -352,7 +356,7 @@ __global__ void __launch_bounds__(kBlock, kBatchMinBlocks)
         part[(M.rb0 + rb) * 2 + 1] = v[1];
       }
     }
-    if (!member_barrier(mb, G.size, err, [&] {
+    if (!member_barrier(mb, G.size, err, wait_ns, [&] {
           if (warp == 0) member_after_update<TI>(S, M, part);
         }))
       return;
@@ -370,7 +374,7 @@ __global__ void __launch_bounds__(kBlock, kBatchMinBlocks)
           M.x[i] += (double)M.xi[i];
       }
     }
-    if (!member_barrier(mb, G.size, err, [] {})) return;
+    if (!member_barrier(mb, G.size, err, wait_ns, [] {})) return;
   }
 }
 
@@ -399,6 +403,7 @@ struct pbgpu_batch {
   bool own_stream = false;
   int sm_count = 148;
   int blocks_per_sm = 0;  // 0: as many as fit
+  double wait_s = 2.0;    // limit of each member barrier wait (pbgpu_batch_set_wait_limit)
   std::string err;
   std::vector<pbgpu_ctx*> slots;
   std::vector<char> pending;  // member needs its vectors and state set up
@@ -669,7 +674,8 @@ int batch_launch(pbgpu_batch* B, int steps) {
     MemBar* a_bars = B->bars.get();
     int* a_err = B->errf.get();
     int a_steps = steps;
-    void* args[] = {&a_mem, &a_groups, &a_st, &a_part, &a_bars, &a_err, &a_steps};
+    unsigned long long a_wait = (unsigned long long)(B->wait_s * 1e9);
+    void* args[] = {&a_mem, &a_groups, &a_st, &a_part, &a_bars, &a_err, &a_steps, &a_wait};
     BATCH_CUDA(B, cudaEventRecord(B->ev0, B->stream));
     BATCH_CUDA(B, cudaLaunchCooperativeKernel((const void*)k_batch_cg<TI>, dim3(grid), dim3(kBlock), args, 0,
                                               B->stream));
@@ -744,6 +750,10 @@ int check_opts(pbgpu_batch* b, const pbgpu_solver_opts& o) {
 }
 
 }  // namespace
+
+namespace pbgpu {
+int64_t batch_launch_count(const pbgpu_batch* b) { return b ? b->launches : 0; }
+}  // namespace pbgpu
 
 extern "C" {
 
@@ -844,6 +854,12 @@ int pbgpu_batch_size(const pbgpu_batch* b) {
 int pbgpu_batch_set_blocks_per_sm(pbgpu_batch* b, int blocks) {
   if (!b || blocks < 0) return PBGPU_ERR_ARG;
   b->blocks_per_sm = blocks;
+  return PBGPU_OK;
+}
+
+int pbgpu_batch_set_wait_limit(pbgpu_batch* b, double seconds) {
+  if (!b || !(seconds >= 0.0) || seconds > 60.0) return PBGPU_ERR_ARG;
+  b->wait_s = seconds;
   return PBGPU_OK;
 }
 

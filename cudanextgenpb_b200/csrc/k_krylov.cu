@@ -59,9 +59,11 @@ __host__ __device__ constexpr size_t tma_smem_bytes() {
 }
 
 // Calls fn(row, y) for every row of every slice of this warp; false when a
-// bounded wait gave up (the warp's outstanding copies are waited for first).
+// bounded wait (limit wait_ns) gave up (the warp's outstanding copies are then
+// waited for, with the default limit, before it returns).
 template <typename T, int NC, typename Fn>
-__device__ __forceinline__ bool spmv_tma_rows(const SellT<T>& A, const T* __restrict__ x, Fn&& fn) {
+__device__ __forceinline__ bool spmv_tma_rows(const SellT<T>& A, const T* __restrict__ x, Fn&& fn,
+                                              uint64_t wait_ns) {
   extern __shared__ __align__(128) unsigned char tma_smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int64_t nwarps = (int64_t)gridDim.x * kTmaWarps;
@@ -117,7 +119,7 @@ __device__ __forceinline__ bool spmv_tma_rows(const SellT<T>& A, const T* __rest
       issue(Pn, 0, Wn, b ^ 1);
     // every lane observes the phase itself (acquiring the copied bytes); the
     // vote keeps the warp together should any lane reach the limit
-    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bars[b], (phases >> b) & 1u))) {
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bars[b], (phases >> b) & 1u, wait_ns))) {
       // give up: let this warp's copies land before the block can exit
       mbar_wait_bounded(&bars[b], (phases >> b) & 1u);
       if (next) mbar_wait_bounded(&bars[b ^ 1], (phases >> (b ^ 1)) & 1u);
@@ -679,7 +681,7 @@ __global__ void __launch_bounds__(kBlock, tma_min_blocks(NC))
   if (!spmv_tma_rows<T, NC>(A, p, [&](int64_t i, T y) {
         q[i] = y;
         v[0] += (double)p[i] * (double)y;
-      }))
+      }, ks->wait_ns))
     tma_timeout(ks);
   if (grid_sum<1>(v, partials, &ks->ticket[1]) && threadIdx.x == 0 && !timed_out(ks)) {
     ks->pq = v[0];
@@ -700,7 +702,7 @@ __global__ void __launch_bounds__(kBlock, tma_min_blocks(NC))
   if (!spmv_tma_rows<T, NC>(A, ph, [&](int64_t i, T y) {
         v[i] = y;
         s[0] += (double)rh[i] * (double)y;
-      }))
+      }, ks->wait_ns))
     tma_timeout(ks);
   if (grid_sum<1>(s, partials, &ks->ticket[1]) && threadIdx.x == 0 && !timed_out(ks)) {
     ks->alpha = ks->rv / s[0];
@@ -721,7 +723,7 @@ __global__ void __launch_bounds__(kBlock, tma_min_blocks(NC))
         t[i] = y;
         a[0] += (double)y * (double)s[i];
         a[1] += (double)y * (double)y;
-      }))
+      }, ks->wait_ns))
     tma_timeout(ks);
   if (grid_sum<2>(a, partials, &ks->ticket[3]) && threadIdx.x == 0 && !timed_out(ks)) {
     ks->ts = a[0];
@@ -743,7 +745,7 @@ __global__ void __launch_bounds__(kBlock, tma_min_blocks(NC))
         a[1] += i < n ? b[i] * b[i] : 0.0;
         a[2] += fabs(ri);
         a[3] += i < n ? fabs(b[i]) : 0.0;
-      }))
+      }, ks->wait_ns))
     tma_timeout(ks);
   if (grid_sum<4>(a, partials, &ks->ticket[5]) && threadIdx.x == 0) {
     ks->rr = a[0];
@@ -828,9 +830,9 @@ __global__ void k_cgs_q(int64_t n, const T* __restrict__ u, T* __restrict__ v, T
 
 // The rows of y = A x for this kernel: staged (NC > 0) or direct.
 template <typename T, int G, int NC, typename Fn>
-__device__ __forceinline__ bool spmv_rows(const SellT<T>& A, const T* __restrict__ x, Fn&& fn) {
+__device__ __forceinline__ bool spmv_rows(const SellT<T>& A, const T* __restrict__ x, Fn&& fn, uint64_t wait_ns) {
   if constexpr (NC > 0) {
-    return spmv_tma_rows<T, NC>(A, x, fn);
+    return spmv_tma_rows<T, NC>(A, x, fn, wait_ns);
   } else {
     spmv_direct_rows<T, G>(A, x, fn);
     return true;
@@ -847,7 +849,7 @@ __global__ void __launch_bounds__(kBlock, NC > 0 ? tma_min_blocks(NC) : spmv_min
   if (!spmv_rows<T, G, NC>(A, ph, [&](int64_t i, T y) {
         v[i] = y;
         a[0] += (double)rh[i] * (double)y;
-      }))
+      }, ks->wait_ns))
     tma_timeout(ks);
   if (grid_sum<1>(a, partials, &ks->ticket[1]) && threadIdx.x == 0 && !timed_out(ks)) {
     ks->alpha = ks->rv / a[0];
@@ -873,7 +875,7 @@ __global__ void __launch_bounds__(kBlock, NC > 0 ? tma_min_blocks(NC) : kSpmvMin
         a[0] += (double)ri * (double)ri;
         a[1] += (double)rh[i] * (double)ri;
         a[2] += fabs((double)ri);
-      }))
+      }, ks->wait_ns))
     tma_timeout(ks);
   if (grid_sum<3>(a, partials, &ks->ticket[3]) && threadIdx.x == 0 && !timed_out(ks)) {
     ks->iter += 1;
@@ -929,6 +931,23 @@ static int grid_blocks(const Context* c, int64_t n) {
   return (int)(g < 1 ? 1 : g);
 }
 
+// Blocks of a grid-stride kernel that fill the GPU in exactly one wave: its
+// resident blocks per SM (kBlock threads, no dynamic shared memory) times the
+// SMs, or fewer when the rows need fewer.  The SpMV kernels hold 5 or 6
+// blocks per SM; a grid of 8 per SM would leave a second wave of blocks
+// running on a partly occupied GPU after the first finished (every block of a
+// grid-stride loop has the same number of rows).
+static int wave_grid(const Context* c, const void* kernel, int64_t rows) {
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kBlock, 0) != cudaSuccess || occ <= 0) {
+    cudaGetLastError();
+    return grid_blocks(c, rows);
+  }
+  const int64_t need = (rows + kBlock - 1) / kBlock;
+  const int64_t g = std::min<int64_t>(need, (int64_t)c->sm_count * occ);
+  return (int)(g < 1 ? 1 : g);
+}
+
 // Chunk width (columns per bulk copy) of the staged SpMV for this context:
 // 0 when the staged path does not apply (layouts other than C = 32, G = 1) or
 // is switched off with PBGPU_SPMV=direct; PBGPU_SPMV_COLS=8|12|16 overrides
@@ -940,6 +959,13 @@ static int staged_cols(const Context* c, int C, int G) {
   int nc = c->spmv_cols;
   if (const char* e2 = std::getenv("PBGPU_SPMV_COLS")) nc = std::atoi(e2);
   return (nc == 8 || nc == 12 || nc == 16) ? nc : 16;
+}
+
+// PBGPU_SPMV_PAIRS=1 walks the G = 4 layout two column groups per iteration
+// (sell_row<T, 8>).
+static bool spmv_pairs() {
+  const char* e = std::getenv("PBGPU_SPMV_PAIRS");
+  return e && e[0] == '1';
 }
 
 // Grid of the staged SpMV kernels for storage type T and chunk width NC:
@@ -993,11 +1019,18 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
                     int* iters, int* status) {
   const int64_t n = K.A.n_pad;
   const int G = grid_blocks(c, n);
+  // one-wave grids of the kernels that multiply by the matrix
+  const int Gs = wave_grid(c, method == PBGPU_CG    ? (const void*)k_cg_spmv<T, GW>
+                              : method == PBGPU_CGS ? (const void*)k_cgs_v<T, GW, 0>
+                                                    : (const void*)k_bicg_v<T, GW>, n);
+  const int Gw = wave_grid(c, method == PBGPU_CGS ? (const void*)k_cgs_r<T, GW, 0> : (const void*)k_bicg_t<T, GW>, n);
   KrylovScalars* ks = c->ks.get();
   double* part = c->partials.get();
   PBGPU_CUDA(c, cudaMemsetAsync(ks, 0, sizeof(KrylovScalars), c->stream));
   int mi = max_iter;
   PBGPU_CUDA(c, cudaMemcpyAsync(&ks->max_iter, &mi, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  unsigned long long wns = (unsigned long long)(c->wait_s * 1e9);
+  PBGPU_CUDA(c, cudaMemcpyAsync(&ks->wait_ns, &wns, sizeof(wns), cudaMemcpyHostToDevice, c->stream));
   if (K.x64 && method == PBGPU_CG) {
     static const int on = 1;
     static const double delta2 = 0.01;  // an FP64 residual every 10x reduction of the FP32 one
@@ -1059,16 +1092,16 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
       if (tg)
         k_cg_spmv_tma<T, (NC > 0 ? NC : 16)><<<tg, kBlock, smem, c->stream>>>(K.A, K.p, K.q, ks, part);
       else
-        k_cg_spmv<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.p, K.q, ks, part);
+        k_cg_spmv<T, GW><<<Gs, kBlock, 0, c->stream>>>(K.A, K.p, K.q, ks, part);
       mark(k, 0, 1);
       k_cg_update<T><<<G, kBlock, 0, c->stream>>>(n, K.x, K.r, K.p, K.q, K.dinv, ks, part);
       if constexpr (std::is_same<T, float>::value) {
         if (K.x64) {
           k_ru_apply<<<G, kBlock, 0, c->stream>>>(n, K.x64, K.x, ks);
           switch (K.A64->G) {
-            case 1: k_ru_residual<1><<<G, kBlock, 0, c->stream>>>(*K.A64, K.n_rows, K.b64, K.x64, K.r, K.dinv, ks, part); break;
-            case 2: k_ru_residual<2><<<G, kBlock, 0, c->stream>>>(*K.A64, K.n_rows, K.b64, K.x64, K.r, K.dinv, ks, part); break;
-            default: k_ru_residual<4><<<G, kBlock, 0, c->stream>>>(*K.A64, K.n_rows, K.b64, K.x64, K.r, K.dinv, ks, part); break;
+            case 1: k_ru_residual<1><<<wave_grid(c, (const void*)k_ru_residual<1>, K.A64->n_pad), kBlock, 0, c->stream>>>(*K.A64, K.n_rows, K.b64, K.x64, K.r, K.dinv, ks, part); break;
+            case 2: k_ru_residual<2><<<wave_grid(c, (const void*)k_ru_residual<2>, K.A64->n_pad), kBlock, 0, c->stream>>>(*K.A64, K.n_rows, K.b64, K.x64, K.r, K.dinv, ks, part); break;
+            default: k_ru_residual<4><<<wave_grid(c, (const void*)k_ru_residual<4>, K.A64->n_pad), kBlock, 0, c->stream>>>(*K.A64, K.n_rows, K.b64, K.x64, K.r, K.dinv, ks, part); break;
           }
         }
       }
@@ -1081,7 +1114,7 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
       if (tg)
         k_cgs_v<T, 1, (NC > 0 ? NC : 16)><<<tg, kBlock, smem, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
       else
-        k_cgs_v<T, GW, 0><<<G, kBlock, 0, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
+        k_cgs_v<T, GW, 0><<<Gs, kBlock, 0, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
       mark(k, 0, 1);
       k_cgs_q<T><<<G, kBlock, 0, c->stream>>>(n, K.s, K.v, K.q, K.sh, K.dinv, ks);
       if (bj) bj_apply(K.v, K.sh, false);
@@ -1089,7 +1122,7 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
       if (tg)
         k_cgs_r<T, 1, (NC > 0 ? NC : 16)><<<tg, kBlock, smem, c->stream>>>(K.A, K.sh, K.x, K.r, K.rh, ks, part);
       else
-        k_cgs_r<T, GW, 0><<<G, kBlock, 0, c->stream>>>(K.A, K.sh, K.x, K.r, K.rh, ks, part);
+        k_cgs_r<T, GW, 0><<<Gw, kBlock, 0, c->stream>>>(K.A, K.sh, K.x, K.r, K.rh, ks, part);
       mark(k, 1, 1);
     } else {
       k_bicg_p<T><<<G, kBlock, 0, c->stream>>>(n, K.p, K.ph, K.r, K.v, K.dinv, ks);
@@ -1098,7 +1131,7 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
       if (tg)
         k_bicg_v_tma<T, (NC > 0 ? NC : 16)><<<tg, kBlock, smem, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
       else
-        k_bicg_v<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
+        k_bicg_v<T, GW><<<Gs, kBlock, 0, c->stream>>>(K.A, K.ph, K.v, K.rh, ks, part);
       mark(k, 0, 1);
       k_bicg_s<T><<<G, kBlock, 0, c->stream>>>(n, K.r, K.v, K.s, K.sh, K.dinv, ks, part);
       if (bj) bj_apply(K.s, K.sh, false);
@@ -1106,7 +1139,7 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
       if (tg)
         k_bicg_t_tma<T, (NC > 0 ? NC : 16)><<<tg, kBlock, smem, c->stream>>>(K.A, K.sh, K.t, K.s, ks, part);
       else
-        k_bicg_t<T, GW><<<G, kBlock, 0, c->stream>>>(K.A, K.sh, K.t, K.s, ks, part);
+        k_bicg_t<T, GW><<<Gw, kBlock, 0, c->stream>>>(K.A, K.sh, K.t, K.s, ks, part);
       mark(k, 1, 1);
       k_bicg_x<T><<<G, kBlock, 0, c->stream>>>(n, K.x, K.r, K.ph, K.sh, K.s, K.t, K.rh, ks, part);
     }
@@ -1186,13 +1219,17 @@ static int krylov(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr, i
   switch (K.A.G) {
     case 1: return krylov_g<T, 1, 0>(c, method, K, cr, max_iter, check_every, iters, status);
     case 2: return krylov_g<T, 2, 0>(c, method, K, cr, max_iter, check_every, iters, status);
-    default: return krylov_g<T, 4, 0>(c, method, K, cr, max_iter, check_every, iters, status);
+    default:
+      if (spmv_pairs())  // the G = 4 layout walked two groups per iteration
+        return krylov_g<T, 8, 0>(c, method, K, cr, max_iter, check_every, iters, status);
+      return krylov_g<T, 4, 0>(c, method, K, cr, max_iter, check_every, iters, status);
   }
 }
 
 // r = b - A x (fp64); optional fp64 / fp32 copies of r; norms into ks
 static void launch_residual(Context* c, const SellT<double>& A, int64_t n, double* r, float* r32) {
-  const int g = grid_blocks(c, A.n_pad);
+  const int g = wave_grid(c, A.G == 1 ? (const void*)k_residual<1> : A.G == 2 ? (const void*)k_residual<2>
+                                                                      : (const void*)k_residual<4>, A.n_pad);
   auto staged = [&](auto nc_tag) -> bool {
     constexpr int NC = decltype(nc_tag)::value;
     const int tg = tma_grid<double, NC>(c);
@@ -1269,6 +1306,14 @@ int run_solve(Context* c, const pbgpu_solver_opts* o, pbgpu_solve_stats* st) {
   const bool mixed = opt.precision == PBGPU_MIXED;
   const int64_t n = c->n, n_pad = c->n_slices * c->C;
   PBGPU_CUDA(c, alloc_vectors(c, n_pad, mixed));
+  // the scalars start from zero (tickets included) before any kernel of this
+  // solve reads them: the mixed path's first residual runs before the first
+  // Krylov run clears them itself
+  PBGPU_CUDA(c, cudaMemsetAsync(c->ks.get(), 0, sizeof(KrylovScalars), c->stream));
+  {
+    const unsigned long long wns = (unsigned long long)(c->wait_s * 1e9);
+    PBGPU_CUDA(c, cudaMemcpyAsync(&c->ks.get()->wait_ns, &wns, sizeof(wns), cudaMemcpyHostToDevice, c->stream));
+  }
   PBGPU_CUDA(c, cudaEventRecord(c->ev0, c->stream));
   int iters = 0, status = PBGPU_OK, outer = 0;
   SellT<double> A64{c->slice_ptr.get(), c->slice_w.get(), c->scol.get(), c->sval.get(), n_pad, c->C, c->G};

@@ -3,8 +3,9 @@
 // hanging nodes that p8est_nodes / tmesh_3d provide, and the ray crossing
 // tables of the three axes (NanoShaper's ray cache, src/raytracer.cpp:379-467;
 // here the analytic van der Waals union of spheres).  Starts from the initial
-// octree of init_tmesh* (small; built on the host) and leaves the context as
-// pbgpu_set_mesh + pbgpu_set_rays would, with no host round trip of the mesh.
+// octree of init_tmesh* (given by the host, or built here: a uniform octree
+// refined inside a box) and leaves the context as pbgpu_set_mesh +
+// pbgpu_set_rays would, with no host round trip of the mesh.
 //
 // Every step restates the host build (host/octree.cpp, host/surface.cpp,
 // host/pb_class.cpp) with the same expressions, so the GPU and host meshes are
@@ -359,6 +360,45 @@ __global__ void k_surface_marks(Tree t, const uint8_t* __restrict__ hm, const ui
     marks[i] = (mxv > 0.5 && mn < 0.5) && q.w < kQMaxLevel;
   else
     marks[i] = mn > 0.5 || mxv < 0.5;
+}
+
+// ---------------------------------------------------------------------------
+// The initial octree of init_tmesh* (src/pb_class.cpp:1290-1391): a uniform
+// octree, then box refinement (host Octree::uniform and refine_in_box).
+
+// leaf i of the uniform octree at `level`, in Morton order
+__global__ void k_uniform(int level, int64_t n, int4* __restrict__ leaves) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t x = 0, y = 0, z = 0;
+  for (int b = 0; b < level; ++b) {
+    x |= (uint32_t)((i >> (3 * b)) & 1) << b;
+    y |= (uint32_t)((i >> (3 * b + 1)) & 1) << b;
+    z |= (uint32_t)((i >> (3 * b + 2)) & 1) << b;
+  }
+  const int32_t s = qsize(level);
+  leaves[i] = make_int4((int32_t)x * s, (int32_t)y * s, (int32_t)z * s, level);
+}
+
+// refine marks of one box-refinement pass: leaves below `level` with a
+// non-hanging corner inside the closed box [bl, br]
+__global__ void k_box_marks(Tree t, const uint8_t* __restrict__ hm, RayDom D, double3 bl, double3 br, int level,
+                            uint8_t* __restrict__ marks) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= t.n) return;
+  const int4 q = t.leaves[i];
+  uint8_t m = 0;
+  if (q.w < level) {
+    const int32_t s = qsize(q.w);
+    for (int c = 0; c < 8 && !m; ++c) {
+      if (hm[i] >> c & 1) continue;
+      const double x = coord(D.lo[0], D.len[0], q.x + (c & 1) * s);
+      const double y = coord(D.lo[1], D.len[1], q.y + ((c >> 1) & 1) * s);
+      const double z = coord(D.lo[2], D.len[2], q.z + ((c >> 2) & 1) * s);
+      m = x >= bl.x && x <= br.x && y >= bl.y && y <= br.y && z >= bl.z && z <= br.z;
+    }
+  }
+  marks[i] = m;
 }
 
 // ---------------------------------------------------------------------------
@@ -959,6 +999,36 @@ struct Builder {
     return PBGPU_OK;
   }
 
+  // uniform octree at `level`
+  int uniform(int level) {
+    if (level < 0 || level > 8) return c->fail(PBGPU_ERR_ARG, "build_mesh: uniform level must be 0..8");
+    n = int64_t(1) << (3 * level);
+    PBGPU_CUDA(c, leaves.alloc(n));
+    k_uniform<<<grid_for(n, 256), 256, 0, st()>>>(level, n, leaves.get());
+    PBGPU_LAUNCHED(c);
+    return rekey();
+  }
+
+  // refine_in_box: up to `level` passes, each splitting the leaves below
+  // `level` with a non-hanging corner in the box and restoring 2:1 balance; a
+  // pass that marks nothing ends it (every later pass would mark nothing too)
+  int box_refine(const double bl[3], const double br[3], int level) {
+    int rc;
+    for (int it = 0; it < level; ++it) {
+      if ((rc = hanging()) != PBGPU_OK) return rc;
+      PBGPU_CUDA(c, marks.alloc((n + 3) & ~int64_t(3)));
+      k_box_marks<<<grid_for(n, 128), 128, 0, st()>>>(tree(), hm.get(), D, make_double3(bl[0], bl[1], bl[2]),
+                                                      make_double3(br[0], br[1], br[2]), level, marks.get());
+      PBGPU_LAUNCHED(c);
+      DBuf<int4> parents, none;
+      int64_t np = 0;
+      if ((rc = split(parents, &np)) != PBGPU_OK) return rc;
+      if (np == 0) break;
+      if ((rc = balance(parents, np, none, 0, false)) != PBGPU_OK) return rc;
+    }
+    return PBGPU_OK;
+  }
+
   int refine_step(int maxlevel) {
     int rc;
     if ((rc = surface_marks(0, 0, maxlevel)) != PBGPU_OK) return rc;
@@ -1018,9 +1088,11 @@ using namespace pbgpu;
 extern "C" int pbgpu_build_mesh(pbgpu_ctx* h, const pbgpu_mesh_build* in) {
   if (!h) return PBGPU_ERR_ARG;
   Context* c = &h->c;
-  if (!in || in->n_oct <= 0 || !in->oct_xyz || !in->oct_level || in->n_spheres < 0 ||
+  if (!in || in->n_oct < 0 || (in->n_oct > 0 && (!in->oct_xyz || !in->oct_level)) || in->n_spheres < 0 ||
       (in->n_spheres > 0 && !in->spheres))
-    return c->fail(PBGPU_ERR_ARG, "build_mesh: empty initial octree or null arrays");
+    return c->fail(PBGPU_ERR_ARG, "build_mesh: bad initial octree or null arrays");
+  if (in->n_oct == 0 && (in->init_level < 0 || in->init_level > 8 || in->box_level < 0 || in->box_level > kQMaxLevel))
+    return c->fail(PBGPU_ERR_ARG, "build_mesh: init_level must be 0..8 and box_level 0..18");
   for (int a = 0; a < 3; ++a)
     if (!(in->hi[a] > in->lo[a])) return c->fail(PBGPU_ERR_ARG, "build_mesh: empty domain box");
   AcctScope acct(&c->dev_bytes);
@@ -1061,18 +1133,21 @@ extern "C" int pbgpu_build_mesh(pbgpu_ctx* h, const pbgpu_mesh_build* in) {
                                     cudaMemcpyHostToDevice, c->stream));
     B.S.bins[a] = SphereBins{bins[a].o0, bins[a].o1, cell, bins[a].n0, bins[a].n1, B.bstart[a].get(), B.bitems[a].get()};
   }
-  // the initial octree
-  B.n = in->n_oct;
-  {
+  // the initial octree: the caller's, or built here (init_tmesh*)
+  int rc;
+  if (in->n_oct > 0) {
+    B.n = in->n_oct;
     std::vector<int4> q(B.n);
     for (int64_t i = 0; i < B.n; ++i)
       q[i] = make_int4(in->oct_xyz[3 * i], in->oct_xyz[3 * i + 1], in->oct_xyz[3 * i + 2], in->oct_level[i]);
     PBGPU_CUDA(c, B.leaves.alloc(B.n));
     PBGPU_CUDA(c, cudaMemcpyAsync(B.leaves.get(), q.data(), B.n * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
     PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    if ((rc = B.rekey()) != PBGPU_OK) return rc;
+  } else {
+    if ((rc = B.uniform(in->init_level)) != PBGPU_OK) return rc;
+    if (in->box_level > 0 && (rc = B.box_refine(in->box_lo, in->box_hi, in->box_level)) != PBGPU_OK) return rc;
   }
-  int rc;
-  if ((rc = B.rekey()) != PBGPU_OK) return rc;
   // refine_surface: refinement / coarsening cycles
   if (in->refine) {
     const int cycles = std::max(in->maxlevel - in->unilevel, in->unilevel - in->minlevel);

@@ -38,7 +38,11 @@ static __device__ __align__(256) double g_partials[kStaticBlocks];
 static __device__ __align__(256) unsigned int g_ticket;
 
 // Device addresses of the arrays, looked up once per device with that device
-// current (in host code the symbols are only host-side stand-ins).
+// current (in host code the symbols are only host-side stand-ins).  They are
+// addresses in the device's primary context, the one the CUDA runtime uses;
+// the cache is never invalidated, so after cudaDeviceReset (which unloads the
+// module) or from another context the cached addresses would be stale: the
+// entry point is for processes that keep the primary context for their life.
 struct StaticScratch {
   double4* atoms = nullptr;
   double* partials = nullptr;
@@ -83,6 +87,10 @@ __global__ void __launch_bounds__(kStaticThreads) k_static_coulomb(const double4
       __syncthreads();
       if (a0 + threadIdx.x < m) tile[threadIdx.x] = atoms[a0 + threadIdx.x];
       __syncthreads();
+      // an uncharged row adds nothing: it skips its pairs (a zero charge on
+      // top of a charged atom would otherwise give 0 * inf), but still takes
+      // part in every tile load and barrier of the block
+      if (P.w == 0.0) continue;
       const int lim = (int)min((int64_t)kStaticThreads, m - a0);
       for (int j = 0; j < lim; ++j) {
         if (a0 + j <= i) continue;
@@ -92,7 +100,7 @@ __global__ void __launch_bounds__(kStaticThreads) k_static_coulomb(const double4
         s += A.w * rsqrt_nr_static(dx * dx + dy * dy + dz * dz);
       }
     }
-    if (i < m) acc += P.w * s;
+    if (i < m && P.w != 0.0) acc += P.w * s;
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
@@ -149,13 +157,12 @@ extern "C" int pbgpu_coulomb_energy_static(const double* atoms, int64_t n_atoms,
   // eps_in in the reference's units (src/pb_class.cpp:1800)
   const double e_0 = 8.85418781762e-12, kb = 1.380649e-23, e = 1.602176634e-19, Angs = 1e-10;
   const double eps_in = 4.0 * kPi * e_0 * e_in * kb * T * Angs / (e * e);
-  if (cudaMemsetAsync(S.ticket, 0, sizeof(unsigned int), stream) != cudaSuccess) return PBGPU_ERR_CUDA;
   if (n_atoms < 2) {
-    const double zero = 0.0;
-    if (cudaMemcpyAsync(out_energy, &zero, sizeof(double), cudaMemcpyHostToDevice, stream) != cudaSuccess)
-      return PBGPU_ERR_CUDA;
-    return cudaStreamSynchronize(stream) == cudaSuccess ? PBGPU_OK : PBGPU_ERR_CUDA;
+    // no pair: the energy is zero, written on the stream like any other result
+    // (all-zero bytes are +0.0); nothing here waits for the stream
+    return cudaMemsetAsync(out_energy, 0, sizeof(double), stream) == cudaSuccess ? PBGPU_OK : PBGPU_ERR_CUDA;
   }
+  if (cudaMemsetAsync(S.ticket, 0, sizeof(unsigned int), stream) != cudaSuccess) return PBGPU_ERR_CUDA;
   k_static_copy<<<kStaticBlocks, kStaticThreads, 0, stream>>>(atoms, n_atoms, S.atoms);
   int64_t blocks = (n_atoms + kStaticThreads - 1) / kStaticThreads;
   if (blocks > kStaticBlocks) blocks = kStaticBlocks;

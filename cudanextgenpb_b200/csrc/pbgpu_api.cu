@@ -634,6 +634,13 @@ int pbgpu_set_profiling(pbgpu_ctx* h, int on) {
   return PBGPU_OK;
 }
 
+int pbgpu_set_wait_limit(pbgpu_ctx* h, double seconds) {
+  CTX_CHECK(h);
+  if (!(seconds >= 0.0) || seconds > 60.0) return h->c.fail(PBGPU_ERR_ARG, "set_wait_limit: seconds must be in [0, 60]");
+  h->c.wait_s = seconds;
+  return PBGPU_OK;
+}
+
 int pbgpu_get_counters(pbgpu_ctx* h, pbgpu_counters* out) {
   CTX_CHECK(h);
   if (!out) return PBGPU_ERR_ARG;

@@ -163,6 +163,7 @@ struct KrylovScalars {
   double rr_ref, delta2;  // ||r||^2 at the last FP64 residual; update when rr < delta2 rr_ref
   int iter, max_iter, done, status, s_conv;
   unsigned int ticket[8]; // last-block tickets, one per reducing kernel
+  unsigned long long wait_ns;  // limit of each bounded wait of the staged SpMV (0: give up at once)
 };
 
 // Element j of the SELL row in lane `lane` of a slice that starts at element
@@ -293,6 +294,7 @@ struct Context {
   DBuf<double> phi;          // node order
   bool have_phi = false;
   int sm_count = 148;
+  double wait_s = 1.0;       // limit of each bounded device-side wait (pbgpu_set_wait_limit)
 
   // ---- energy scratch
   DBuf<double4> elem_a;      // element position + coefficient
@@ -486,6 +488,11 @@ int export_system(Context* c, int64_t* nnz, int64_t* row_ptr, int32_t* col, doub
 
 // scratch for CUB temporaries
 cudaError_t ensure_tmp(Context* c, size_t bytes);
+}  // namespace pbgpu
+struct pbgpu_batch;
+namespace pbgpu {
+// persistent kernels a batch has launched (k_batch.cu)
+int64_t batch_launch_count(const pbgpu_batch* b);
 // Morton keys of the octants' lower corners
 void launch_oct_keys(const int4* oct, int64_t n_oct, uint64_t* key, cudaStream_t s);
 

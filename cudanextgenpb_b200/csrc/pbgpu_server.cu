@@ -90,19 +90,25 @@ struct pbgpu_server {
   int64_t next_id = 1;
   bool in_session = false;
   std::string err;
-  int64_t admitted = 0, completed = 0;
+  int64_t admitted = 0, completed = 0, rejected = 0;
+  int64_t retired_launches = 0;  // kernels of contexts the server has destroyed
   int fail(int code, const std::string& m) {
     err = m;
     return code;
   }
 };
 
-// Inputs, markers, density map and SELL system of one request on `ctx`.
+// Inputs (the mesh set or built), markers, density map and SELL system of one
+// request on `ctx`.
 static int setup_request(pbgpu_server* s, pbgpu_ctx* ctx, const pbgpu_request& r) {
   int st;
-  if ((st = pbgpu_set_mesh(ctx, r.mesh)) != PBGPU_OK) return st;
-  for (int a = 0; a < 3; ++a)
-    if ((st = pbgpu_set_rays(ctx, a, &r.rays[a])) != PBGPU_OK) return st;
+  if (r.mesh) {
+    if ((st = pbgpu_set_mesh(ctx, r.mesh)) != PBGPU_OK) return st;
+    for (int a = 0; a < 3; ++a)
+      if ((st = pbgpu_set_rays(ctx, a, &r.rays[a])) != PBGPU_OK) return st;
+  } else if ((st = pbgpu_build_mesh(ctx, r.build)) != PBGPU_OK) {
+    return st;
+  }
   if ((st = pbgpu_set_atoms(ctx, r.n_atoms, r.pos, r.charge)) != PBGPU_OK) return st;
   if ((st = pbgpu_set_model(ctx, r.model)) != PBGPU_OK) return st;
   if ((st = pbgpu_create_markers(ctx)) != PBGPU_OK) return st;
@@ -144,10 +150,36 @@ static void worker_loop(pbgpu_server* s, int w) {
   }
 }
 
+// The result of a request that can never fit the budget.
+static pbgpu_result rejection(const Pending& p) {
+  pbgpu_result o;
+  std::memset(&o, 0, sizeof(o));
+  o.id = p.id;
+  o.user_tag = p.req.user_tag;
+  o.status = PBGPU_REJECTED;
+  o.latency_ms = ms_since(p.t_submit);
+  o.queue_ms = o.latency_ms;
+  return o;
+}
+
 extern "C" {
 
 int64_t pbgpu_request_bytes_estimate(const pbgpu_request* r) {
-  if (!r || !r->mesh) return 0;
+  if (!r || (!r->mesh && !r->build)) return 0;
+  if (!r->mesh) {
+    // Mesh still to build: every refinement level above the initial octree
+    // splits surface octants into 8; measured, each surface level multiplies
+    // the octant count by at most ~3.5 (the refined shell is thin), and nodes
+    // and hanging nodes stay below 0.8 and 0.7 per octant.  Bound the final
+    // octants by 4x per level.
+    const pbgpu_mesh_build* b = r->build;
+    int top = 0;
+    for (int64_t i = 0; i < b->n_oct; ++i) top = std::max(top, (int)b->oct_level[i]);
+    const int levels = b->refine ? std::max(0, b->maxlevel - top) : 0;
+    double no = (double)b->n_oct;
+    for (int l = 0; l < levels; ++l) no *= 4.0;
+    return (int64_t)(870.0 * no + 1000.0 * (double)b->n_spheres) + ((int64_t)64 << 20);
+  }
   const double no = (double)r->mesh->n_oct, n = (double)r->mesh->n_nodes, nh = (double)r->mesh->n_hang;
   // mesh, incidence lists, per-octant local coefficients (assembly scratch),
   // SELL matrix (~11 nonzeros per row, 12 B each), Krylov vectors (FP64 and
@@ -239,11 +271,31 @@ void pbgpu_server_destroy(pbgpu_server* s) {
 const char* pbgpu_server_last_error(const pbgpu_server* s) { return s ? s->err.c_str() : "null server"; }
 
 int pbgpu_server_submit(pbgpu_server* s, const pbgpu_request* req, int64_t* id) {
-  if (!s || !req || !req->mesh || !req->model || req->n_atoms < 0 || (req->n_atoms > 0 && (!req->pos || !req->charge)))
+  if (!s || !req || (!req->mesh && !req->build) || !req->model || req->n_atoms < 0 ||
+      (req->n_atoms > 0 && (!req->pos || !req->charge)))
     return PBGPU_ERR_ARG;
   Pending p{s->next_id++, *req, Clock::now()};
   s->queue.push_back(p);
   if (id) *id = p.id;
+  return PBGPU_OK;
+}
+
+int pbgpu_server_stats(const pbgpu_server* sc, int64_t* admitted, int64_t* completed, int64_t* rejected,
+                       int64_t* launches) {
+  if (!sc) return PBGPU_ERR_ARG;
+  pbgpu_server* s = const_cast<pbgpu_server*>(sc);
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (admitted) *admitted = s->admitted;
+  if (completed) *completed = s->completed;
+  if (rejected) *rejected = s->rejected;
+  if (launches) {
+    int64_t l = s->retired_launches + (s->batch ? pbgpu::batch_launch_count(s->batch) : 0);
+    for (pbgpu_ctx* c : s->worker_ctx) l += c->c.launches;
+    for (const Running& r : s->running) l += r.ctx->c.launches;
+    for (const Retire& x : s->finishing) l += x.r.ctx->c.launches;
+    for (pbgpu_ctx* c : s->idle) l += c->c.launches;
+    *launches = l;
+  }
   return PBGPU_OK;
 }
 
@@ -295,6 +347,13 @@ static int progress_concurrent(pbgpu_server* s, pbgpu_result* out, int cap, int*
   }
   while (!s->queue.empty() && s->in_flight < nw) {
     const int64_t need = pbgpu_request_bytes_estimate(&s->queue.front().req);
+    if ((double)need > s->opts.hbm_budget_bytes) {
+      // alone it already exceeds the budget: reject instead of admitting
+      s->finished.push_back(rejection(s->queue.front()));
+      s->queue.pop_front();
+      ++s->rejected;
+      continue;
+    }
     // a worker may grow to this request's size: at worst all of them do
     if (held - largest + (int64_t)nw * std::max(largest, need) > (int64_t)s->opts.hbm_budget_bytes &&
         s->in_flight > 0)
@@ -347,6 +406,15 @@ int pbgpu_server_progress(pbgpu_server* s, pbgpu_result* out, int cap, int* n_ou
   while (!s->queue.empty() && (int)adm.size() < max_new) {
     const Pending& p = s->queue.front();
     const int64_t need = pbgpu_request_bytes_estimate(&p.req);
+    if ((double)need > s->opts.hbm_budget_bytes) {
+      // alone it already exceeds the budget: reject instead of admitting (it
+      // waits in the queue for the next tick if the output array is full)
+      if (*n_out >= cap) break;
+      out[(*n_out)++] = rejection(p);
+      s->queue.pop_front();
+      ++s->rejected;
+      continue;
+    }
     // the idle context whose buffers are closest above the need, else the largest
     int pick = -1;
     for (size_t k = 0; k < s->idle.size(); ++k) {
@@ -369,6 +437,7 @@ int pbgpu_server_progress(pbgpu_server* s, pbgpu_result* out, int cap, int* n_ou
       if (big < 0) break;
       after -= ctx_bytes(s->idle[big]);
       held -= ctx_bytes(s->idle[big]);
+      s->retired_launches += s->idle[big]->c.launches;
       pbgpu_ctx_destroy(s->idle[big]);
       s->idle.erase(s->idle.begin() + big);
       if (pick > big) --pick;
@@ -388,7 +457,7 @@ int pbgpu_server_progress(pbgpu_server* s, pbgpu_result* out, int cap, int* n_ou
   }
   //    and the members that converged last tick compute their energies (as
   //    many as the output array holds), also one host thread each
-  const size_t n_fin = std::min(s->finishing.size(), (size_t)std::max(cap, 0));
+  const size_t n_fin = std::min(s->finishing.size(), (size_t)std::max(cap - *n_out, 0));
   auto energy_of = [s](Retire& x) {
     if (x.st == PBGPU_OK) x.st = pbgpu_energy(x.r.ctx, s->opts.energy_fast, &x.energy);
   };

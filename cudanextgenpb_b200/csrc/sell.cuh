@@ -16,10 +16,13 @@ constexpr int kBlock = 256;
 constexpr int kSpmvMinBlocks = 5;
 constexpr int kSpmvMinBlocksWide = 4;
 // the G = 4 row product (one group per iteration, no unrolling) fits in 40
-// registers: 6 blocks, 48 warps per SM, to keep more gathers in flight
+// registers: 6 blocks, 48 warps per SM, to keep more gathers in flight.
+// G = 8 names the same G = 4 layout walked two groups per iteration (all
+// index and value loads of both groups issued before the first gather): half
+// the dependent load round trips per 8-wide row, at 64 registers (4 blocks)
 template <int G>
 __host__ __device__ constexpr int spmv_min_blocks() {
-  return G == 4 ? 6 : kSpmvMinBlocks;
+  return G == 4 ? 6 : G == 8 ? 4 : kSpmvMinBlocks;
 }
 
 template <typename T>
@@ -73,6 +76,65 @@ __device__ __forceinline__ T sell_row(const SellT<T>& A, int lane, const T* __re
       const typename V2<T>::t v = __ldcs(reinterpret_cast<const typename V2<T>::t*>(A.sval + k));
       acc += v.x * x[c.x];
       acc += v.y * x[c.y];
+    }
+  } else if constexpr (G == 8) {
+    // the G = 4 layout, two groups per iteration
+    const int64_t base = sb + 4 * lane;
+    const int64_t stride = 4 * (int64_t)A.C;
+    const int ng = W >> 2;
+    int g = 0;
+#pragma unroll 1
+    for (; g + 1 < ng; g += 2) {
+      const int64_t k0 = base + g * stride, k1 = k0 + stride;
+      const int4 c0 = __ldcs(reinterpret_cast<const int4*>(A.scol + k0));
+      const int4 c1 = __ldcs(reinterpret_cast<const int4*>(A.scol + k1));
+      if constexpr (sizeof(T) == 8) {
+        const double2 v00 = __ldcs(reinterpret_cast<const double2*>(A.sval + k0));
+        const double2 v01 = __ldcs(reinterpret_cast<const double2*>(A.sval + k0 + 2));
+        const double2 v10 = __ldcs(reinterpret_cast<const double2*>(A.sval + k1));
+        const double2 v11 = __ldcs(reinterpret_cast<const double2*>(A.sval + k1 + 2));
+        const T x0 = x[c0.x], x1 = x[c0.y], x2 = x[c0.z], x3 = x[c0.w];
+        const T x4 = x[c1.x], x5 = x[c1.y], x6 = x[c1.z], x7 = x[c1.w];
+        acc += v00.x * x0;
+        acc += v00.y * x1;
+        acc += v01.x * x2;
+        acc += v01.y * x3;
+        acc += v10.x * x4;
+        acc += v10.y * x5;
+        acc += v11.x * x6;
+        acc += v11.y * x7;
+      } else {
+        const float4 v0 = __ldcs(reinterpret_cast<const float4*>(A.sval + k0));
+        const float4 v1 = __ldcs(reinterpret_cast<const float4*>(A.sval + k1));
+        const T x0 = x[c0.x], x1 = x[c0.y], x2 = x[c0.z], x3 = x[c0.w];
+        const T x4 = x[c1.x], x5 = x[c1.y], x6 = x[c1.z], x7 = x[c1.w];
+        acc += v0.x * x0;
+        acc += v0.y * x1;
+        acc += v0.z * x2;
+        acc += v0.w * x3;
+        acc += v1.x * x4;
+        acc += v1.y * x5;
+        acc += v1.z * x6;
+        acc += v1.w * x7;
+      }
+    }
+    if (g < ng) {
+      const int64_t k = base + g * stride;
+      const int4 c = __ldcs(reinterpret_cast<const int4*>(A.scol + k));
+      if constexpr (sizeof(T) == 8) {
+        const double2 v0 = __ldcs(reinterpret_cast<const double2*>(A.sval + k));
+        const double2 v1 = __ldcs(reinterpret_cast<const double2*>(A.sval + k + 2));
+        acc += v0.x * x[c.x];
+        acc += v0.y * x[c.y];
+        acc += v1.x * x[c.z];
+        acc += v1.y * x[c.w];
+      } else {
+        const float4 v = __ldcs(reinterpret_cast<const float4*>(A.sval + k));
+        acc += v.x * x[c.x];
+        acc += v.y * x[c.y];
+        acc += v.z * x[c.z];
+        acc += v.w * x[c.w];
+      }
     }
   } else {
     const int64_t base = sb + 4 * lane;

@@ -56,17 +56,20 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Wait for the barrier's phase for at most about kWaitNs of wall time (and
+// Wait for the barrier's phase for at most about limit_ns of wall time (and
 // kWaitLimit polls as a backstop; each try_wait may suspend the thread for a
-// short hardware-defined time).  Returns false when the limit was reached.
+// short hardware-defined time).  Returns false when the limit was reached; a
+// zero limit gives up at once without polling (tests drive the timeout path
+// with it).
 constexpr uint32_t kWaitLimit = 1u << 24;
 constexpr uint64_t kWaitNs = 1000000000ull;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint64_t limit_ns = kWaitNs) {
+  if (limit_ns == 0) return false;
   if (mbar_try_wait(bar, phase)) return true;
   const uint64_t t0 = global_ns();
   for (uint32_t it = 0; it < kWaitLimit; ++it) {
     if (mbar_try_wait(bar, phase)) return true;
-    if ((it & 63u) == 63u && global_ns() - t0 > kWaitNs) return false;
+    if ((it & 63u) == 63u && global_ns() - t0 > limit_ns) return false;
   }
   return false;
 }

@@ -636,33 +636,45 @@ void poisson_boltzmann::build_problem() {
               << t3 - t2 << " s, " << tmsh.size() << " octants\n";
 }
 
-int poisson_boltzmann::build_problem_on_gpu(pbgpu_ctx* ctx) {
-  const double t0 = omp_get_wtime();
+void poisson_boltzmann::initial_octree(pbgpu_mesh_build* out, bool on_gpu) {
   create_mesh();
-  if (mesh_shape == 0 || refine_box == 1 || mesh_shape == 4)
+  // the init_tmesh* variant of the driver (uniform level, box and its level)
+  const bool scale_box = mesh_shape == 0 || refine_box == 1 || mesh_shape == 4;
+  const int init_level = (scale_box || mesh_shape == 3) ? outlevel : unilevel;
+  const int box_level = (scale_box || mesh_shape == 3) ? scale_level : 0;
+  const double* bl = scale_box ? l_c : l_box;
+  const double* br = scale_box ? r_c : r_box;
+  if (on_gpu && init_level <= 8) {
+    tmsh.leaves.clear();
+    tmsh.keys.clear();
+    gb_xyz.clear();
+    gb_level.clear();
+  } else if (scale_box) {
     init_tmesh_with_refine_scale();
-  else if (mesh_shape == 3)
+  } else if (mesh_shape == 3) {
     init_tmesh_with_refine_box_scale();
-  else
+  } else {
     init_tmesh();
-  const int64_t no = tmsh.size();
-  std::vector<int32_t> xyz(3 * no);
-  std::vector<int8_t> lv(no);
+  }
+  const int64_t no = (on_gpu && init_level <= 8) ? 0 : tmsh.size();
+  gb_xyz.assign(3 * no, 0);
+  gb_level.assign(no, 0);
   for (int64_t i = 0; i < no; ++i) {
-    xyz[3 * i + 0] = tmsh.leaves[i].x;
-    xyz[3 * i + 1] = tmsh.leaves[i].y;
-    xyz[3 * i + 2] = tmsh.leaves[i].z;
-    lv[i] = (int8_t)tmsh.leaves[i].level;
+    gb_xyz[3 * i + 0] = tmsh.leaves[i].x;
+    gb_xyz[3 * i + 1] = tmsh.leaves[i].y;
+    gb_xyz[3 * i + 2] = tmsh.leaves[i].z;
+    gb_level[i] = (int8_t)tmsh.leaves[i].level;
   }
-  std::vector<double> sph(4 * atoms.size());
+  gb_spheres.assign(4 * atoms.size(), 0.0);
   for (size_t i = 0; i < atoms.size(); ++i) {
-    for (int k = 0; k < 3; ++k) sph[4 * i + k] = atoms[i].pos[k];
-    sph[4 * i + 3] = atoms[i].radius;
+    for (int k = 0; k < 3; ++k) gb_spheres[4 * i + k] = atoms[i].pos[k];
+    gb_spheres[4 * i + 3] = atoms[i].radius;
   }
-  pbgpu_mesh_build b{};
+  pbgpu_mesh_build& b = *out;
+  b = pbgpu_mesh_build{};
   b.n_oct = no;
-  b.oct_xyz = xyz.data();
-  b.oct_level = lv.data();
+  b.oct_xyz = gb_xyz.data();
+  b.oct_level = gb_level.data();
   for (int a = 0; a < 3; ++a) {
     b.lo[a] = dom.lo[a];
     b.hi[a] = dom.hi[a];
@@ -673,7 +685,19 @@ int poisson_boltzmann::build_problem_on_gpu(pbgpu_ctx* ctx) {
   b.maxlevel = maxlevel;
   b.unilevel = unilevel;
   b.n_spheres = (int64_t)atoms.size();
-  b.spheres = sph.data();
+  b.spheres = gb_spheres.data();
+  b.init_level = init_level;
+  b.box_level = box_level;
+  for (int a = 0; a < 3; ++a) {
+    b.box_lo[a] = bl[a];
+    b.box_hi[a] = br[a];
+  }
+}
+
+int poisson_boltzmann::build_problem_on_gpu(pbgpu_ctx* ctx) {
+  const double t0 = omp_get_wtime();
+  pbgpu_mesh_build b{};
+  initial_octree(&b, true);
   if (gpu && own_gpu && gpu != ctx) pbgpu_ctx_destroy(gpu);
   gpu = ctx;
   own_gpu = false;

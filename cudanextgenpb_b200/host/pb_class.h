@@ -107,6 +107,13 @@ struct poisson_boltzmann {
   // the GPU (pbgpu_build_mesh) into `ctx`, which then also holds the atoms and
   // the model: the domain and the initial octree are built here.
   int build_problem_on_gpu(pbgpu_ctx* ctx);
+  // The host half of build_problem_on_gpu: the domain, and the initial
+  // octree either built here (arrays in this object until the next call) or,
+  // with on_gpu, described for pbgpu_build_mesh to build (n_oct = 0).
+  void initial_octree(pbgpu_mesh_build* out, bool on_gpu);
+  std::vector<int32_t> gb_xyz;
+  std::vector<int8_t> gb_level;
+  std::vector<double> gb_spheres;
 
   // ---- the GPU path (src/poisson_boltzmann.cpp:192-299)
   int upload();

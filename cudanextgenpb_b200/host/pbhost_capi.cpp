@@ -136,6 +136,21 @@ int pbhost_build_on_gpu(pbhost* h, pbgpu_ctx* ctx) {
   return st;
 }
 
+int pbhost_initial_octree(pbhost* h, int on_gpu, pbgpu_mesh_build* out) {
+  if (!h || !out) return PBGPU_ERR_ARG;
+  if (h->pb.atoms.empty()) {
+    h->err = "no atoms";
+    return PBGPU_ERR_STATE;
+  }
+  try {
+    h->pb.initial_octree(out, on_gpu != 0);
+  } catch (const std::exception& ex) {
+    h->err = ex.what();
+    return PBGPU_ERR_ARG;
+  }
+  return PBGPU_OK;
+}
+
 int pbhost_write_vtu(pbhost* h, const char* basename, const char* fieldname, const double* values) {
   if (!h || !basename || !fieldname || !values) return PBGPU_ERR_ARG;
   int st;

@@ -86,6 +86,15 @@ class Problem:
             out[k] = list(v) if hasattr(v, "__len__") else v
         return out
 
+    def mesh_build(self, on_gpu: bool = True) -> N.PbgpuMeshBuild:
+        """The host half of build_on_gpu alone: the pbgpu_mesh_build input of
+        GpuPath.build_mesh or of a server request.  on_gpu leaves the initial
+        octree (init_tmesh*) to the GPU; otherwise it is built here.  Its
+        arrays belong to this problem (valid until the next call)."""
+        b = N.PbgpuMeshBuild()
+        self._check(self._lib.pbhost_initial_octree(self._h, 1 if on_gpu else 0, C.byref(b)))
+        return b
+
     def build_on_gpu(self, g: "GpuPath") -> "GpuPath":
         """Domain and initial octree here, surface refinement, nodes and ray
         tables on the GPU into g's context (which also gets the atoms and the
@@ -226,6 +235,17 @@ class GpuPath:
         self.n, self.n_oct = m.n_nodes, m.n_oct
         return self
 
+    def build_mesh(self, build: N.PbgpuMeshBuild):
+        """pbgpu_build_mesh: surface refinement, nodes and ray tables on the GPU
+        from a host initial octree (Problem.mesh_build())."""
+        self._check(self._lib.pbgpu_build_mesh(self._ctx, C.byref(build)))
+        no, nn, nh = C.c_int64(), C.c_int64(), C.c_int64()
+        nr = (C.c_int64 * 3)()
+        self._check(self._lib.pbgpu_get_mesh_counts(self._ctx, C.byref(no), C.byref(nn), C.byref(nh), nr))
+        self.n, self.n_oct, self.n_hang = nn.value, no.value, nh.value
+        self.n_rays = list(nr)
+        return self
+
     def set_atoms(self, pos, q):
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
         q = np.ascontiguousarray(q, dtype=np.float64)
@@ -352,6 +372,10 @@ class GpuPath:
     def set_profiling(self, on=True):
         self._check(self._lib.pbgpu_set_profiling(self._ctx, 1 if on else 0))
 
+    def set_wait_limit(self, seconds: float):
+        """Limit of each bounded device-side wait of this context (0: give up at once)."""
+        self._check(self._lib.pbgpu_set_wait_limit(self._ctx, float(seconds)))
+
     def counters(self) -> dict:
         c = N.PbgpuCounters()
         self._check(self._lib.pbgpu_get_counters(self._ctx, C.byref(c)))
@@ -420,6 +444,10 @@ class Batch:
     def set_blocks_per_sm(self, blocks: int):
         self._check(self._lib.pbgpu_batch_set_blocks_per_sm(self._b, blocks))
 
+    def set_wait_limit(self, seconds: float):
+        """Limit of each member-barrier wait in the persistent kernel (0: give up at once)."""
+        self._check(self._lib.pbgpu_batch_set_wait_limit(self._b, float(seconds)))
+
     def close(self):
         if self._b:
             self._lib.pbgpu_batch_destroy(self._b)
@@ -463,24 +491,30 @@ class Server:
         if st != 0:
             raise PBError(st, self._lib.pbgpu_server_last_error(self._s).decode())
 
-    def request(self, prob: Problem, pos=None, q=None, tag: int = 0) -> N.PbgpuRequest:
+    def request(self, prob: Problem, pos=None, q=None, tag: int = 0, build: N.PbgpuMeshBuild | None = None
+                ) -> N.PbgpuRequest:
         """The request structure of a built host problem (optionally with other
-        charges on the same atoms)."""
-        m = prob.mesh_struct()
+        charges on the same atoms), or, with `build` (Problem.mesh_build()), of
+        a problem whose mesh the server builds on the GPU."""
         p0, q0, _ = prob.atoms()
         pos = np.ascontiguousarray(p0 if pos is None else pos, dtype=np.float64).reshape(-1, 3)
         q = np.ascontiguousarray(q0 if q is None else q, dtype=np.float64)
         md = prob.model()
         r = N.PbgpuRequest()
-        r.mesh = C.pointer(m)
-        for a in range(3):
-            r.rays[a] = prob.rays_struct(a)
+        m = None
+        if build is not None:
+            r.build = C.pointer(build)
+        else:
+            m = prob.mesh_struct()
+            r.mesh = C.pointer(m)
+            for a in range(3):
+                r.rays[a] = prob.rays_struct(a)
         r.n_atoms = len(q)
         r.pos = _dptr(pos)
         r.charge = _dptr(q)
         r.model = C.pointer(md)
         r.user_tag = tag
-        r._keep = (m, pos, q, md, prob)
+        r._keep = (m, pos, q, md, prob, build)
         return r
 
     def submit(self, req: N.PbgpuRequest) -> int:
@@ -505,6 +539,12 @@ class Server:
         q, r, b = C.c_int(), C.c_int(), C.c_int64()
         self._check(self._lib.pbgpu_server_pending(self._s, C.byref(q), C.byref(r), C.byref(b)))
         return q.value, r.value, b.value
+
+    def stats(self) -> dict:
+        """Requests admitted / completed / rejected and kernels launched so far."""
+        a, c, r, l = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        self._check(self._lib.pbgpu_server_stats(self._s, C.byref(a), C.byref(c), C.byref(r), C.byref(l)))
+        return {"admitted": a.value, "completed": c.value, "rejected": r.value, "launches": l.value}
 
     def estimate(self, req: N.PbgpuRequest) -> int:
         return int(self._lib.pbgpu_request_bytes_estimate(C.byref(req)))

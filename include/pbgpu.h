@@ -50,7 +50,8 @@ enum {
   PBGPU_ERR_CAPACITY = 5,     /* a fixed-size structure overflowed (row too long, ...) */
   PBGPU_NOT_CONVERGED = 10,   /* Krylov iteration hit max_iter (result kept) */
   PBGPU_BREAKDOWN = 11,       /* Krylov breakdown (rho or omega ~ 0) or non-finite value */
-  PBGPU_TIMEOUT = 12          /* a bounded device-side wait gave up */
+  PBGPU_TIMEOUT = 12,         /* a bounded device-side wait gave up */
+  PBGPU_REJECTED = 13         /* server: the request's device-memory estimate exceeds the whole HBM budget */
 };
 
 enum { PBGPU_CG = 0, PBGPU_BICGSTAB = 1, PBGPU_CGS = 2 };
@@ -245,6 +246,13 @@ typedef struct {
   int64_t device_bytes;      /* device memory the context holds now */
 } pbgpu_counters;
 int pbgpu_set_profiling(pbgpu_ctx* ctx, int on);
+/* Upper bound in seconds (0 .. 60, default 1) on each bounded device-side wait
+ * of this context's kernels: the staged SpMV's waits for its bulk copies.  A
+ * wait that reaches it ends the solve with PBGPU_TIMEOUT, after the kernel has
+ * waited for its own copies in flight, and the context stays usable.  0 makes
+ * every such wait give up at once: tests drive the timeout path with it.  No
+ * counterpart in the reference. */
+int pbgpu_set_wait_limit(pbgpu_ctx* ctx, double seconds);
 int pbgpu_get_counters(pbgpu_ctx* ctx, pbgpu_counters* out);
 int pbgpu_reset_counters(pbgpu_ctx* ctx);
 
@@ -265,8 +273,12 @@ int pbgpu_reset_counters(pbgpu_ctx* ctx);
  * GPU that loads it until the process exits): at most 131072 atoms
  * (PBGPU_ERR_CAPACITY beyond).  The first call on a device looks up the
  * arrays' device addresses (cudaGetSymbolAddress) with that device current;
- * make that first call before any stream capture.  All calls share the arrays:
- * calls whose work overlaps on the GPU race and must be serialised. */
+ * make that first call before any stream capture.  The addresses are those of
+ * the device's primary context and stay cached for the life of the process:
+ * do not call it after cudaDeviceReset or from a non-primary context.  With
+ * fewer than 2 atoms the energy (0) is written by a memset on the stream; the
+ * call never waits for the stream.  All calls share the arrays: calls whose
+ * work overlaps on the GPU race and must be serialised. */
 int pbgpu_coulomb_energy_static(const double* atoms, int64_t n_atoms, double e_in, double T, double* out_energy,
                                 void* cuda_stream);
 
@@ -276,11 +288,15 @@ int pbgpu_coulomb_energy_static(const double* atoms, int64_t n_atoms, double e_i
  * (NanoShaper's ray cache, src/raytracer.cpp:379-467; here the van der Waals
  * union of the spheres), on the device.  Input: the initial octree that
  * init_tmesh* builds (Morton order), the domain box, the refinement levels and
- * the spheres (x, y, z, radius; radius <= 0 skipped).  Afterwards the context
- * holds the mesh and rays as after pbgpu_set_mesh / pbgpu_set_rays, identical
- * to the host build of the same problem. */
+ * the spheres (x, y, z, radius; radius <= 0 skipped).  The initial octree is
+ * the caller's (n_oct > 0) or, with n_oct = 0, built here as init_tmesh*
+ * builds it (src/pb_class.cpp:1290-1391): uniform at init_level, then
+ * box_level passes that split every leaf below box_level with a non-hanging
+ * corner inside [box_lo, box_hi], each followed by 2:1 balance.  Afterwards
+ * the context holds the mesh and rays as after pbgpu_set_mesh /
+ * pbgpu_set_rays, identical to the host build of the same problem. */
 typedef struct {
-  int64_t n_oct;
+  int64_t n_oct;             /* 0: build the initial octree from init_level / box_* */
   const int32_t* oct_xyz;    /* 3*n_oct */
   const int8_t* oct_level;   /* n_oct */
   double lo[3], hi[3];
@@ -289,6 +305,9 @@ typedef struct {
   int minlevel, maxlevel, unilevel;
   int64_t n_spheres;
   const double* spheres;     /* 4*n_spheres */
+  int init_level;            /* n_oct == 0: uniform level (outlevel, or unilevel for init_tmesh), 0..8 */
+  int box_level;             /* n_oct == 0: scale_level of init_tmesh_with_refine_(box_)scale; 0: none */
+  double box_lo[3], box_hi[3];  /* the box: l_c / r_c (mesh_shape 0, 4, refine_box) or l_box / r_box (3) */
 } pbgpu_mesh_build;
 int pbgpu_build_mesh(pbgpu_ctx* ctx, const pbgpu_mesh_build* build);
 /* sizes of the context's mesh; n_rays: 3 entries (rays with crossings per axis) */
@@ -363,6 +382,13 @@ int pbgpu_batch_wait(pbgpu_batch* batch, int* n_active);
 /* resident blocks per SM of the persistent kernel (0: as many as fit); fewer
  * leave room for other streams' kernels to run beside it */
 int pbgpu_batch_set_blocks_per_sm(pbgpu_batch* batch, int blocks);
+/* Upper bound in seconds (0 .. 60, default 2) on each wait of a member's CTAs
+ * at the member's barrier inside the persistent kernel.  A wait that reaches
+ * it makes every CTA of the launch return at its next barrier, and the call
+ * returns PBGPU_TIMEOUT; the batch stays usable (the next begin or solve
+ * restarts its members).  0 makes every such wait give up at once: tests
+ * drive the timeout path with it. */
+int pbgpu_batch_set_wait_limit(pbgpu_batch* batch, double seconds);
 
 /* ---- server: continuous batching of PB solves ----------------------------
  * No counterpart in the reference.  Requests (one molecule each: mesh, rays,
@@ -371,16 +397,21 @@ int pbgpu_batch_set_blocks_per_sm(pbgpu_batch* batch, int blocks);
  * the HBM budget allow (device bytes held by all contexts plus an estimate for
  * the request), builds their systems on their own contexts, advances all
  * member systems with one persistent multi-system launch, and returns the
- * requests that finished (energies, solve statistics, latency).  The arrays a
- * request points to must stay valid until its result is returned. */
+ * requests that finished (energies, solve statistics, latency).  A request
+ * whose estimate alone exceeds the budget can never be admitted: it leaves the
+ * queue at once and comes back as a result with status PBGPU_REJECTED.  The
+ * arrays a request points to must stay valid until its result is returned. */
 typedef struct {
-  const pbgpu_mesh* mesh;
-  pbgpu_rays rays[3];
+  const pbgpu_mesh* mesh;    /* the molecule's mesh, or NULL to build it from `build` */
+  pbgpu_rays rays[3];        /* with `mesh`; ignored when the mesh is built */
   int64_t n_atoms;
   const double* pos;         /* 3 n_atoms */
   const double* charge;      /* n_atoms */
   const pbgpu_model* model;
   int64_t user_tag;
+  const pbgpu_mesh_build* build;  /* used when mesh is NULL: the server runs pbgpu_build_mesh (surface
+                                     refinement, nodes, hanging nodes, ray tables) on the request's
+                                     context as the first step of serving it */
 } pbgpu_request;
 
 typedef struct {
@@ -417,7 +448,13 @@ int pbgpu_server_submit(pbgpu_server* server, const pbgpu_request* request, int6
 /* one tick; writes up to `cap` finished requests to out[0 .. *n_out) */
 int pbgpu_server_progress(pbgpu_server* server, pbgpu_result* out, int cap, int* n_out);
 int pbgpu_server_pending(const pbgpu_server* server, int* queued, int* running, int64_t* device_bytes);
-/* device bytes the server plans for a request before it holds any */
+/* Requests admitted, completed and rejected so far, and the kernels the
+ * server's contexts and persistent batch have launched (any may be NULL). */
+int pbgpu_server_stats(const pbgpu_server* server, int64_t* admitted, int64_t* completed, int64_t* rejected,
+                       int64_t* launches);
+/* device bytes the server plans for a request before it holds any; for a
+ * request that carries a mesh build, from the initial octree and the number of
+ * refinement levels above it (an upper bound of the refined mesh's size) */
 int64_t pbgpu_request_bytes_estimate(const pbgpu_request* request);
 
 #ifdef __cplusplus

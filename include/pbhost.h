@@ -52,6 +52,15 @@ int pbhost_build_problem(pbhost* h);
  * atoms and the model; the host keeps no mesh (pbhost_get_mesh / _rays then
  * describe nothing). */
 int pbhost_build_on_gpu(pbhost* h, pbgpu_ctx* ctx);
+/* The host half of pbhost_build_on_gpu alone: the domain (create_mesh) and
+ * the initial octree (init_tmesh*) as the input of pbgpu_build_mesh, for a
+ * caller that builds the rest on a context of its own or hands it to the
+ * server in a pbgpu_request.  on_gpu = 1 leaves the initial octree to
+ * pbgpu_build_mesh (n_oct = 0 with its uniform level and box; what
+ * pbhost_build_on_gpu does); on_gpu = 0 builds it here.  The arrays `out`
+ * points to belong to the handle and stay valid until the next call or
+ * pbhost_destroy. */
+int pbhost_initial_octree(pbhost* h, int on_gpu, pbgpu_mesh_build* out);
 /* One node field (values in node order, n_nodes) on the problem's mesh to
  * <basename>_0000.vtu in the layout of the reference's VTKWriter
  * (src/vtk_class.cpp:20-429): the host's mesh, or the GPU context's when the

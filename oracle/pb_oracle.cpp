@@ -32,7 +32,7 @@
 #include <parallel/algorithm>
 #include <vector>
 
-#include "../cudanextgenpb_b200/csrc/mc_tables.h"
+#include "mc_tri_table.h"
 
 namespace {
 
@@ -41,8 +41,29 @@ const double kPi = 3.14159265358979323846;
 const double e_0 = 8.85418781762e-12, kb = 1.380649e-23, e_ch = 1.602176634e-19, N_av = 6.022e23, Angs = 1e-10;
 const int kRoot = 1 << 19;
 
-const int* E2N = pbmc::kEdgeNodes;
-const int* EAX = pbmc::kEdgeAxis;
+// edge2nodes / edge_axis (include/pb_class.h:190-207): the 12 octant edges in
+// p8est corner order, x in bit 0
+const int E2N[24] = {0, 1, 1, 3, 2, 3, 0, 2, 4, 5, 5, 7, 6, 7, 4, 6, 0, 4, 1, 5, 3, 7, 2, 6};
+const int EAX[12] = {0, 1, 0, 1, 0, 1, 0, 1, 2, 2, 2, 2};
+// p8est corner of marching-cubes vertex v (src/pb_class.cpp:2579-2581)
+const int MC_CORNER[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+
+// Edges whose two end vertices lie on different sides in marching-cubes case k
+// (bit v of k: vertex v inside).
+int mc_cut_edges(int k) {
+  int vertex_of_corner[8];
+  for (int v = 0; v < 8; ++v) vertex_of_corner[MC_CORNER[v]] = v;
+  int m = 0;
+  for (int e = 0; e < 12; ++e)
+    if (((k >> vertex_of_corner[E2N[2 * e]]) ^ (k >> vertex_of_corner[E2N[2 * e + 1]])) & 1) m |= 1 << e;
+  return m;
+}
+
+// The oracle's triangle table (oracle/mc_tri_table.h, from the reference's triTable).
+void load_tri_table(signed char tri[256][16]) {
+  for (int k = 0; k < 256; ++k)
+    for (int j = 0; j < 16; ++j) tri[k][j] = (signed char)oracle_mc::kTriTable[k][j];
+}
 
 uint64_t spread3(uint64_t v) {
   v &= 0x1fffffULL;
@@ -157,6 +178,13 @@ struct oracle_state {
 };
 
 extern "C" {
+
+int oracle_tri_table(int* out) {
+  if (!out) return 1;
+  for (int k = 0; k < 256; ++k)
+    for (int j = 0; j < 16; ++j) out[16 * k + j] = oracle_mc::kTriTable[k][j];
+  return 0;
+}
 
 oracle_state* oracle_create(const pbgpu_mesh* m, const pbgpu_rays* rays3, int64_t n_atoms, const double* pos,
                             const double* charge, const pbgpu_model* model) {
@@ -1023,7 +1051,7 @@ int oracle_energy(oracle_state* s, int fast, pbgpu_energy_out* out) {
   const bool polar = s->model.calc_energy == 1 || (s->model.calc_energy == 2 && s->k < 1.e-5);
   double first_int = 0.0, second_int = 0.0, charge_pol = 0.0;
   signed char tri[256][16];
-  pbmc::expand_tri_table(tri);
+  load_tri_table(tri);
   const int64_t nb = (int64_t)s->border.size();
   double h0[3] = {0, 0, 0};
   if (fast && nb) octant_h(s, s->border[0], h0);
@@ -1092,8 +1120,8 @@ int oracle_energy(oracle_state* s, int fast, pbgpu_energy_out* out) {
       if (!ionic) continue;
       int cube = 0;
       for (int v = 0; v < 8; ++v)
-        if (te[pbmc::kMcCorner[v]] < (s->eps_out - 1e-10)) cube |= 1 << v;
-      if (pbmc::cut_edges(cube) == 0) continue;
+        if (te[MC_CORNER[v]] < (s->eps_out - 1e-10)) cube |= 1 << v;
+      if (mc_cut_edges(cube) == 0) continue;
       for (int t = 0; tri[cube][3 * t] != -1; ++t) {
         double VT[3][3], NT[3][3], ps[3];
         for (int j = 0; j < 3; ++j) {
@@ -1193,7 +1221,7 @@ int oracle_pot_field(oracle_state* s, int fast, int pt, int ft, double* per_atom
   std::vector<Vert> verts;
   double charge_pol = 0.0;
   signed char tri[256][16];
-  pbmc::expand_tri_table(tri);
+  load_tri_table(tri);
   const int64_t nb = (int64_t)s->border.size();
   double h0[3] = {0, 0, 0};
   if (fast && nb) octant_h(s, s->border[0], h0);
@@ -1235,7 +1263,7 @@ int oracle_pot_field(oracle_state* s, int fast, int pt, int ft, double* per_atom
       int cube = 0;
       if (ionic)
         for (int v = 0; v < 8; ++v)
-          if (te[pbmc::kMcCorner[v]] < (s->eps_out - 1e-10)) cube |= 1 << v;
+          if (te[MC_CORNER[v]] < (s->eps_out - 1e-10)) cube |= 1 << v;
       for (int e = 0; e < 12; ++e) {
         const int i1 = E2N[2 * e], i2 = E2N[2 * e + 1];
         double dir;
@@ -1253,7 +1281,7 @@ int oracle_pot_field(oracle_state* s, int fast, int pt, int ft, double* per_atom
         charge_pol += f.F;
         flux.push_back(f);
       }
-      if (!ionic || pbmc::cut_edges(cube) == 0) continue;
+      if (!ionic || mc_cut_edges(cube) == 0) continue;
       for (int t = 0; tri[cube][3 * t] != -1; ++t) {
         Vert T[3];
         for (int j = 0; j < 3; ++j) {

@@ -82,6 +82,8 @@ int oracle_set_system(oracle_state* s, int64_t n, const int64_t* row_ptr, const 
 int oracle_spmv(const oracle_state* s, const double* x, double* y, int threads);
 /* Time `iters` Jacobi-CG iterations on the assembled system (CPU baseline). */
 double oracle_time_cg_iterations(oracle_state* s, int iters, int threads);
+/* the oracle's marching-cubes triangle table, 256 x 16 edge ids (-1 padded) */
+int oracle_tri_table(int* out);
 
 #ifdef __cplusplus
 }

@@ -47,6 +47,7 @@ def load():
         L.oracle_set_phi.argtypes = [sp, P(C.c_double)]
         L.oracle_set_system.argtypes = [sp, C.c_int64, P(C.c_int64), P(C.c_int32), P(C.c_double), P(C.c_double)]
         L.oracle_spmv.argtypes = [sp, P(C.c_double), P(C.c_double), C.c_int]
+        L.oracle_tri_table.argtypes = [P(C.c_int)]
         L.oracle_time_cg_iterations.restype = C.c_double
         L.oracle_time_cg_iterations.argtypes = [sp, C.c_int, C.c_int]
         _lib = L
@@ -192,3 +193,66 @@ class Oracle:
         self.assemble()
         phi, it, rel = self.solve(method, tol)
         return self.energy(fast), phi, it, rel
+
+
+def problem_arrays(prob) -> dict:
+    """A built host problem's oracle inputs as plain numpy arrays (mesh, rays of
+    the three axes, atoms, model), for saving and for ArrayProblem."""
+    m = prob.mesh()
+    d = {"mesh_" + k: np.asarray(v) for k, v in m.items()}
+    for a in range(3):
+        r = prob.rays(a)
+        for k, v in r.items():
+            d["rays%d_%s" % (a, k)] = np.asarray(v)
+    pos, q, rad = prob.atoms()
+    d["atoms_pos"], d["atoms_q"] = pos, q
+    md = prob.model()
+    d["model"] = np.array([getattr(md, k) for k, _ in md._fields_], dtype=np.float64)
+    return d
+
+
+class ArrayProblem:
+    """The inputs Oracle takes (mesh_struct, rays_struct, atoms, model), from
+    the arrays of problem_arrays, with no native library besides the oracle."""
+
+    def __init__(self, d):
+        self.d = {k: np.ascontiguousarray(v) for k, v in d.items()}
+
+    def _p(self, key, ct):
+        return self.d[key].ctypes.data_as(P(ct))
+
+    def mesh_struct(self):
+        d = self.d
+        m = N.PbgpuMesh()
+        m.n_oct, m.n_nodes, m.n_hang = int(d["mesh_n_oct"]), int(d["mesh_n_nodes"]), int(d["mesh_n_hang"])
+        m.oct_xyz = self._p("mesh_oct_xyz", C.c_int32)
+        m.oct_level = self._p("mesh_oct_level", C.c_int8)
+        m.oct_nodes = self._p("mesh_oct_nodes", C.c_int32)
+        m.node_xyz = self._p("mesh_node_xyz", C.c_int32)
+        if m.n_hang:
+            m.hang_np = self._p("mesh_hang_np", C.c_int8)
+            m.hang_par = self._p("mesh_hang_par", C.c_int32)
+        for a in range(3):
+            m.lo[a], m.hi[a] = float(d["mesh_lo"][a]), float(d["mesh_hi"][a])
+        m.locate_tol = float(d["mesh_locate_tol"])
+        return m
+
+    def rays_struct(self, a):
+        r = N.PbgpuRays()
+        pre = "rays%d_" % a
+        r.n_rays = len(self.d[pre + "keys"])
+        r.keys = self._p(pre + "keys", C.c_uint64)
+        r.ptr = self._p(pre + "ptr", C.c_int64)
+        r.inters = self._p(pre + "inters", C.c_double)
+        r.normals = self._p(pre + "normals", C.c_double)
+        return r
+
+    def atoms(self):
+        q = self.d["atoms_q"]
+        return self.d["atoms_pos"], q, np.zeros_like(q)
+
+    def model(self):
+        md = N.PbgpuModel()
+        for (k, t), v in zip(md._fields_, self.d["model"]):
+            setattr(md, k, t(int(v)).value if t is C.c_int else float(v))
+        return md

@@ -54,3 +54,20 @@ def test_gpu_mesh_equals_host_mesh(name):
         assert eh[k] == pytest.approx(ed[k], rel=1e-13, abs=1e-15), k
     g_host.close()
     g_dev.close()
+
+
+@pytest.mark.parametrize("name", ["born", "mol60", "mol150"])
+def test_initial_octree_on_gpu_equals_host_initial_octree(name):
+    """init_tmesh* on the GPU (n_oct = 0: uniform level, then box refinement
+    with 2:1 balance) and on the host give the same refined mesh."""
+    p_host, p_dev = CASES[name](), CASES[name]()
+    b_host, b_dev = p_host.mesh_build(on_gpu=False), p_dev.mesh_build(on_gpu=True)
+    assert b_host.n_oct > 0 and b_dev.n_oct == 0
+    g_host, g_dev = GpuPath().build_mesh(b_host), GpuPath().build_mesh(b_dev)
+    assert (g_host.n_oct, g_host.n, g_host.n_hang) == (g_dev.n_oct, g_dev.n, g_dev.n_hang)
+    assert g_host.n_rays == g_dev.n_rays
+    dh, dd = g_host.mesh_arrays(), g_dev.mesh_arrays()
+    for k in ("oct_xyz", "oct_level", "oct_nodes", "node_xyz", "hang_np", "hang_par", "lo", "extent"):
+        assert np.array_equal(dh[k], dd[k]), k
+    g_host.close()
+    g_dev.close()

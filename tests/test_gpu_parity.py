@@ -212,10 +212,17 @@ def test_preconditioners(case_name, method, precond, precision):
     g.assemble()
     st = g.solve(solver_opts(method, tol=1e-8, precond=precond, precision=precision))
     assert st.status == 0 and st.rel_residual <= 1e-8
-    if precision == "fp64":
-        _, oit, _ = o.solve(method, 1e-8, precond=precond)
-        # BiCGStab's iteration count is sensitive to the rounding of its scalars
-        assert abs(st.iterations - oit) <= max(2, oit // (25 if method == "cg" else 8)), (st.iterations, oit)
+    if precision == "fp64" and method == "cg":
+        _, oit, _ = o.solve(method, 1e-8, precond=precond, threads=1)
+        assert abs(st.iterations - oit) <= max(2, oit // 25), (st.iterations, oit)
+    elif precision == "fp64":
+        # BiCGStab's iteration count depends on the rounding of its scalars: the
+        # oracle alone moves it by 15 % and more when only its summation order
+        # changes (its thread count).  The GPU's count must lie within that
+        # spread, widened by 1/8.
+        its = [o.solve(method, 1e-8, precond=precond, threads=t)[1] for t in (1, 2, 3, 4, 6, 8)]
+        lo, hi = min(its), max(its)
+        assert lo - max(2, lo // 8) <= st.iterations <= hi + max(2, hi // 8), (st.iterations, its)
     ophi, _, _ = o.solve("cg", 1e-12)
     assert np.linalg.norm(g.phi() - ophi) / np.linalg.norm(ophi) < 1e-6
     g.close()

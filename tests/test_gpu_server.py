@@ -104,3 +104,30 @@ def test_server_charges_on_same_mesh(pool):
         g.close()
         assert got[k] == pytest.approx(e["sum"], rel=1e-6)
     srv.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_server_builds_request_meshes(pool, mode):
+    """Requests that carry only the molecule (atoms, options): the server
+    builds each mesh on the GPU (initial octree, surface refinement, nodes,
+    rays) as the first step of serving it; results equal the host-meshed
+    plain solves."""
+    srv = Server(tol=1e-10, precision="mixed", max_members=3, steps_per_tick=24, mode=mode, workers=3)
+    probs = []
+    for k, (na, rad, net, seed, lv) in enumerate(SPECS):
+        p = configs.make_globular_problem(na, rad, net, seed=seed, levels=lv)
+        b = p.mesh_build()
+        probs.append((p, b))
+        srv.submit(srv.request(p, tag=k, build=b))
+    results = {}
+    for _ in range(20000):
+        for r in srv.progress():
+            results[r["tag"]] = r
+        q, running, _ = srv.pending()
+        if len(results) == len(SPECS) and q == 0 and running == 0:
+            break
+    srv.close()
+    assert sorted(results) == list(range(len(SPECS)))
+    for k, r in results.items():
+        assert r["status"] == 0 and r["rel_residual"] <= 1e-10
+        assert r["energy"]["sum"] == pytest.approx(pool[k][1], rel=1e-6)

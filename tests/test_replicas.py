@@ -37,9 +37,22 @@ def test_max_over_ranks_gloo():
 def test_reference_arm_under_two_ranks_prints_once():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", "29518", os.path.join(ROOT, "bench.py"),
-           "--impl", "reference", "--workload", "mol60", "--steps", "1", "--warmup", "3", "--cpu-iters", "5"]
+           "--impl", "reference", "--workload", "mol60", "--steps", "1", "--warmup", "3"]
     env = dict(os.environ, OMP_NUM_THREADS="2")
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1 and '"impl": "reference"' in lines[0]
+
+
+def test_gpus_flag_spawns_replicas_without_torchrun():
+    """`bench.py --gpus 2` started as a plain process (no WORLD_SIZE) starts
+    its own two ranks; rank 0 alone prints the line, which names 2 GPUs."""
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--impl", "reference",
+           "--workload", "mol60", "--steps", "1", "--warmup", "3"]
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    env["OMP_NUM_THREADS"] = "2"
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1 and '"impl": "reference"' in lines[0] and '"n_gpus": 2' in lines[0]
