@@ -163,6 +163,8 @@ def spmv_kernel_name(args):
     """The CG SpMV kernel the solve runs for the bench's layout."""
     if args.chunk == 32 and args.group == 1 and os.environ.get("PBGPU_SPMV") != "direct":
         return "k_cg_spmv_tma<double, %s>" % os.environ.get("PBGPU_SPMV_COLS", "16")
+    if args.group == 4 and os.environ.get("PBGPU_SPMV_PAIRS", "1") != "0":
+        return "k_cg_spmv<double, 8>"  # the G = 4 layout walked two column groups per iteration
     return "k_cg_spmv<double, %d>" % args.group
 
 
@@ -727,6 +729,81 @@ def run_batch(args, rank, world, local):
     }
 
 
+CHARGES = {
+    # name: (n_atoms, net charge, seed, surface levels, charge vectors, titratable sites flipped per vector)
+    "charges64": (5000, 0.0, 5000, 1, 64, 8),
+}
+
+
+def run_charges(args, rank, world, local):
+    """Many charge vectors on one molecule: each vector flips +-1 e on 8
+    random titratable sites of a 5,000-atom synthetic molecule; a step solves
+    all 64 through one pbgpu_solve_charges call (one matrix, 64 right-hand
+    sides sharing every SpMV), against the plain FP64 path solving them one at
+    a time (new charges, density map, right-hand side, solve, energy)."""
+    import torch
+
+    from cudanextgenpb_b200 import GpuPath, configs, solve_charges, solver_opts
+
+    if rank != 0 and world > 1:
+        return None
+    torch.cuda.set_device(local)
+    na, net, seed, levels, k, flips = CHARGES[args.workload]
+    prob = configs.make_globular_problem(na, configs.radius_for(na), net, seed, scale=2.0, levels=levels)
+    g = prob.build_on_gpu(GpuPath(local))
+    g.create_markers()
+    g.create_density_map()
+    g.assemble()
+    pos, q, _ = prob.atoms()
+    rng = np.random.default_rng(64)
+    Q = np.repeat(q[None, :], k, axis=0)
+    for j in range(k):
+        Q[j, rng.choice(na, size=flips, replace=False)] += rng.choice([-1.0, 1.0], size=flips)
+    opts = solver_opts("cg", tol=args.tol, max_iter=50000)
+    plain = GpuPath(local)
+    prob2 = configs.make_globular_problem(na, configs.radius_for(na), net, seed, scale=2.0, levels=levels)
+    prob2.build_on_gpu(plain)
+
+    def plain_all():
+        out = []
+        for j in range(k):
+            plain.set_atoms(pos, Q[j])
+            e, _ = plain.run(opts)
+            out.append(e["sum"])
+        return out
+
+    for _ in range(args.warmup):
+        solve_charges(g, Q, opts)
+    plain_all()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        es, ss = solve_charges(g, Q, opts)
+    torch.cuda.synchronize()
+    t_multi = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ep = plain_all()
+    t_plain = time.perf_counter() - t0
+    ck = clocks.stop()
+    err = max(abs(a["sum"] - b) / abs(b) for a, b in zip(es, ep))
+    value = k * args.steps / t_multi
+    g.close()
+    plain.close()
+    return {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_multi / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "%d charge vectors (+-1 e on %d random sites each, seed 64) on a %d-atom synthetic "
+                                   "molecule (net %+g e, seed %d), scale 2/A, %d surface level(s), %d DoF; one "
+                                   "multi-right-hand-side solve per step" % (k, flips, na, net, seed, levels, g.n),
+                       "plain_solves_per_s": k / t_plain, "speedup_vs_plain_fp64": value / (k / t_plain),
+                       "max_rel_energy_err_vs_plain": err, "tol": args.tol,
+                       "iterations_max": max(s.iterations for s in ss),
+                       "wall_clock": "host perf_counter after a device synchronize"},
+            "clocks": ck}
+
+
 SERVES = {
     # name: (pool size, min atoms, max atoms, seed, surface levels drawn from, requests per step)
     # the request stream: seeded synthetic molecules (atoms log-uniform in
@@ -829,7 +906,7 @@ def spmv_roofline(local):
     peak, kind = measured_peak()
     achieved = cnt["spmv_bytes"] / (avg / 1e3) / 1e9
     tr = spmv_traffic()
-    kname = "k_cg_spmv<double, 4>"
+    kname = "k_cg_spmv<double, 8>" if os.environ.get("PBGPU_SPMV_PAIRS", "1") != "0" else "k_cg_spmv<double, 4>"
     traffic = None
     if tr and kname in tr.get("kernels", {}):
         traffic = tr["kernels"][kname]["dram_bytes_per_launch"] * (nnz / tr["nnz"])
@@ -927,8 +1004,10 @@ def run_serve(args, rank, world, local):
 
     # ---- plain FP64, one request at a time
     g = GpuPath(local)
+    size = {}  # pool molecule -> (DoF, nonzeros)
     for k in warm:
         plain_request(g, pool[k], opts64)
+        size[int(k)] = (g.n, info_nnz(g))
     g.reset_counters()
     sync_all()
     clocks = Clocks(local)
@@ -941,6 +1020,8 @@ def run_serve(args, rank, world, local):
         lat_p.append(1e3 * (time.perf_counter() - a))
         e_plain[int(k)] = e["sum"]
         it_p.append(st.iterations)
+        if int(k) not in size:
+            size[int(k)] = (g.n, info_nnz(g))
     torch.cuda.synchronize()
     t_plain = max_over_ranks(time.perf_counter() - t0, dist)
     plain_launches = g.counters()["launches"]
@@ -983,6 +1064,19 @@ def run_serve(args, rank, world, local):
         pct = lambda a: {"p50": float(np.percentile(a, 50)), "p95": float(np.percentile(a, 95)),
                          "p99": float(np.percentile(a, 99))}
         h2d = sum(pool[k].upload_bytes for k in timed)
+        # the Krylov iterations' algorithmic bytes over each stream's time: how
+        # close the streams run to the HBM bound of their solves alone
+        peak, peak_kind = measured_peak()
+        b_plain = sum(it * (12 * size[int(k)][1] + 104 * size[int(k)][0]) for it, k in zip(it_p, timed))
+        b_served = sum(res[j]["iterations"] * (8 * size[int(k)][1] + 52 * size[int(k)][0])
+                       for j, k in enumerate(timed))
+        stream_bw = {
+            "plain_solve_gbs": b_plain / t_plain / 1e9, "served_solve_gbs": b_served / t_served / 1e9,
+            "peak_gbs": peak, "peak_kind": peak_kind_text(peak_kind),
+            "served_solve_floor_s": b_served / (peak * 1e9), "served_s": t_served,
+            "what": "CG iterations x algorithmic bytes per iteration (FP64: 12 nnz + 104 n; FP32 inner: 8 nnz + "
+                    "52 n) summed over the timed requests, divided by the stream's time; mesh build, set-up "
+                    "and energy excluded from the bytes but not from the time"}
         # the oracle on the three smallest molecules the stream served (tight solve)
         served_ids = sorted(set(int(k) for k in timed), key=lambda k: pool[k].spec[0])[:3]
         parity = oracle_serve_parity(pool, served_ids, e_plain, e_served)
@@ -1010,6 +1104,7 @@ def run_serve(args, rank, world, local):
                                 "latency from arrival to result" % (rate, len(timed)),
                 "max_rel_energy_err_served_vs_plain_fp64": err_plain,
                 "oracle_parity": parity,
+                "stream_bandwidth": stream_bw,
                 "failed_requests": len(bad),
                 "plain_cg_iterations_median": float(np.median(it_p)),
                 "served_iterations_median": float(np.median([r["iterations"] for r in res.values()])),
@@ -1055,7 +1150,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="serve", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(SERVES))
+    ap.add_argument("--workload", default="serve",
+                    choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(SERVES) + sorted(CHARGES))
     ap.add_argument("--max-members", type=int, default=64)
     ap.add_argument("--via-batch", action="store_true", help="solve through the persistent multi-system kernel")
     ap.add_argument("--server-mode", default="concurrent", choices=["concurrent", "batched"])
@@ -1085,8 +1181,11 @@ def main():
     from cudanextgenpb_b200 import build as b
     if rank == 0:
         b.build_all()
-    if args.impl == "reference" and args.workload not in BATCHES:
+    if args.impl == "reference" and args.workload not in BATCHES and args.workload not in CHARGES:
         res = run_reference(args, rank, world)
+    elif args.workload in CHARGES:
+        res = run_charges(args, rank, world, local) if args.impl == "ours" else {
+            "impl": "reference", "unavailable": "the charge-vector workload is measured against the plain GPU path"}
     elif args.workload in SERVES:
         res = run_serve(args, rank, world, local)
     elif args.workload in BATCHES:

@@ -322,6 +322,14 @@ __global__ void k_row_fill(AsmView A, LocalView L, SellOut S) {
   }
 }
 
+// a[1] = stored elements (the slice offsets' end), a[2] = overflow flag; a[0]
+// holds nnz already
+__global__ void k_asm_totals(const int64_t* __restrict__ slice_end, const int* __restrict__ ovf,
+                             unsigned long long* __restrict__ a) {
+  a[1] = (unsigned long long)*slice_end;
+  a[2] = (unsigned long long)*ovf;
+}
+
 // Padding rows past n in the last slice.
 __global__ void k_pad_rows(SellOut S, int64_t n, int64_t n_pad) {
   const int64_t p = n + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -505,21 +513,19 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(c->tmp.get(), bytes, elems.get(), c->slice_ptr.get(), n_slices + 1,
                                               c->stream));
   c->launches += kCubScanLaunches;
-  int64_t total = 0;
-  PBGPU_CUDA(c, cudaMemcpyAsync(&total, c->slice_ptr.get() + n_slices, sizeof(int64_t), cudaMemcpyDeviceToHost,
-                                c->stream));
-  // nnz = sum of row lengths
+  // nnz = sum of row lengths; the stored length, nnz and the overflow flag
+  // come back in one read (the only host wait of the assembly)
   Scratch<unsigned long long> nnz_d(c, kScAsmNnz);
-  PBGPU_CUDA(c, nnz_d.alloc(1));
+  PBGPU_CUDA(c, nnz_d.alloc(4));
   PBGPU_CUDA(c, cudaMemsetAsync(nnz_d.get(), 0, sizeof(unsigned long long), c->stream));
   k_sum_rowlen<<<grid_for(n, 256), 256, 0, c->stream>>>(c->rowlen.get(), n, nnz_d.get());
   PBGPU_LAUNCHED(c);
-  int64_t nnz = 0;
-  int h_ovf = 0;
-  PBGPU_CUDA(c, cudaMemcpyAsync(&nnz, nnz_d.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
-  PBGPU_CUDA(c, cudaMemcpyAsync(&h_ovf, ovf.get(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
-  if (h_ovf) return c->fail(PBGPU_ERR_CAPACITY, "assemble: a matrix row has more than kMaxRow columns");
+  k_asm_totals<<<1, 1, 0, c->stream>>>(c->slice_ptr.get() + n_slices, ovf.get(), nnz_d.get());
+  PBGPU_LAUNCHED(c);
+  unsigned long long tot[3] = {0, 0, 0};
+  PBGPU_CUDA(c, readback(c, tot, nnz_d.get(), sizeof(tot)));
+  const int64_t nnz = (int64_t)tot[0], total = (int64_t)tot[1];
+  if (tot[2]) return c->fail(PBGPU_ERR_CAPACITY, "assemble: a matrix row has more than kMaxRow columns");
   c->n_slices = n_slices;
   c->sell_len = total;
   c->nnz = nnz;
@@ -543,7 +549,6 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
     k_pad_rows<<<grid_for(n_pad - n, 128), 128, 0, c->stream>>>(S, n, n_pad);
     PBGPU_LAUNCHED(c);
   }
-  PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   c->have_system = true;
   c->bj_ready = false;
   c->have_phi = false;

@@ -99,7 +99,7 @@ int build_incidence(Context* c) {
   PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(c->tmp.get(), bytes, cnt.get(), c->inc_ptr.get(), n + 1, c->stream));
   c->launches += kCubScanLaunches;
   int64_t total = 0;
-  PBGPU_CUDA(c, cudaMemcpyAsync(&total, c->inc_ptr.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, readback(c, &total, c->inc_ptr.get() + n, sizeof(int64_t)));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   PBGPU_CUDA(c, c->inc.alloc(total > 0 ? total : 1));
   PBGPU_CUDA(c, cudaMemsetAsync(cnt.get(), 0, (n + 1) * sizeof(int32_t), c->stream));

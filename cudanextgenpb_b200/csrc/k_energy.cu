@@ -10,7 +10,12 @@
 //  (1) one thread per border octant evaluates the reference's per-element
 //      coefficients (flux F, and coef * N with coef = phi0 * area / (12 pi) for
 //      a triangle vertex) and adds them into an accumulator of the crossing
-//      they sit on (elements whose edge has no crossing keep their own point);
+//      they sit on (elements whose edge has no crossing keep their own point).
+//      The accumulators are 128-bit fixed point (2^-64 resolution) updated by
+//      integer atomics: integer addition is associative, so each crossing's
+//      sum is exact and the same whatever order the octants add in, and the
+//      energies are bit-for-bit reproducible; the elements without a crossing
+//      are put in (octant, element) order before they become points;
 //  (2) the used crossings are compacted into a point list (V, F, D);
 //  (3) one FP64 pair kernel over points x charged atoms, atoms staged in shared
 //      memory tiles, evaluates sum_a q_a / r (flux) and sum_a q_a (V - x_a).D / r^3
@@ -37,11 +42,12 @@ struct EnergyView {
   const double* phi;
   RayView rays[3];
   int64_t slot_base[3];   // first accumulator slot of each axis' crossings
-  double4* acc;           // per crossing: F, Dx, Dy, Dz
+  unsigned long long* acc;  // per crossing: F, Dx, Dy, Dz, each 128-bit fixed point (low, high words)
   uint8_t* used;
   int32_t* slot_ray;      // ray of each used crossing
   double4* extra_p;       // elements on edges without a crossing
   double4* extra_d;
+  unsigned long long* extra_key;  // (border octant << 8) | element number in the octant
   unsigned long long* n_extra;
   int64_t extra_cap;
   int64_t n, nb;
@@ -139,14 +145,31 @@ __device__ __forceinline__ int cube_index(const CellCtx& C, double eps_out) {
   return k;
 }
 
-__device__ __forceinline__ void add_point(const EnergyView& E, int64_t slot, int32_t ray, const double V[3], double F,
-                                          double Dx, double Dy, double Dz) {
+// a[0] (low word) and a[1] (high word, signed) += v as 128-bit fixed point
+// with 64 fraction bits: v = hi + lo 2^-64 with 0 <= lo < 2^64 is exact for
+// |v| < 2^63 down to 2^-64 (smaller parts drop, 5e-20 absolute); the carry of
+// the low word goes into the high one, so the total is exact in any order.
+__device__ __forceinline__ void add_fixed128(unsigned long long* a, double v) {
+  const double fl = floor(v);
+  const unsigned long long lo = (unsigned long long)((v - fl) * 0x1p64);
+  const unsigned long long hi = (unsigned long long)(long long)fl;
+  const unsigned long long old = atomicAdd(a, lo);
+  atomicAdd(a + 1, hi + (old + lo < old ? 1ull : 0ull));
+}
+
+__device__ __forceinline__ double fixed128_value(const unsigned long long* a) {
+  return (double)(long long)a[1] + (double)a[0] * 0x1p-64;
+}
+
+__device__ __forceinline__ void add_point(const EnergyView& E, int64_t b, int& local, int64_t slot, int32_t ray,
+                                          const double V[3], double F, double Dx, double Dy, double Dz) {
+  const int elem = local++;
   if (slot >= 0) {
-    double* a = reinterpret_cast<double*>(E.acc + slot);
-    if (F != 0.0) atomicAdd(a, F);
-    if (Dx != 0.0) atomicAdd(a + 1, Dx);
-    if (Dy != 0.0) atomicAdd(a + 2, Dy);
-    if (Dz != 0.0) atomicAdd(a + 3, Dz);
+    unsigned long long* a = E.acc + 8 * slot;
+    if (F != 0.0) add_fixed128(a, F);
+    if (Dx != 0.0) add_fixed128(a + 2, Dx);
+    if (Dy != 0.0) add_fixed128(a + 4, Dy);
+    if (Dz != 0.0) add_fixed128(a + 6, Dz);
     E.used[slot] = 1;
     E.slot_ray[slot] = ray;
     return;
@@ -155,6 +178,7 @@ __device__ __forceinline__ void add_point(const EnergyView& E, int64_t slot, int
   if ((int64_t)i < E.extra_cap) {
     E.extra_p[i] = make_double4(V[0], V[1], V[2], F);
     E.extra_d[i] = make_double4(Dx, Dy, Dz, 0.0);
+    E.extra_key[i] = ((unsigned long long)b << 8) | (unsigned long long)elem;
   }
 }
 
@@ -165,6 +189,7 @@ __global__ void k_energy_accumulate(EnergyView E) {
   if (b >= E.nb) return;
   CellCtx C;
   cell_load(E, b, C);
+  int local = 0;  // element number in this octant (at most 12 + 15)
   for (int e = 0; e < 12; ++e) {
     const int i1 = d_edge_nodes[2 * e], i2 = d_edge_nodes[2 * e + 1];
     double dir;
@@ -180,7 +205,7 @@ __global__ void k_energy_accumulate(EnergyView E) {
     double V[3];
     edge_point(E, C, e, f, V);
     const double F = -(C.tp[i2] - C.tp[i1]) * wha(C.te[i1], C.te[i2], f) * dir * C.area_h[d_edge_axis[e]];
-    add_point(E, slot, ray, V, F, 0.0, 0.0, 0.0);
+    add_point(E, b, local, slot, ray, V, F, 0.0, 0.0, 0.0);
   }
   if (!E.ionic) return;
   const int k = cube_index(C, E.eps_out);
@@ -209,7 +234,7 @@ __global__ void k_energy_accumulate(EnergyView E) {
         0.5 * norm3d(ab[1] * ac[2] - ab[2] * ac[1], ab[0] * ac[2] - ab[2] * ac[0], ab[1] * ac[0] - ab[0] * ac[1]);
     for (int j = 0; j < 3; ++j) {
       const double coef = ps[j] * inv_4pi * area / 3.0;
-      add_point(E, sl[j], ry[j], VT[j], 0.0, coef * NT[j][0], coef * NT[j][1], coef * NT[j][2]);
+      add_point(E, b, local, sl[j], ry[j], VT[j], 0.0, coef * NT[j][0], coef * NT[j][1], coef * NT[j][2]);
     }
   }
 }
@@ -230,9 +255,24 @@ __global__ void k_energy_points(const int32_t* __restrict__ used_slots, int64_t 
   V[axis] = R.inters[k];
   V[t0] = coord(E.lo[t0], E.len[t0], (int32_t)(key >> 20));
   V[t1] = coord(E.lo[t1], E.len[t1], (int32_t)(key & 0xfffff));
-  const double4 a = E.acc[slot];
-  P[i] = make_double4(V[0], V[1], V[2], a.x);
-  D[i] = make_double4(a.y, a.z, a.w, 0.0);
+  const unsigned long long* a = E.acc + 8 * slot;
+  P[i] = make_double4(V[0], V[1], V[2], fixed128_value(a));
+  D[i] = make_double4(fixed128_value(a + 2), fixed128_value(a + 4), fixed128_value(a + 6), 0.0);
+}
+
+__global__ void k_iota_u64(unsigned long long* __restrict__ a, int64_t m) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < m) a[i] = (unsigned long long)i;
+}
+
+// the elements without a crossing in (octant, element) order
+__global__ void k_gather_extras(const unsigned long long* __restrict__ order, int64_t m, const double4* __restrict__ xp,
+                                const double4* __restrict__ xd, double4* __restrict__ P, double4* __restrict__ D) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int64_t j = (int64_t)order[i];
+  P[i] = xp[j];
+  D[i] = xd[j];
 }
 
 constexpr int kTile = 256;
@@ -395,7 +435,7 @@ int run_phi_atoms(Context* c, double* out) {
 
 static int sum_partials(Context* c, const double* d, int nblk, int stride, double* out) {
   std::vector<double> h((size_t)nblk * stride);
-  PBGPU_CUDA(c, cudaMemcpyAsync(h.data(), d, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, readback(c, h.data(), d, h.size() * sizeof(double)));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   for (int k = 0; k < stride; ++k) {
     double s = 0.0;
@@ -423,9 +463,9 @@ int surface_points(Context* c, int fast, bool ionic, SurfacePoints* out) {
   if (fast) {
     int32_t b0 = 0;
     int4 q;
-    PBGPU_CUDA(c, cudaMemcpyAsync(&b0, c->border.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    PBGPU_CUDA(c, readback(c, &b0, c->border.get(), sizeof(int32_t)));
     PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
-    PBGPU_CUDA(c, cudaMemcpyAsync(&q, c->oct.get() + b0, sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+    PBGPU_CUDA(c, readback(c, &q, c->oct.get() + b0, sizeof(int4)));
     PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     const int32_t s = 1 << (kRootLog - q.w);
     const int32_t qc[3] = {q.x, q.y, q.z};
@@ -437,7 +477,7 @@ int surface_points(Context* c, int fast, bool ionic, SurfacePoints* out) {
   }
   const int64_t nslots = c->rays[0].nc + c->rays[1].nc + c->rays[2].nc;
   const int64_t ns = nslots > 0 ? nslots : 1;
-  Scratch<double4> acc(c, kScEnAcc);
+  Scratch<unsigned long long> acc(c, kScEnAcc);
   Scratch<uint8_t> used(c, kScEnUsed);
   Scratch<int32_t> slot_ray(c, kScEnSlotRay), sel(c, kScEnSel);
   Scratch<int64_t> nsel(c, kScEnNsel);
@@ -447,7 +487,8 @@ int surface_points(Context* c, int fast, bool ionic, SurfacePoints* out) {
   // is grown and the pass repeated if it overflows
   int64_t extra_cap = nb + 1024;
   Scratch<double4> xp(c, kScEnXp), xd(c, kScEnXd);
-  PBGPU_CUDA(c, acc.alloc(ns));
+  Scratch<unsigned long long> xk(c, kScEnXk), xk2(c, kScEnXk2), xi(c, kScEnXi), xi2(c, kScEnXi2);
+  PBGPU_CUDA(c, acc.alloc(8 * ns));
   PBGPU_CUDA(c, used.alloc(ns));
   PBGPU_CUDA(c, slot_ray.alloc(ns));
   PBGPU_CUDA(c, sel.alloc(ns));
@@ -461,15 +502,17 @@ int surface_points(Context* c, int fast, bool ionic, SurfacePoints* out) {
   for (int attempt = 0; attempt < 2; ++attempt) {
     PBGPU_CUDA(c, xp.alloc(extra_cap));
     PBGPU_CUDA(c, xd.alloc(extra_cap));
-    PBGPU_CUDA(c, cudaMemsetAsync(acc.get(), 0, ns * sizeof(double4), c->stream));
+    PBGPU_CUDA(c, xk.alloc(extra_cap));
+    PBGPU_CUDA(c, cudaMemsetAsync(acc.get(), 0, 8 * ns * sizeof(unsigned long long), c->stream));
     PBGPU_CUDA(c, cudaMemsetAsync(used.get(), 0, ns, c->stream));
     PBGPU_CUDA(c, cudaMemsetAsync(n_extra.get(), 0, sizeof(unsigned long long), c->stream));
     E.extra_p = xp.get();
     E.extra_d = xd.get();
+    E.extra_key = xk.get();
     E.extra_cap = extra_cap;
     k_energy_accumulate<<<grid_for(nb, 128), 128, 0, c->stream>>>(E);
     PBGPU_LAUNCHED(c);
-    PBGPU_CUDA(c, cudaMemcpyAsync(&nx, n_extra.get(), sizeof(nx), cudaMemcpyDeviceToHost, c->stream));
+    PBGPU_CUDA(c, readback(c, &nx, n_extra.get(), sizeof(nx)));
     PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     if ((int64_t)nx <= extra_cap) break;
     extra_cap = (int64_t)nx;
@@ -482,7 +525,7 @@ int surface_points(Context* c, int fast, bool ionic, SurfacePoints* out) {
   PBGPU_CUDA(c, cub::DeviceSelect::Flagged(c->tmp.get(), bytes, idx, used.get(), sel.get(), nsel.get(), ns, c->stream));
   c->launches += kCubSelectLaunches;
   int64_t np = 0;
-  PBGPU_CUDA(c, cudaMemcpyAsync(&np, nsel.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, readback(c, &np, nsel.get(), sizeof(int64_t)));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   const int64_t npts = np + (int64_t)nx;
   Scratch<double4> P(c, kScEnP), D(c, kScEnD);
@@ -493,8 +536,23 @@ int surface_points(Context* c, int fast, bool ionic, SurfacePoints* out) {
     PBGPU_LAUNCHED(c);
   }
   if (nx) {
-    PBGPU_CUDA(c, cudaMemcpyAsync(P.get() + np, xp.get(), nx * sizeof(double4), cudaMemcpyDeviceToDevice, c->stream));
-    PBGPU_CUDA(c, cudaMemcpyAsync(D.get() + np, xd.get(), nx * sizeof(double4), cudaMemcpyDeviceToDevice, c->stream));
+    // the order the atomics handed out is arbitrary: sort by (octant, element)
+    const int m = (int)nx;
+    PBGPU_CUDA(c, xk2.alloc(m));
+    PBGPU_CUDA(c, xi.alloc(m));
+    PBGPU_CUDA(c, xi2.alloc(m));
+    k_iota_u64<<<grid_for(m, 256), 256, 0, c->stream>>>(xi.get(), m);
+    PBGPU_LAUNCHED(c);
+    size_t bytes = 0;
+    PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(nullptr, bytes, xk.get(), xk2.get(), xi.get(), xi2.get(), m, 0, 64,
+                                                  c->stream));
+    PBGPU_CUDA(c, ensure_tmp(c, bytes));
+    PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(c->tmp.get(), bytes, xk.get(), xk2.get(), xi.get(), xi2.get(), m, 0,
+                                                  64, c->stream));
+    c->launches += cub_radix_launches(m, 64);
+    k_gather_extras<<<grid_for(m, 256), 256, 0, c->stream>>>(xi2.get(), m, xp.get(), xd.get(), P.get() + np,
+                                                             D.get() + np);
+    PBGPU_LAUNCHED(c);
   }
   out->P = P.get();
   out->D = D.get();

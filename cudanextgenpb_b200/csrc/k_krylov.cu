@@ -961,11 +961,13 @@ static int staged_cols(const Context* c, int C, int G) {
   return (nc == 8 || nc == 12 || nc == 16) ? nc : 16;
 }
 
-// PBGPU_SPMV_PAIRS=1 walks the G = 4 layout two column groups per iteration
-// (sell_row<T, 8>).
+// The G = 4 layout is walked two column groups per iteration (sell_row<T, 8>:
+// the same sums in the same order, with half the dependent load round trips;
+// measured 2-4 % faster than one group per iteration on 3.3 M and 14.5 M DoF
+// systems).  PBGPU_SPMV_PAIRS=0 selects the one-group kernel.
 static bool spmv_pairs() {
   const char* e = std::getenv("PBGPU_SPMV_PAIRS");
-  return e && e[0] == '1';
+  return !(e && e[0] == '0');
 }
 
 // Grid of the staged SpMV kernels for storage type T and chunk width NC:

@@ -53,7 +53,7 @@ int build_ray_hash_from(Context* c, int axis, const uint64_t* d_keys) {
                                                            ovf.get());
   PBGPU_LAUNCHED(c);
   int h_ovf = 0;
-  PBGPU_CUDA(c, cudaMemcpyAsync(&h_ovf, ovf.get(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, readback(c, &h_ovf, ovf.get(), sizeof(int)));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   if (h_ovf) return c->fail(PBGPU_ERR_CAPACITY, "ray hash table overflow");
   return PBGPU_OK;
@@ -192,7 +192,7 @@ int run_markers(Context* c) {
   PBGPU_CUDA(c, cub::DeviceSelect::Flagged(c->tmp.get(), bytes, idx, flags.get(), sel.get(), nsel.get(), no, c->stream));
   c->launches += kCubSelectLaunches;
   int64_t nb = 0;
-  PBGPU_CUDA(c, cudaMemcpyAsync(&nb, nsel.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, readback(c, &nb, nsel.get(), sizeof(int64_t)));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   c->nb = nb;
   PBGPU_CUDA(c, c->border.alloc(nb > 0 ? nb : 1));

@@ -818,7 +818,7 @@ struct Builder {
     PBGPU_CUDA(c, ensure_tmp(c, bytes));
     PBGPU_CUDA(c, cub::DeviceScan::InclusiveSum(c->tmp.get(), bytes, cnt.get(), off.get(), m + 1, st()));
     c->launches += kCubScanLaunches;
-    PBGPU_CUDA(c, cudaMemcpyAsync(total, off.get() + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st()));
+    PBGPU_CUDA(c, readback(c, total, off.get() + m, sizeof(int64_t)));
     PBGPU_CUDA(c, cudaStreamSynchronize(st()));
     return PBGPU_OK;
   }
@@ -856,7 +856,7 @@ struct Builder {
     PBGPU_CUDA(c, ensure_tmp(c, bytes));
     PBGPU_CUDA(c, cub::DeviceSelect::Unique(c->tmp.get(), bytes, k2.get(), k.get(), nsel.get(), (int)m, st()));
     c->launches += kCubSelectLaunches;
-    PBGPU_CUDA(c, cudaMemcpyAsync(nu, nsel.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, st()));
+    PBGPU_CUDA(c, readback(c, nu, nsel.get(), sizeof(int64_t)));
     PBGPU_CUDA(c, cudaStreamSynchronize(st()));
     return PBGPU_OK;
   }
@@ -952,7 +952,7 @@ struct Builder {
     PBGPU_CUDA(c, cub::DeviceSelect::Flagged(c->tmp.get(), bytes, leaves.get(), marks.get(), parents.get(),
                                              nsel.get(), (int)n, st()));
     c->launches += kCubSelectLaunches;
-    PBGPU_CUDA(c, cudaMemcpyAsync(np, nsel.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, st()));
+    PBGPU_CUDA(c, readback(c, np, nsel.get(), sizeof(int64_t)));
     PBGPU_CUDA(c, leaves2.alloc(nn > 0 ? nn : 1));
     k_split_fill<<<grid_for(n, 256), 256, 0, st()>>>(leaves.get(), marks.get(), n, off.get(), leaves2.get());
     PBGPU_LAUNCHED(c);
@@ -981,7 +981,7 @@ struct Builder {
         PBGPU_LAUNCHED(c);
       }
       unsigned long long hm_ = 0;
-      PBGPU_CUDA(c, cudaMemcpyAsync(&hm_, nmark.get(), sizeof(hm_), cudaMemcpyDeviceToHost, st()));
+      PBGPU_CUDA(c, readback(c, &hm_, nmark.get(), sizeof(hm_)));
       PBGPU_CUDA(c, cudaStreamSynchronize(st()));
       if (hm_ == 0) return PBGPU_OK;
       int64_t np = 0;
@@ -1062,7 +1062,7 @@ struct Builder {
                                              (int)n, st()));
     c->launches += kCubSelectLaunches;
     int64_t nm = 0;
-    PBGPU_CUDA(c, cudaMemcpyAsync(&nm, nsel.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, st()));
+    PBGPU_CUDA(c, readback(c, &nm, nsel.get(), sizeof(int64_t)));
     PBGPU_CUDA(c, leaves2.alloc(nn > 0 ? nn : 1));
     k_merge_fill<<<grid_for(n, 256), 256, 0, st()>>>(leaves.get(), fam.get(), n, off.get(), leaves2.get());
     PBGPU_LAUNCHED(c);
@@ -1205,7 +1205,7 @@ extern "C" int pbgpu_build_mesh(pbgpu_ctx* h, const pbgpu_mesh_build* in) {
                                                             B.bad.get());
   PBGPU_LAUNCHED(c);
   int bad = 0;
-  PBGPU_CUDA(c, cudaMemcpyAsync(&bad, B.bad.get(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, readback(c, &bad, B.bad.get(), sizeof(int)));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   if (bad) return c->fail(PBGPU_ERR_STATE, "build_mesh: a corner or hanging parent is not an independent node");
   PBGPU_CUDA(c, c->oct.alloc(no));
@@ -1251,7 +1251,7 @@ extern "C" int pbgpu_build_mesh(pbgpu_ctx* h, const pbgpu_mesh_build* in) {
       PBGPU_CUDA(c, cub::DeviceSelect::Flagged(c->tmp.get(), bytes, idx, flag.get(), sel.get(), nsel.get(), (int)nk,
                                                c->stream));
       c->launches += kCubSelectLaunches;
-      PBGPU_CUDA(c, cudaMemcpyAsync(&ns, nsel.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+      PBGPU_CUDA(c, readback(c, &ns, nsel.get(), sizeof(int64_t)));
       PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     }
     PBGPU_CUDA(c, R.keys.alloc(ns > 0 ? ns : 1));
@@ -1264,7 +1264,7 @@ extern "C" int pbgpu_build_mesh(pbgpu_ctx* h, const pbgpu_mesh_build* in) {
       PBGPU_CUDA(c, cudaMemsetAsync(R.ptr.get(), 0, sizeof(int64_t), c->stream));
     }
     int64_t nc = 0;
-    if (nk > 0) PBGPU_CUDA(c, cudaMemcpyAsync(&nc, coff.get() + nk, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+    if (nk > 0) PBGPU_CUDA(c, readback(c, &nc, coff.get() + nk, sizeof(int64_t)));
     PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     R.n = ns;
     R.nc = nc;

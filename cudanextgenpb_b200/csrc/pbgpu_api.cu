@@ -50,7 +50,17 @@ cudaMemPool_t device_pool() {
     props.location.id = dev;
     if (cudaMemPoolCreate(&pool, &props) == cudaSuccess) {
       uint64_t threshold = UINT64_MAX;
-      if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold) != cudaSuccess) {
+      // Contexts on different streams share the pool.  By default the driver
+      // may hand one stream memory another stream freed and make the first
+      // wait for the second (internal dependencies), which chains concurrent
+      // requests together; here memory moves between streams only once its
+      // free is known to be complete.  PBGPU_POOL_CROSS_STREAM=1 restores the
+      // driver's default.
+      const char* cross = std::getenv("PBGPU_POOL_CROSS_STREAM");
+      int reuse = (cross && cross[0] == '1') ? 1 : 0;
+      if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold) != cudaSuccess ||
+          cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &reuse) != cudaSuccess ||
+          cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowOpportunistic, &reuse) != cudaSuccess) {
         cudaMemPoolDestroy(pool);
         pool = nullptr;
       }
@@ -167,7 +177,8 @@ int pbgpu_ctx_create(pbgpu_ctx** out, int device, void* cuda_stream) {
     c->own_stream = true;
   }
   if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaMallocHost(&c->ks_host, sizeof(KrylovScalars)) != cudaSuccess) {
+      cudaMallocHost(&c->ks_host, sizeof(KrylovScalars)) != cudaSuccess ||
+      cudaMallocHost(&c->rb_host, kReadbackBytes) != cudaSuccess) {
     pbgpu_ctx_destroy(h);
     return PBGPU_ERR_CUDA;
   }
@@ -185,6 +196,7 @@ void pbgpu_ctx_destroy(pbgpu_ctx* h) {
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ks_host) cudaFreeHost(c->ks_host);
+  if (c->rb_host) cudaFreeHost(c->rb_host);
   delete h;  // DBuf destructors free device memory (pool buffers on the stream)
   if (st) cudaStreamSynchronize(st);
   if (own && st) cudaStreamDestroy(st);
@@ -257,7 +269,7 @@ static const char* kInputErrMsg[kNumInputErr] = {
 // Waits for the stream and reports the first input check that failed.
 static int input_errors(Context* c, const int* d_err) {
   int h[kNumInputErr];
-  PBGPU_CUDA(c, cudaMemcpyAsync(h, d_err, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  PBGPU_CUDA(c, readback(c, h, d_err, sizeof(h)));
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   for (int k = 0; k < kNumInputErr; ++k)
     if (h[k]) return c->fail(PBGPU_ERR_ARG, kInputErrMsg[k]);

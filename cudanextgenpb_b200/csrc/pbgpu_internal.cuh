@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -185,12 +186,20 @@ enum ScratchSlot {
   kScAsmOvf, kScAsmK0, kScAsmK1, kScAsmId0, kScAsmElems, kScAsmNnz, kScAsmCond, kScAsmKd, kScAsmFr,
   kScKrBad, kScKrRh32, kScKrV32, kScKrS32, kScKrT32, kScKrPh32, kScKrSh32,
   kScEnPhi, kScEnQ, kScEnAcc, kScEnUsed, kScEnSlotRay, kScEnSel, kScEnNsel, kScEnNextra, kScEnXp, kScEnXd,
-  kScEnP, kScEnD, kScPfAtoms, kScPfPart, kScPfOut,
+  kScEnP, kScEnD, kScEnXk, kScEnXk2, kScEnXi, kScEnXi2, kScPfAtoms, kScPfPart, kScPfOut,
   kScInOctXyz, kScInOctLvl, kScInNodeXyz, kScInHangNp, kScInHangPar, kScInErr,
   kScratchSlots
 };
 
 struct Context;
+
+// Small device-to-host reads (counts, totals, flags, block partials) go
+// through the context's pinned scratch and wait for its stream.  A copy into
+// pageable memory is staged by the driver through buffers that the threads of
+// the process share, which serialised the set-up of requests running on
+// concurrent worker contexts.  Larger reads copy directly.
+constexpr size_t kReadbackBytes = 65536;
+inline cudaError_t readback(Context* c, void* dst, const void* src, size_t bytes);
 
 // A typed view of one scratch slot with DBuf's alloc() / get() interface.
 template <typename T>
@@ -291,6 +300,7 @@ struct Context {
   DBuf<double> partials;     // block partial sums
   DBuf<KrylovScalars> ks;
   KrylovScalars* ks_host = nullptr;   // pinned mirror
+  void* rb_host = nullptr;            // pinned scratch of small device-to-host reads (readback)
   DBuf<double> phi;          // node order
   bool have_phi = false;
   int sm_count = 148;
@@ -326,10 +336,22 @@ struct Context {
   }
 };
 
+inline cudaError_t readback(Context* c, void* dst, const void* src, size_t bytes) {
+  if (!c->rb_host || bytes > kReadbackBytes) {
+    const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+    return e != cudaSuccess ? e : cudaStreamSynchronize(c->stream);
+  }
+  cudaError_t e = cudaMemcpyAsync(c->rb_host, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) std::memcpy(dst, c->rb_host, bytes);
+  return e;
+}
+
 template <typename T>
 Scratch<T>::Scratch(Context* c, int which) : slot(&c->scratch[which]) {}
 
 int cuda_fail(Context* c, cudaError_t e, const char* what);
+
 
 #define PBGPU_STR2(x) #x
 #define PBGPU_STR(x) PBGPU_STR2(x)
