@@ -9,8 +9,11 @@
 //
 // Every step restates the host build (host/octree.cpp, host/surface.cpp,
 // host/pb_class.cpp) with the same expressions, so the GPU and host meshes are
-// identical: leaves stay in Morton order; leaf lookups are binary searches on
-// the sorted Morton keys; refinement splits marked leaves in place and
+// identical: leaves stay in Morton order; the hanging-corner and 2:1 balance
+// kernels find neighbor cells in a hash table of the leaves (Morton key and
+// level -> leaf index; the leaf containing a point is the one cell of level
+// <= l found by probing the levels downward), the other lookups by binary
+// search on the sorted Morton keys; refinement splits marked leaves in place and
 // restores 2:1 balance by ripple iterations from the split parents (refine)
 // or the merged parents (coarsen); rays are cast through the spheres of one
 // 2D bin per ray, the intervals sorted by (lo, hi) and merged.  Compiled
@@ -59,10 +62,75 @@ struct Tree {
   int4* leaves;
   uint64_t* keys;
   int64_t n;
+  const uint64_t* hk;  // open-addressing table of (Morton key << 5 | level) of every leaf, or null
+  const int32_t* hv;   // the leaf's index in each used slot of hk
+  int cap_log;         // the table's capacity is 2^cap_log
 };
 
+__device__ __forceinline__ uint64_t leaf_hash_key(int32_t x, int32_t y, int32_t z, int level) {
+  return (morton3((uint32_t)x, (uint32_t)y, (uint32_t)z) << 5) | (uint64_t)level;
+}
+
+// inserts every leaf and its index into the table (capacity at least twice
+// the leaves; keys are distinct, one per leaf)
+__global__ void k_leaf_hash(const int4* __restrict__ leaves, int64_t n, uint64_t* __restrict__ hk,
+                            int32_t* __restrict__ hv, int cap_log) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 q = leaves[i];
+  const uint64_t key = leaf_hash_key(q.x, q.y, q.z, q.w);
+  const uint64_t mask = (1ull << cap_log) - 1;
+  uint64_t s = hash_slot(key, cap_log);
+  for (uint64_t probe = 0; probe <= mask; ++probe) {
+    const unsigned long long prev =
+        atomicCAS(reinterpret_cast<unsigned long long*>(hk + s), (unsigned long long)kEmptyKey, (unsigned long long)key);
+    if (prev == kEmptyKey) {
+      hv[s] = (int32_t)i;
+      return;
+    }
+    s = (s + 1) & mask;
+  }
+}
+
+// index of the leaf of `level` with lower corner (x, y, z), or -1
+__device__ __forceinline__ int64_t leaf_index(const Tree& t, int32_t x, int32_t y, int32_t z, int level) {
+  const uint64_t key = leaf_hash_key(x, y, z, level);
+  const uint64_t mask = (1ull << t.cap_log) - 1;
+  uint64_t s = hash_slot(key, t.cap_log);
+  for (uint64_t probe = 0; probe <= mask; ++probe) {
+    const uint64_t k = t.hk[s];
+    if (k == key) return t.hv[s];
+    if (k == kEmptyKey) return -1;
+    s = (s + 1) & mask;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ bool leaf_in_hash(const Tree& t, int32_t x, int32_t y, int32_t z, int level) {
+  return leaf_index(t, x, y, z, level) >= 0;
+}
+
+// index of the leaf that contains the point (x, y, z) when that leaf's level
+// is at most lmax, else -1 (the containing leaf is finer): one probe per
+// level, from lmax down, as exactly one leaf contains the point
+__device__ __forceinline__ int64_t containing_leaf_upto(const Tree& t, int32_t x, int32_t y, int32_t z, int lmax) {
+  if (t.hk) {
+    for (int l = lmax; l >= 0; --l) {
+      const int32_t m = ~(qsize(l) - 1);
+      const int64_t j = leaf_index(t, x & m, y & m, z & m, l);
+      if (j >= 0) return j;
+    }
+    return -1;
+  }
+  const int64_t j = find_leaf(t.keys, t.n, x, y, z);
+  return t.leaves[j].w <= lmax ? j : -1;
+}
+
+// is the cell of `level` with lower corner (x, y, z) (aligned to that level) a
+// leaf: a table probe when the tree has its table, else a binary search
 __device__ __forceinline__ bool is_leaf_at(const Tree& t, int32_t x, int32_t y, int32_t z, int level) {
   if (!inside_root(x, y, z)) return false;
+  if (t.hk) return leaf_in_hash(t, x, y, z, level);
   return t.leaves[find_leaf(t.keys, t.n, x, y, z)].w == level;
 }
 
@@ -456,7 +524,7 @@ __device__ bool touches_too_fine(const Tree& t, const int4 X) {
             for (int k = 0; k < nopt[2]; ++k) {
               const int32_t sx = opts[0][i], sy = opts[1][j], sz = opts[2][k];
               if (!inside_root(sx, sy, sz)) continue;
-              if (t.leaves[find_leaf(t.keys, t.n, sx, sy, sz)].w > X.w + 1) return true;
+              if (containing_leaf_upto(t, sx, sy, sz, X.w + 1) < 0) return true;
             }
       }
   return false;
@@ -474,8 +542,8 @@ __global__ void k_balance_coarse(Tree t, const int4* __restrict__ seeds, int64_t
         if (!dx && !dy && !dz) continue;
         const int32_t nx = P.x + dx * sz, ny = P.y + dy * sz, nz = P.z + dz * sz;
         if (!inside_root(nx, ny, nz)) continue;
-        const int64_t j = find_leaf(t.keys, t.n, nx, ny, nz);
-        if (t.leaves[j].w < P.w) {
+        const int64_t j = containing_leaf_upto(t, nx, ny, nz, P.w - 1);
+        if (j >= 0) {
           // byte flags: mark once, count the first marker
           unsigned* word = reinterpret_cast<unsigned*>(marks + (j & ~int64_t(3)));
           const unsigned bit = 1u << (8 * (j & 3));
@@ -489,9 +557,15 @@ __global__ void k_balance_fine(Tree t, const int4* __restrict__ seeds, int64_t n
   const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= ns) return;
   const int4 X = seeds[s];
-  const int64_t j = find_leaf(t.keys, t.n, X.x, X.y, X.z);
-  const int4 L = t.leaves[j];
-  if (L.w != X.w || L.x != X.x || L.y != X.y || L.z != X.z) return;  // no longer a leaf
+  int64_t j;
+  if (t.hk) {
+    j = leaf_index(t, X.x, X.y, X.z, X.w);
+    if (j < 0) return;  // no longer a leaf
+  } else {
+    j = find_leaf(t.keys, t.n, X.x, X.y, X.z);
+    const int4 L = t.leaves[j];
+    if (L.w != X.w || L.x != X.x || L.y != X.y || L.z != X.z) return;  // no longer a leaf
+  }
   if (touches_too_fine(t, X)) {
     unsigned* word = reinterpret_cast<unsigned*>(marks + (j & ~int64_t(3)));
     const unsigned bit = 1u << (8 * (j & 3));
@@ -806,7 +880,30 @@ struct Builder {
   DBuf<unsigned long long> nmark;
   DBuf<int> bad;
 
-  Tree tree() { return Tree{leaves.get(), keys.get(), n}; }
+  // table of the current leaves for exact-cell lookups (k_hanging), rebuilt
+  // on first use after the tree changes
+  DBuf<uint64_t> lhash;
+  DBuf<int32_t> lhval;
+  int lhash_log = 0;
+  bool lhash_ok = false;
+
+  Tree tree() { return Tree{leaves.get(), keys.get(), n, nullptr, nullptr, 0}; }
+
+  int hashed_tree(Tree* t) {
+    if (!lhash_ok) {
+      int lg = 4;
+      while ((int64_t(1) << lg) < 2 * n) ++lg;
+      PBGPU_CUDA(c, lhash.alloc(size_t(1) << lg));
+      PBGPU_CUDA(c, lhval.alloc(size_t(1) << lg));
+      PBGPU_CUDA(c, cudaMemsetAsync(lhash.get(), 0xff, (size_t(1) << lg) * sizeof(uint64_t), st()));
+      k_leaf_hash<<<grid_for(n, 256), 256, 0, st()>>>(leaves.get(), n, lhash.get(), lhval.get(), lg);
+      PBGPU_LAUNCHED(c);
+      lhash_log = lg;
+      lhash_ok = true;
+    }
+    *t = Tree{leaves.get(), keys.get(), n, lhash.get(), lhval.get(), lhash_log};
+    return PBGPU_OK;
+  }
   cudaStream_t st() const { return c->stream; }
 
   int fail_cuda(cudaError_t e, const char* what) { return cuda_fail(c, e, what); }
@@ -830,6 +927,7 @@ struct Builder {
   }
 
   int rekey() {
+    lhash_ok = false;
     PBGPU_CUDA(c, keys.alloc(n > 0 ? n : 1));
     k_tree_keys<<<grid_for(n, 256), 256, 0, st()>>>(leaves.get(), n, keys.get());
     PBGPU_LAUNCHED(c);
@@ -904,7 +1002,10 @@ struct Builder {
 
   int hanging() {
     PBGPU_CUDA(c, hm.alloc(n > 0 ? n : 1));
-    k_hanging<<<grid_for(n, 128), 128, 0, st()>>>(tree(), hm.get());
+    Tree t;
+    const int rc = hashed_tree(&t);
+    if (rc != PBGPU_OK) return rc;
+    k_hanging<<<grid_for(n, 128), 128, 0, st()>>>(t, hm.get());
     PBGPU_LAUNCHED(c);
     return PBGPU_OK;
   }
@@ -972,12 +1073,14 @@ struct Builder {
       PBGPU_CUDA(c, marks.alloc((n + 3) & ~int64_t(3)));
       PBGPU_CUDA(c, cudaMemsetAsync(marks.get(), 0, (n + 3) & ~int64_t(3), st()));
       PBGPU_CUDA(c, cudaMemsetAsync(nmark.get(), 0, sizeof(unsigned long long), st()));
+      Tree ht;
+      if ((rc = hashed_tree(&ht)) != PBGPU_OK) return rc;
       if (nc > 0) {
-        k_balance_coarse<<<grid_for(nc, 128), 128, 0, st()>>>(tree(), coarse.get(), nc, marks.get(), nmark.get());
+        k_balance_coarse<<<grid_for(nc, 128), 128, 0, st()>>>(ht, coarse.get(), nc, marks.get(), nmark.get());
         PBGPU_LAUNCHED(c);
       }
       if (nf > 0) {
-        k_balance_fine<<<grid_for(nf, 128), 128, 0, st()>>>(tree(), fine.get(), nf, marks.get(), nmark.get());
+        k_balance_fine<<<grid_for(nf, 128), 128, 0, st()>>>(ht, fine.get(), nf, marks.get(), nmark.get());
         PBGPU_LAUNCHED(c);
       }
       unsigned long long hm_ = 0;

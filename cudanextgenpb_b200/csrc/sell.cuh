@@ -19,11 +19,14 @@ constexpr int kSpmvMinBlocksWide = 4;
 // registers: 6 blocks, 48 warps per SM, to keep more gathers in flight.
 // G = 8 names the same G = 4 layout walked two groups per iteration (all
 // index and value loads of both groups issued before the first gather): half
-// the dependent load round trips per 8-wide row; bounded to 6 blocks it also
-// compiles to 40 registers without spills (60 when left at 4 blocks)
+// the dependent load round trips per 8-wide row.  Bounded to 5 blocks it
+// compiles to 48 registers: measured on a 14.5 M DoF system, 0.494 ms per
+// SpMV against 0.526 at 4 blocks (60 registers, fewer warps) and 0.552 at 6
+// (40 registers: the compiler then issues the second group's loads after the
+// first group's gathers, as the one-group loop does)
 template <int G>
 __host__ __device__ constexpr int spmv_min_blocks() {
-  return G == 4 ? 6 : G == 8 ? 6 : kSpmvMinBlocks;
+  return G == 4 ? 6 : G == 8 ? 5 : kSpmvMinBlocks;
 }
 
 template <typename T>

@@ -131,3 +131,4 @@ def test_server_builds_request_meshes(pool, mode):
     for k, r in results.items():
         assert r["status"] == 0 and r["rel_residual"] <= 1e-10
         assert r["energy"]["sum"] == pytest.approx(pool[k][1], rel=1e-6)
+
