@@ -10,11 +10,12 @@
 // independent nodes behind each local corner (a hanging corner over its parents
 // with weight 1/num_parents: A = P^T K P).  Pass 1 counts each row's distinct
 // columns, the SELL layout is derived from those lengths (rows sorted by length
-// inside windows of sigma rows, slices of C rows padded to a multiple of 4
-// columns), pass 2 writes values and columns in SELL numbering.  Dirichlet
+// inside windows of sigma rows, slices of C rows as wide as their longest
+// row), pass 2 writes values and columns in SELL numbering.  Dirichlet
 // nodes become identity rows and are eliminated from the other rows into the
 // right-hand side, which keeps the matrix symmetric.
 #include <algorithm>
+#include <cstdlib>
 #include <cub/cub.cuh>
 
 #include "pbgpu_internal.cuh"
@@ -401,7 +402,8 @@ __global__ void k_iperm(const int32_t* __restrict__ perm, int64_t n, int32_t* __
 }
 
 __global__ void k_slice_width(const int32_t* __restrict__ perm, const int32_t* __restrict__ rowlen, int64_t n,
-                              int64_t n_slices, int C, int G, int32_t* __restrict__ w, int64_t* __restrict__ elems) {
+                              int64_t n_slices, int C, int G, bool pad, int32_t* __restrict__ w,
+                              int64_t* __restrict__ elems) {
   const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= n_slices) return;
   int mx = 1;
@@ -409,9 +411,16 @@ __global__ void k_slice_width(const int32_t* __restrict__ perm, const int32_t* _
     const int64_t p = s * C + l;
     if (p < n) mx = max(mx, rowlen[perm[p]]);
   }
-  mx = (mx + G - 1) / G * G;  // padded to whole groups: the SpMV then needs no tail loop
+  if (pad) mx = (mx + G - 1) / G * G;  // padded to whole groups: no tail columns
   w[s] = mx;
   elems[s] = (int64_t)mx * C;
+}
+
+// Slice widths padded to a multiple of the group (PBGPU_SELL_PAD=1), or the
+// last W mod G columns of a slice stored one per lane with no padding.
+static bool sell_pad() {
+  const char* e = std::getenv("PBGPU_SELL_PAD");
+  return e && e[0] == '1';
 }
 
 // The assembly's view of a context (dirichlet / gval must be current).
@@ -505,7 +514,7 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   PBGPU_CUDA(c, elems.alloc(n_slices + 1));
   PBGPU_CUDA(c, cudaMemsetAsync(elems.get(), 0, (n_slices + 1) * sizeof(int64_t), c->stream));
   k_slice_width<<<grid_for(n_slices, 128), 128, 0, c->stream>>>(c->perm.get(), c->rowlen.get(), n, n_slices, C, G,
-                                                                 c->slice_w.get(), elems.get());
+                                                                 sell_pad(), c->slice_w.get(), elems.get());
   PBGPU_LAUNCHED(c);
   size_t bytes = 0;
   PBGPU_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, bytes, elems.get(), c->slice_ptr.get(), n_slices + 1, c->stream));

@@ -274,6 +274,7 @@ __global__ void k_cg_update(int64_t n, T* __restrict__ x, T* __restrict__ r, con
   }
   if (grid_sum<3>(v, partials, &ks->ticket[2]) && threadIdx.x == 0) {
     ks->iter += 1;
+    ks->fold = 0;  // the last p-update has folded the previous correction
     ks->rr = v[1];
     ks->r1 = v[2];
     if (!finite(v[0]) || !finite(v[1])) {
@@ -296,36 +297,48 @@ __global__ void k_cg_update(int64_t n, T* __restrict__ x, T* __restrict__ r, con
 // ---------------------------------------------------------------------------
 // Reliable updates of the FP32 CG (mixed precision): once its recursive
 // residual has fallen by delta since the last FP64 residual (or meets the
-// target), the FP32 correction is added to the FP64 solution, b - A x is
-// recomputed in FP64 and the CG continues from it with its search direction,
-// so it needs the iterations of FP64 CG.  Both kernels return at once unless
-// an update is due.
-__global__ void k_ru_apply(int64_t n, double* __restrict__ x, float* __restrict__ d, const KrylovScalars* ks) {
-  if (ks->done || !ks->ru) return;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    x[i] += (double)d[i];
-    d[i] = 0.f;
+// target), b - A (x + d) is computed in FP64 with the FP32 correction d, CG
+// continues from it keeping its search direction, and the p-update of the
+// same iteration folds d into x (x += d, d = 0), so the solve needs the
+// iterations of FP64 CG and one kernel per iteration more than it (the
+// residual, which returns at once unless an update is due).
+
+// y_p = sum_j A(p, j) (x_j + d_j) in the order of sell_row, x_j + d_j formed
+// first (the value x_j takes once d is folded in)
+__device__ __forceinline__ double sell_row_sum(const SellT<double>& A, int64_t p, const double* __restrict__ x,
+                                               const float* __restrict__ d) {
+  const int64_t s = p / A.C;
+  const int lane = (int)(p - s * A.C);
+  const int W = A.slice_w[s];
+  const int64_t sb = A.slice_ptr[s];
+  double acc = 0.0;
+  for (int j = 0; j < W; ++j) {
+    const int64_t k = sell_elem(sb, W, A.C, A.G, lane, j);
+    const int32_t c = __ldcs(A.scol + k);
+    acc += __ldcs(A.sval + k) * (x[c] + (double)d[c]);
   }
+  return acc;
 }
 
-template <int G>
 __global__ void __launch_bounds__(kBlock, kSpmvMinBlocksWide)
     k_ru_residual(SellT<double> A, int64_t n, const double* __restrict__ b, const double* __restrict__ x,
-                  float* __restrict__ r32, const float* __restrict__ dinv32, KrylovScalars* ks, double* partials) {
+                  const float* __restrict__ d, float* __restrict__ r32, const float* __restrict__ dinv32,
+                  KrylovScalars* ks, double* partials) {
   if (ks->done || !ks->ru) return;
   double a[3] = {0.0, 0.0, 0.0};
-  spmv_direct_rows<double, G>(A, x, [&](int64_t i, double y) {
-    const double ri = i < n ? b[i] - y : 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_pad; i += (int64_t)gridDim.x * blockDim.x) {
+    const double ri = i < n ? b[i] - sell_row_sum(A, i, x, d) : 0.0;
     const float rf = (float)ri;
     r32[i] = rf;
     a[0] += ri * ri;
     a[1] += (double)rf * (double)(dinv32[i] * rf);
     a[2] += fabs(ri);
-  });
+  }
   if (grid_sum<3>(a, partials, &ks->ticket[7]) && threadIdx.x == 0) {
     ks->rr = a[0];
     ks->r1 = a[2];
     ks->ru = 0;
+    ks->fold = 1;
     if (!finite(a[0]) || !finite(a[1])) {
       ks->status = PBGPU_BREAKDOWN;
       ks->done = 1;
@@ -338,6 +351,22 @@ __global__ void __launch_bounds__(kBlock, kSpmvMinBlocksWide)
       ks->beta = a[1] / ks->rz;
       ks->rz = a[1];
       ks->rr_ref = a[0];
+    }
+  }
+}
+
+// p = Dinv r + beta p (FP32, Jacobi), and x += d, d = 0 after an FP64 residual
+__global__ void k_cg_pupdate_fold(int64_t n, float* __restrict__ p, const float* __restrict__ r,
+                                  const float* __restrict__ dinv, double* __restrict__ x, float* __restrict__ d,
+                                  const KrylovScalars* ks) {
+  if (ks->done) return;
+  const float beta = (float)ks->beta;
+  const bool fold = ks->fold != 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    p[i] = dinv[i] * r[i] + beta * p[i];
+    if (fold) {
+      x[i] += (double)d[i];
+      d[i] = 0.f;
     }
   }
 }
@@ -1088,7 +1117,7 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
   int kernels_per_chunk = 0;
   for (int k = 0; k < check_every; ++k) {
     kernels_per_chunk += (method == PBGPU_CG ? 3 : method == PBGPU_CGS ? 4 : 5) + (bj ? (method == PBGPU_CG ? 1 : 2) : 0) +
-                         (K.x64 && method == PBGPU_CG ? 2 : 0);
+                         (K.x64 && method == PBGPU_CG ? 1 : 0);
     if (method == PBGPU_CG) {
       mark(k, 0, 0);
       if (tg)
@@ -1097,18 +1126,21 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
         k_cg_spmv<T, GW><<<Gs, kBlock, 0, c->stream>>>(K.A, K.p, K.q, ks, part);
       mark(k, 0, 1);
       k_cg_update<T><<<G, kBlock, 0, c->stream>>>(n, K.x, K.r, K.p, K.q, K.dinv, ks, part);
+      bool folded = false;
       if constexpr (std::is_same<T, float>::value) {
         if (K.x64) {
-          k_ru_apply<<<G, kBlock, 0, c->stream>>>(n, K.x64, K.x, ks);
-          switch (K.A64->G) {
-            case 1: k_ru_residual<1><<<wave_grid(c, (const void*)k_ru_residual<1>, K.A64->n_pad), kBlock, 0, c->stream>>>(*K.A64, K.n_rows, K.b64, K.x64, K.r, K.dinv, ks, part); break;
-            case 2: k_ru_residual<2><<<wave_grid(c, (const void*)k_ru_residual<2>, K.A64->n_pad), kBlock, 0, c->stream>>>(*K.A64, K.n_rows, K.b64, K.x64, K.r, K.dinv, ks, part); break;
-            default: k_ru_residual<4><<<wave_grid(c, (const void*)k_ru_residual<4>, K.A64->n_pad), kBlock, 0, c->stream>>>(*K.A64, K.n_rows, K.b64, K.x64, K.r, K.dinv, ks, part); break;
-          }
+          // the FP64 residual b - A (x + d) when an update is due, then the
+          // p-update that also folds d into x
+          k_ru_residual<<<wave_grid(c, (const void*)k_ru_residual, K.A64->n_pad), kBlock, 0, c->stream>>>(
+              *K.A64, K.n_rows, K.b64, K.x64, K.x, K.r, K.dinv, ks, part);
+          k_cg_pupdate_fold<<<G, kBlock, 0, c->stream>>>(n, K.p, K.r, K.dinv, K.x64, K.x, ks);
+          folded = true;
         }
       }
-      if (bj) bj_apply(K.r, K.z, true);
-      k_cg_pupdate<T><<<G, kBlock, 0, c->stream>>>(n, K.p, K.r, K.dinv, K.z, ks);
+      if (!folded) {
+        if (bj) bj_apply(K.r, K.z, true);
+        k_cg_pupdate<T><<<G, kBlock, 0, c->stream>>>(n, K.p, K.r, K.dinv, K.z, ks);
+      }
     } else if (method == PBGPU_CGS) {
       k_cgs_p<T><<<G, kBlock, 0, c->stream>>>(n, K.r, K.q, K.s, K.p, K.ph, K.dinv, ks);
       if (bj) bj_apply(K.p, K.ph, false);

@@ -9,11 +9,10 @@
 //
 // Every step restates the host build (host/octree.cpp, host/surface.cpp,
 // host/pb_class.cpp) with the same expressions, so the GPU and host meshes are
-// identical: leaves stay in Morton order; the hanging-corner and 2:1 balance
-// kernels find neighbor cells in a hash table of the leaves (Morton key and
-// level -> leaf index; the leaf containing a point is the one cell of level
-// <= l found by probing the levels downward), the other lookups by binary
-// search on the sorted Morton keys; refinement splits marked leaves in place and
+// identical: leaves stay in Morton order; the hanging-corner kernel finds
+// neighbor cells in a hash table of the leaves (Morton key and level -> leaf
+// index), the other lookups are binary searches on the sorted Morton keys;
+// refinement splits marked leaves in place and
 // restores 2:1 balance by ripple iterations from the split parents (refine)
 // or the merged parents (coarsen); rays are cast through the spheres of one
 // 2D bin per ray, the intervals sorted by (lo, hi) and merged.  Compiled
@@ -1073,8 +1072,9 @@ struct Builder {
       PBGPU_CUDA(c, marks.alloc((n + 3) & ~int64_t(3)));
       PBGPU_CUDA(c, cudaMemsetAsync(marks.get(), 0, (n + 3) & ~int64_t(3), st()));
       PBGPU_CUDA(c, cudaMemsetAsync(nmark.get(), 0, sizeof(unsigned long long), st()));
-      Tree ht;
-      if ((rc = hashed_tree(&ht)) != PBGPU_OK) return rc;
+      // binary searches here: the table would be rebuilt after every pass of
+      // the ripple, which measured slower than the searches it saves
+      const Tree ht = tree();
       if (nc > 0) {
         k_balance_coarse<<<grid_for(nc, 128), 128, 0, st()>>>(ht, coarse.get(), nc, marks.get(), nmark.get());
         PBGPU_LAUNCHED(c);

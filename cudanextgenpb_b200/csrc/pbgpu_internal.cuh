@@ -160,6 +160,7 @@ struct KrylovScalars {
   double r1, b1, tol1;    // ||r||_1, ||b||_1, tol_w ||b||_1 + tol (LIS conv_cond 2)
   int conv;               // 2: stop on the 1-norm rule, else on the 2-norm rule
   int ru;                 // FP32 CG with reliable updates: 1 while an FP64 residual is due
+  int fold;               // 1 from that FP64 residual until the next p-update has folded d into x
   int reliable;           // reliable updates on (the FP64 residual decides convergence)
   double rr_ref, delta2;  // ||r||^2 at the last FP64 residual; update when rr < delta2 rr_ref
   int iter, max_iter, done, status, s_conv;

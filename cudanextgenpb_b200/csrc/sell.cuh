@@ -51,11 +51,34 @@ struct V2<float> {
   using t = float2;
 };
 
+// The last W mod 4 columns of a G = 4 row (G = 2: W mod 2), stored one per
+// lane after the groups (a warp's loads of one tail column are contiguous):
+// all index and value loads first, then the gathers, in column order.
+template <typename T, int G>
+__device__ __forceinline__ void sell_tail(const SellT<T>& A, int lane, const T* __restrict__ x, int W, int64_t sb,
+                                          T& acc) {
+  constexpr int kMaxTail = G - 1;
+  const int Wg = W & ~(G - 1);
+  const int nt = W - Wg;
+  if (nt == 0) return;
+  const int64_t tb = sb + (int64_t)Wg * A.C + lane;
+  int32_t tc[kMaxTail];
+  T tv[kMaxTail];
+#pragma unroll
+  for (int j = 0; j < kMaxTail; ++j)
+    if (j < nt) {
+      tc[j] = __ldcs(A.scol + tb + (int64_t)j * A.C);
+      tv[j] = __ldcs(A.sval + tb + (int64_t)j * A.C);
+    }
+#pragma unroll
+  for (int j = 0; j < kMaxTail; ++j)
+    if (j < nt) acc += tv[j] * x[tc[j]];
+}
+
 // y_p = sum_j A(p, j) x_j for SELL row p, element j at sell_elem(): columns
 // in groups of G (one vector load per group, a warp's loads of one group
-// contiguous).  The assembly pads slice widths to a multiple of G, so there
-// are no tail columns (a tail loop costs the registers that keep 40 warps per
-// SM resident; the padded layout measured faster despite its extra bytes).
+// contiguous), then the tail columns of a slice whose width the assembly did
+// not pad to a multiple of G.
 // (W and sb: width and first element of the row's slice, lane: the row's
 // position in it)
 template <typename T, int G>
@@ -81,6 +104,7 @@ __device__ __forceinline__ T sell_row(const SellT<T>& A, int lane, const T* __re
       acc += v.x * x[c.x];
       acc += v.y * x[c.y];
     }
+    sell_tail<T, 2>(A, lane, x, W, sb, acc);
   } else if constexpr (G == 8) {
     // the G = 4 layout, two groups per iteration
     const int64_t base = sb + 4 * lane;
@@ -140,6 +164,7 @@ __device__ __forceinline__ T sell_row(const SellT<T>& A, int lane, const T* __re
         acc += v.w * x[c.w];
       }
     }
+    sell_tail<T, 4>(A, lane, x, W, sb, acc);
   } else {
     const int64_t base = sb + 4 * lane;
     const int64_t stride = 4 * (int64_t)A.C;
@@ -162,6 +187,7 @@ __device__ __forceinline__ T sell_row(const SellT<T>& A, int lane, const T* __re
         acc += v.w * x[c.w];
       }
     }
+    sell_tail<T, 4>(A, lane, x, W, sb, acc);
   }
   return acc;
 }

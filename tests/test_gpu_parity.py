@@ -505,3 +505,28 @@ def test_paired_spmv_agrees(monkeypatch, method, precision):
     assert np.linalg.norm(pa - pb) / np.linalg.norm(pb) < 1e-7
     assert abs(ia - ib) <= max(2, ib // (50 if method == "cg" else 5)), (ia, ib)
     g.close()
+
+
+@pytest.mark.parametrize("group,method,precision", [(4, "cg", "fp64"), (4, "cg", "mixed"), (4, "bicgstab", "fp64"),
+                                                    (2, "cg", "fp64")])
+def test_padded_and_unpadded_slices_agree(monkeypatch, group, method, precision):
+    """Slice widths padded to a multiple of the group (PBGPU_SELL_PAD=1) or
+    not (the default: the last W mod G columns stored one per lane): the same
+    matrix, and, since a padding entry only adds 0 * x to a row, bit-identical
+    solves."""
+    prob = CASES["mol150"]().build()
+    g = GpuPath().load(prob)
+    g.create_markers()
+    g.create_density_map()
+    res = {}
+    for pad in ("1", "0"):
+        monkeypatch.setenv("PBGPU_SELL_PAD", pad)
+        g.assemble(32, 2048, group)
+        st = g.solve(solver_opts(method, tol=1e-10, precision=precision))
+        assert st.status == 0
+        res[pad] = (g.system(), g.phi().copy(), st.iterations)
+    (s1, p1, i1), (s0, p0, i0) = res["1"], res["0"]
+    for a, b in zip(s1, s0):
+        assert np.array_equal(a, b)
+    assert i1 == i0 and np.array_equal(p1, p0)
+    g.close()
