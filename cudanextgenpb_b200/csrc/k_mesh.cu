@@ -1052,11 +1052,13 @@ struct Builder {
     PBGPU_CUDA(c, cub::DeviceSelect::Flagged(c->tmp.get(), bytes, leaves.get(), marks.get(), parents.get(),
                                              nsel.get(), (int)n, st()));
     c->launches += kCubSelectLaunches;
-    PBGPU_CUDA(c, readback(c, np, nsel.get(), sizeof(int64_t)));
+    // every split leaf becomes 8 and every other one stays: nn = n + 7 np,
+    // so the parents' count needs no read of its own; the fill and whatever
+    // reads the new leaves next are ordered on the stream
+    *np = (nn - n) / 7;
     PBGPU_CUDA(c, leaves2.alloc(nn > 0 ? nn : 1));
     k_split_fill<<<grid_for(n, 256), 256, 0, st()>>>(leaves.get(), marks.get(), n, off.get(), leaves2.get());
     PBGPU_LAUNCHED(c);
-    PBGPU_CUDA(c, cudaStreamSynchronize(st()));
     leaves.swap(leaves2);
     std::swap(leaves.acct, leaves2.acct);
     n = nn;
@@ -1164,12 +1166,11 @@ struct Builder {
     PBGPU_CUDA(c, cub::DeviceSelect::Flagged(c->tmp.get(), bytes, leaves.get(), fam.get(), merged.get(), nsel.get(),
                                              (int)n, st()));
     c->launches += kCubSelectLaunches;
-    int64_t nm = 0;
-    PBGPU_CUDA(c, readback(c, &nm, nsel.get(), sizeof(int64_t)));
+    // every family of 8 becomes its parent: nn = n - 7 nm
+    const int64_t nm = (n - nn) / 7;
     PBGPU_CUDA(c, leaves2.alloc(nn > 0 ? nn : 1));
     k_merge_fill<<<grid_for(n, 256), 256, 0, st()>>>(leaves.get(), fam.get(), n, off.get(), leaves2.get());
     PBGPU_LAUNCHED(c);
-    PBGPU_CUDA(c, cudaStreamSynchronize(st()));
     if (nm > 0) {
       k_parent_of<<<grid_for(nm, 256), 256, 0, st()>>>(merged.get(), nm);
       PBGPU_LAUNCHED(c);
