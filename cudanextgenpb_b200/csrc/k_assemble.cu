@@ -76,12 +76,37 @@ __device__ __forceinline__ int expand(int32_t nd, const AsmView& A, int32_t g[4]
   return np;
 }
 
-// Small sorted (column, value) accumulator held by one thread.
+// Threads per block of the row kernels; the shared-memory slot arrays below
+// are laid out for exactly this many threads (slot k of thread t at
+// [k * kAsmBlock + t], so the lanes of a warp hit distinct banks whichever
+// slots they are at).
+constexpr int kAsmBlock = 128;
+// The first pass writes each row's distinct columns, sorted, into a 128-byte
+// line of kColLine entries, of which the first kShRow may be used; rows of a
+// 2:1 balanced octree hold at most ~25.  A row with more is gathered into the
+// local-memory accumulator (kMaxRow slots) instead.
+// PBGPU_ASM_SLOTS=4 lowers both limits to 4, which sends most rows down that
+// path (for tests of it).
+constexpr int kColLine = 32;
+constexpr int kHashSlots = 64;  // per-thread hash set of the first pass (at most kColLine used)
+constexpr uint8_t kWideRow = 0xff;
+constexpr int kShRow = 28;
+constexpr int kShFew = 4;
+
+static bool asm_few_slots() {
+  const char* e = std::getenv("PBGPU_ASM_SLOTS");
+  return e && std::atoi(e) == kShFew;
+}
+
+// Sorted (column, value) accumulator of one thread in local memory, used only
+// for rows that overflow the shared-memory one.
 struct RowAcc {
   int32_t col[kMaxRow];
   double val[kMaxRow];
   int m = 0;
   bool overflow = false;
+  __device__ __forceinline__ int32_t c_at(int j) const { return col[j]; }
+  __device__ __forceinline__ double v_at(int j) const { return val[j]; }
   __device__ __forceinline__ void add(int32_t c, double v) {
     int j = m - 1;
     while (j >= 0 && col[j] > c) --j;
@@ -99,6 +124,37 @@ struct RowAcc {
     }
     col[j + 1] = c;
     val[j + 1] = v;
+    ++m;
+  }
+};
+
+// The same accumulator in shared memory (the right-hand-side-only gather).
+template <int K>
+struct ShAcc {
+  int32_t* col;  // this thread's slot 0; slot k at col[k * kAsmBlock]
+  double* val;
+  int m = 0;
+  bool overflow = false;
+  __device__ __forceinline__ int32_t c_at(int j) const { return col[j * kAsmBlock]; }
+  __device__ __forceinline__ double v_at(int j) const { return val[j * kAsmBlock]; }
+  __device__ __forceinline__ void add(int32_t c, double v) {
+    if (overflow) return;
+    int j = m - 1;
+    while (j >= 0 && col[j * kAsmBlock] > c) --j;
+    if (j >= 0 && col[j * kAsmBlock] == c) {
+      val[j * kAsmBlock] += v;
+      return;
+    }
+    if (m == K) {
+      overflow = true;
+      return;
+    }
+    for (int k = m - 1; k > j; --k) {
+      col[(k + 1) * kAsmBlock] = col[k * kAsmBlock];
+      val[(k + 1) * kAsmBlock] = val[k * kAsmBlock];
+    }
+    col[(j + 1) * kAsmBlock] = c;
+    val[(j + 1) * kAsmBlock] = v;
     ++m;
   }
 };
@@ -177,7 +233,8 @@ __device__ __forceinline__ void corner_edges(int a, int ed[3], int ax[3]) {
 
 // Gather row i of A and its right-hand side entry (before Dirichlet handling)
 // from the octants' local coefficients: A = P^T K P over the node's incidences.
-__device__ void gather_row(int64_t i, const AsmView& A, const LocalView& L, RowAcc& R, double& rhs) {
+template <class Acc>
+__device__ void gather_row(int64_t i, const AsmView& A, const LocalView& L, Acc& R, double& rhs) {
   rhs = 0.0;
   for (int64_t e = A.inc_ptr[i]; e < A.inc_ptr[i + 1]; ++e) {
     const uint32_t t = A.inc[e];
@@ -202,11 +259,14 @@ __device__ void gather_row(int64_t i, const AsmView& A, const LocalView& L, RowA
   }
 }
 
-// Sorted set of column ids held by one thread (pass 1 needs no values).
+// Sorted set of column ids held by one thread (pass 1 needs no values), in
+// local memory (kMaxRow slots, the overflow path) or in shared memory with the
+// slot layout of ShAcc.
 struct ColSet {
   int32_t col[kMaxRow];
   int m = 0;
   bool overflow = false;
+  __device__ __forceinline__ int32_t c_at(int j) const { return col[j]; }
   __device__ __forceinline__ void add(int32_t c) {
     int j = m - 1;
     while (j >= 0 && col[j] > c) --j;
@@ -221,7 +281,59 @@ struct ColSet {
   }
 };
 
-__device__ __forceinline__ void add_expanded(int32_t nd, const AsmView& A, ColSet& S) {
+// Set of column ids of one thread in shared memory: open addressing over
+// kHashSlots slots (empty = -1), at most `limit` (< kHashSlots) ids, so a
+// probe always ends at the id or at an empty slot.  One add is a hash and
+// usually one probe, whatever the row's length.
+struct HashSet {
+  int32_t* tab;  // this thread's slot 0; slot k at tab[k * kAsmBlock]
+  int limit;
+  int m = 0;
+  bool overflow = false;
+  __device__ __forceinline__ void clear() {
+#pragma unroll 8
+    for (int k = 0; k < kHashSlots; ++k) tab[k * kAsmBlock] = -1;
+  }
+  __device__ __forceinline__ void add(int32_t c) {
+    if (overflow) return;
+    uint32_t h = ((uint32_t)c * 2654435761u) >> (32 - 6);
+    for (;;) {
+      const int32_t v = tab[h * kAsmBlock];
+      if (v == c) return;
+      if (v < 0) {
+        if (m == limit) {
+          overflow = true;
+          return;
+        }
+        tab[h * kAsmBlock] = c;
+        ++m;
+        return;
+      }
+      h = (h + 1) & (kHashSlots - 1);
+    }
+  }
+  // moves the ids to slots 0 .. m-1 in ascending order (in place: the write
+  // position never passes the slot being read)
+  __device__ __forceinline__ void compact_sorted() {
+    int w = 0;
+    for (int k = 0; k < kHashSlots; ++k) {
+      const int32_t v = tab[k * kAsmBlock];
+      if (v < 0) continue;
+      int j = w - 1;
+      while (j >= 0 && tab[j * kAsmBlock] > v) {
+        tab[(j + 1) * kAsmBlock] = tab[j * kAsmBlock];
+        --j;
+      }
+      tab[(j + 1) * kAsmBlock] = v;
+      ++w;
+    }
+  }
+};
+static_assert(kHashSlots == 64 && kShRow <= kColLine && kColLine < kHashSlots,
+              "the hash takes the top 6 bits; a probe needs a free slot; a row fits its line");
+
+template <class Set>
+__device__ __forceinline__ void add_expanded(int32_t nd, const AsmView& A, Set& S) {
   if (nd < A.n) {
     S.add(nd);
     return;
@@ -236,15 +348,9 @@ __device__ __forceinline__ void add_expanded(int32_t nd, const AsmView& A, ColSe
   }
 }
 
-// Pass 1: number of stored columns of each row (topology only).
-__global__ void k_row_len(AsmView A, int32_t* __restrict__ rowlen, int* __restrict__ overflow) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
-  if (A.dirichlet[i]) {
-    rowlen[i] = 1;
-    return;
-  }
-  ColSet S;
+// Distinct columns of row i before Dirichlet elimination.
+template <class Set>
+__device__ __forceinline__ void row_columns(int64_t i, const AsmView& A, Set& S) {
   for (int64_t e = A.inc_ptr[i]; e < A.inc_ptr[i + 1]; ++e) {
     const uint32_t t = A.inc[e];
     const int64_t o = t >> 3;
@@ -252,11 +358,107 @@ __global__ void k_row_len(AsmView A, int32_t* __restrict__ rowlen, int* __restri
     add_expanded(A.oct_nodes[t], A, S);
     for (int d = 0; d < 3; ++d) add_expanded(A.oct_nodes[8 * o + (a ^ (1 << d))], A, S);
   }
-  if (S.overflow) atomicExch(overflow, 1);
-  int m = 0;
-  for (int j = 0; j < S.m; ++j) m += A.dirichlet[S.col[j]] ? 0 : 1;
-  rowlen[i] = m;
 }
+
+template <class Set>
+__device__ __forceinline__ int32_t live_columns(const Set& S, const AsmView& A) {
+  int32_t m = 0;
+  for (int j = 0; j < S.m; ++j) m += A.dirichlet[S.c_at(j)] ? 0 : 1;
+  return m;
+}
+
+// Pass 1 (topology only): each row's distinct columns before Dirichlet
+// elimination, sorted, into its line of `cols` (kColLine entries from
+// i * kColLine), their number into ucnt, and the number of stored columns
+// (Dirichlet columns removed) into rowlen.  A row with more than `limit`
+// distinct columns gets ucnt = kWideRow and is counted by the local-memory
+// set.  Thread k takes row order[k]: rows sorted by incidence count, so the
+// lanes of a warp walk incidence lists of one length.
+__global__ void __launch_bounds__(kAsmBlock) k_row_cols(AsmView A, const int32_t* __restrict__ order, int limit,
+                                                        int32_t* __restrict__ rowlen, int32_t* __restrict__ cols,
+                                                        uint8_t* __restrict__ ucnt, int* __restrict__ overflow) {
+  __shared__ int32_t s_tab[kHashSlots * kAsmBlock];
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= A.n) return;
+  const int64_t i = order[k];
+  if (A.dirichlet[i]) {
+    rowlen[i] = 1;
+    ucnt[i] = 0;
+    return;
+  }
+  HashSet S{s_tab + threadIdx.x, limit};
+  S.clear();
+  row_columns(i, A, S);
+  if (!S.overflow) {
+    S.compact_sorted();
+    int32_t* line = cols + i * kColLine;
+    int32_t live = 0;
+    for (int j = 0; j < S.m; ++j) {
+      const int32_t c = S.tab[j * kAsmBlock];
+      line[j] = c;
+      live += A.dirichlet[c] ? 0 : 1;
+    }
+    rowlen[i] = live;
+    ucnt[i] = (uint8_t)S.m;
+    return;
+  }
+  ColSet W;
+  row_columns(i, A, W);
+  if (W.overflow) atomicExch(overflow, 1);
+  rowlen[i] = live_columns(W, A);
+  ucnt[i] = kWideRow;
+}
+
+// Rows ordered by incidence count (keys of the ordering sort).
+__global__ void k_inc_count_keys(const int64_t* __restrict__ inc_ptr, int64_t n, uint8_t* __restrict__ key,
+                                 int32_t* __restrict__ id) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t c = inc_ptr[i + 1] - inc_ptr[i];
+  key[i] = (uint8_t)(c < 255 ? c : 255);
+  id[i] = (int32_t)i;
+}
+
+// Accumulator over a row's known sorted columns (the line pass 1 wrote),
+// staged in shared memory with the values: an add finds its column by binary
+// search and adds into the column's value slot.  The value slots start at
+// -0.0, so the first add leaves exactly its own value, and every column sums
+// its contributions in arrival order: the same values as the insertion
+// accumulators.
+struct LineAcc {
+  int32_t* col;  // this thread's slot 0; slot k at col[k * kAsmBlock]
+  double* val;
+  int m;
+  bool overflow = false;
+  __device__ __forceinline__ int32_t c_at(int j) const { return col[j * kAsmBlock]; }
+  __device__ __forceinline__ double v_at(int j) const { return val[j * kAsmBlock]; }
+  // the line is 128-byte aligned: four columns per 16-byte load
+  __device__ __forceinline__ void load(const int32_t* __restrict__ line) {
+    const int4* l4 = reinterpret_cast<const int4*>(line);
+    for (int j = 0; j < m; j += 4) {
+      const int4 q = __ldg(l4 + (j >> 2));
+      col[j * kAsmBlock] = q.x;
+      if (j + 1 < m) col[(j + 1) * kAsmBlock] = q.y;
+      if (j + 2 < m) col[(j + 2) * kAsmBlock] = q.z;
+      if (j + 3 < m) col[(j + 3) * kAsmBlock] = q.w;
+    }
+    for (int j = 0; j < m; ++j) val[j * kAsmBlock] = -0.0;
+  }
+  __device__ __forceinline__ void add(int32_t c, double v) {
+    int lo = 0, hi = m;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (col[mid * kAsmBlock] < c)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    if (lo < m && col[lo * kAsmBlock] == c)
+      val[lo * kAsmBlock] += v;
+    else
+      overflow = true;  // not in the line: cannot happen for lines of pass 1
+  }
+};
 
 struct SellOut {
   const int64_t* slice_ptr;
@@ -277,12 +479,40 @@ __device__ __forceinline__ int64_t sell_index(const SellOut& S, int64_t p, int W
   return sell_elem(S.slice_ptr[sl], W, S.C, S.G, (int)(p - sl * S.C), j);
 }
 
+// Row i (SELL position p, slice width W) from its accumulated entries:
+// Dirichlet columns go to the right-hand side, the others are stored in
+// ascending node order.  Returns the number of elements written.
+template <bool RHS_ONLY, class Acc>
+__device__ __forceinline__ int emit_row(const Acc& R, double rhs, int64_t p, int64_t i, int W, const AsmView& A,
+                                        const SellOut& S) {
+  int j = 0;
+  double diag = 1.0;
+  for (int u = 0; u < R.m; ++u) {
+    const int32_t cn = R.c_at(u);
+    const double v = R.v_at(u);
+    if (A.dirichlet[cn]) {
+      rhs -= v * A.gval[cn];
+      continue;
+    }
+    if (RHS_ONLY) continue;
+    if (cn == i) diag = v;
+    const int64_t k = sell_index(S, p, W, j++);
+    S.scol[k] = S.iperm[cn];
+    S.sval[k] = v;
+  }
+  S.b[p] = rhs;
+  if (!RHS_ONLY) S.dinv[p] = 1.0 / diag;
+  return j;
+}
+
 // Pass 2: values, columns (SELL numbering), right-hand side, 1/diagonal.
 // One thread per SELL position p < n (row perm[p]), so the 32 lanes of a warp
 // fill one slice and every store of element j is one contiguous warp store.
-// RHS_ONLY: the right-hand side alone (new charges on an assembled system).
-template <bool RHS_ONLY>
-__global__ void k_row_fill(AsmView A, LocalView L, SellOut S) {
+__global__ void __launch_bounds__(kAsmBlock) k_row_fill(AsmView A, LocalView L, SellOut S,
+                                                        const int32_t* __restrict__ cols,
+                                                        const uint8_t* __restrict__ ucnt) {
+  __shared__ int32_t s_col[kShRow * kAsmBlock];
+  __shared__ double s_val[kShRow * kAsmBlock];
   const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p >= A.n) return;
   const int64_t i = S.perm[p];
@@ -290,36 +520,60 @@ __global__ void k_row_fill(AsmView A, LocalView L, SellOut S) {
   int j = 0;
   if (A.dirichlet[i]) {
     S.b[p] = A.gval[i];
-    if (RHS_ONLY) return;
     const int64_t k = sell_index(S, p, W, j++);
     S.scol[k] = (int32_t)p;
     S.sval[k] = 1.0;
     S.dinv[p] = 1.0;
   } else {
-    RowAcc R;
+    const uint8_t m = ucnt[i];
+    bool done = false;
     double rhs;
-    gather_row(i, A, L, R, rhs);
-    double diag = 1.0;
-    for (int u = 0; u < R.m; ++u) {
-      const int32_t cn = R.col[u];
-      if (A.dirichlet[cn]) {
-        rhs -= R.val[u] * A.gval[cn];
-        continue;
+    if (m != kWideRow) {
+      LineAcc R{s_col + threadIdx.x, s_val + threadIdx.x, m};
+      R.load(cols + i * kColLine);
+      gather_row(i, A, L, R, rhs);
+      if (!R.overflow) {
+        j = emit_row<false>(R, rhs, p, i, W, A, S);
+        done = true;
       }
-      if (RHS_ONLY) continue;
-      if (cn == i) diag = R.val[u];
-      const int64_t k = sell_index(S, p, W, j++);
-      S.scol[k] = S.iperm[cn];
-      S.sval[k] = R.val[u];
     }
-    S.b[p] = rhs;
-    if (RHS_ONLY) return;
-    S.dinv[p] = 1.0 / diag;
+    if (!done) {
+      RowAcc Q;
+      gather_row(i, A, L, Q, rhs);
+      j = emit_row<false>(Q, rhs, p, i, W, A, S);
+    }
   }
   for (; j < W; ++j) {
     const int64_t k = sell_index(S, p, W, j);
     S.scol[k] = (int32_t)p;
     S.sval[k] = 0.0;
+  }
+}
+
+// The right-hand side alone (new charges on an assembled system): the
+// values are gathered again into a shared-memory insertion accumulator, for
+// the Dirichlet columns' elimination.
+template <int K>
+__global__ void __launch_bounds__(kAsmBlock) k_row_rhs(AsmView A, LocalView L, SellOut S) {
+  __shared__ int32_t s_col[K * kAsmBlock];
+  __shared__ double s_val[K * kAsmBlock];
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= A.n) return;
+  const int64_t i = S.perm[p];
+  const int W = S.slice_w[p / S.C];
+  if (A.dirichlet[i]) {
+    S.b[p] = A.gval[i];
+    return;
+  }
+  ShAcc<K> R{s_col + threadIdx.x, s_val + threadIdx.x};
+  double rhs;
+  gather_row(i, A, L, R, rhs);
+  if (!R.overflow) {
+    emit_row<true>(R, rhs, p, i, W, A, S);
+  } else {
+    RowAcc Q;
+    gather_row(i, A, L, Q, rhs);
+    emit_row<true>(Q, rhs, p, i, W, A, S);
   }
 }
 
@@ -478,9 +732,32 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   Scratch<int> ovf(c, kScAsmOvf);
   PBGPU_CUDA(c, ovf.alloc(1));
   PBGPU_CUDA(c, cudaMemsetAsync(ovf.get(), 0, sizeof(int), c->stream));
+  // pass 1 walks the rows in order of incidence count (a one-byte radix sort)
+  Scratch<uint8_t> okey(c, kScAsmOrdKey), okey2(c, kScAsmOrdKey2);
+  Scratch<int32_t> oid(c, kScAsmOrdId), ord(c, kScAsmOrd);
+  PBGPU_CUDA(c, okey.alloc(n));
+  PBGPU_CUDA(c, okey2.alloc(n));
+  PBGPU_CUDA(c, oid.alloc(n));
+  PBGPU_CUDA(c, ord.alloc(n));
+  k_inc_count_keys<<<grid_for(n, 256), 256, 0, c->stream>>>(c->inc_ptr.get(), n, okey.get(), oid.get());
+  PBGPU_LAUNCHED(c);
+  {
+    size_t ob = 0;
+    PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(nullptr, ob, okey.get(), okey2.get(), oid.get(), ord.get(), (int)n,
+                                                  0, 8, c->stream));
+    PBGPU_CUDA(c, ensure_tmp(c, ob));
+    PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(c->tmp.get(), ob, okey.get(), okey2.get(), oid.get(), ord.get(),
+                                                  (int)n, 0, 8, c->stream));
+    c->launches += cub_radix_launches(n, 8);
+  }
+  Scratch<int32_t> ucols(c, kScAsmCols);
+  Scratch<uint8_t> ucnt(c, kScAsmUcnt);
+  PBGPU_CUDA(c, ucols.alloc(n * kColLine));
+  PBGPU_CUDA(c, ucnt.alloc(n));
   // a row longer than kMaxRow keeps kMaxRow in rowlen and raises the flag,
   // which is read with the matrix size below, before any row is filled
-  k_row_len<<<grid_for(n, 128), 128, 0, c->stream>>>(A, c->rowlen.get(), ovf.get());
+  k_row_cols<<<grid_for(n, kAsmBlock), kAsmBlock, 0, c->stream>>>(A, ord.get(), asm_few_slots() ? kShFew : kShRow,
+                                                                  c->rowlen.get(), ucols.get(), ucnt.get(), ovf.get());
   PBGPU_LAUNCHED(c);
 
   // SELL-C-sigma permutation
@@ -552,8 +829,9 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   k_octant_local<<<grid_for(c->n_oct, 128), 128, 0, c->stream>>>(A, c->n_oct, ocond.get(), okd.get(), ofr.get());
   PBGPU_LAUNCHED(c);
   const LocalView L{ocond.get(), okd.get(), ofr.get()};
-  k_row_fill<false><<<grid_for(n, 128), 128, 0, c->stream>>>(A, L, S);
+  k_row_fill<<<grid_for(n, kAsmBlock), kAsmBlock, 0, c->stream>>>(A, L, S, ucols.get(), ucnt.get());
   PBGPU_LAUNCHED(c);
+  ucols.release();  // 128 B per row, needed by the fill alone (freed in stream order)
   if (n_pad > n) {
     k_pad_rows<<<grid_for(n_pad - n, 128), 128, 0, c->stream>>>(S, n, n_pad);
     PBGPU_LAUNCHED(c);
@@ -588,7 +866,10 @@ int run_rhs(Context* c) {
   k_octant_local<<<grid_for(c->n_oct, 128), 128, 0, c->stream>>>(A, c->n_oct, ocond.get(), okd.get(), ofr.get());
   PBGPU_LAUNCHED(c);
   const LocalView L{ocond.get(), okd.get(), ofr.get()};
-  k_row_fill<true><<<grid_for(n, 128), 128, 0, c->stream>>>(A, L, S);
+  if (asm_few_slots())
+    k_row_rhs<kShFew><<<grid_for(n, kAsmBlock), kAsmBlock, 0, c->stream>>>(A, L, S);
+  else
+    k_row_rhs<kShRow><<<grid_for(n, kAsmBlock), kAsmBlock, 0, c->stream>>>(A, L, S);
   PBGPU_LAUNCHED(c);
   return PBGPU_OK;
 }

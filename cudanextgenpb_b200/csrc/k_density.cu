@@ -6,6 +6,7 @@
 // octant, then corner; charge contributions sorted by atom, corner, parent), so
 // results are deterministic and, compiled without FMA contraction, equal bit for
 // bit to the sequential CPU restatement.
+#include <cstdlib>
 #include <cub/cub.cuh>
 
 #include "pbgpu_internal.cuh"
@@ -66,20 +67,47 @@ __global__ void k_inc_fill(const int32_t* __restrict__ oct_nodes, int64_t n8, in
   }
 }
 
-// Sort each node's incidence list (a handful of entries) ascending.
-__global__ void k_inc_sort(const int64_t* __restrict__ ptr, uint32_t* __restrict__ inc, int64_t n) {
+// Sort each node's incidence list ascending.  The lists hold 8 entries for
+// most nodes and a few dozen at most (parents of hanging nodes), so each
+// thread sorts its list in shared memory (slot k of thread t at
+// [k * kIncBlock + t], conflict-free across a warp) and writes it back once; a
+// longer list is sorted in place in global memory (PBGPU_ASM_SLOTS=4 sets 4
+// slots, which sends most lists down that path, for tests of it).
+constexpr int kIncBlock = 128;
+constexpr int kIncSh = 48;
+constexpr int kIncFew = 4;
+
+template <int K>
+__global__ void __launch_bounds__(kIncBlock) k_inc_sort(const int64_t* __restrict__ ptr, uint32_t* __restrict__ inc,
+                                                        int64_t n) {
+  __shared__ uint32_t s_inc[K * kIncBlock];
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int64_t b = ptr[i], e = ptr[i + 1];
-  for (int64_t k = b + 1; k < e; ++k) {
-    const uint32_t v = inc[k];
-    int64_t j = k - 1;
-    while (j >= b && inc[j] > v) {
-      inc[j + 1] = inc[j];
+  if (e - b > K) {
+    for (int64_t k = b + 1; k < e; ++k) {
+      const uint32_t v = inc[k];
+      int64_t j = k - 1;
+      while (j >= b && inc[j] > v) {
+        inc[j + 1] = inc[j];
+        --j;
+      }
+      inc[j + 1] = v;
+    }
+    return;
+  }
+  uint32_t* my = s_inc + threadIdx.x;
+  const int m = (int)(e - b);
+  for (int k = 0; k < m; ++k) {
+    const uint32_t v = inc[b + k];
+    int j = k - 1;
+    while (j >= 0 && my[j * kIncBlock] > v) {
+      my[(j + 1) * kIncBlock] = my[j * kIncBlock];
       --j;
     }
-    inc[j + 1] = v;
+    my[(j + 1) * kIncBlock] = v;
   }
+  for (int k = 0; k < m; ++k) inc[b + k] = my[k * kIncBlock];
 }
 
 int build_incidence(Context* c) {
@@ -106,7 +134,11 @@ int build_incidence(Context* c) {
   k_inc_fill<<<grid_for(n8, 256), 256, 0, c->stream>>>(c->oct_nodes.get(), n8, n, c->hang_par.get(), c->hang_np.get(),
                                                         c->inc_ptr.get(), cnt.get(), c->inc.get());
   PBGPU_LAUNCHED(c);
-  k_inc_sort<<<grid_for(n, 128), 128, 0, c->stream>>>(c->inc_ptr.get(), c->inc.get(), n);
+  const char* few = std::getenv("PBGPU_ASM_SLOTS");
+  if (few && std::atoi(few) == kIncFew)
+    k_inc_sort<kIncFew><<<grid_for(n, kIncBlock), kIncBlock, 0, c->stream>>>(c->inc_ptr.get(), c->inc.get(), n);
+  else
+    k_inc_sort<kIncSh><<<grid_for(n, kIncBlock), kIncBlock, 0, c->stream>>>(c->inc_ptr.get(), c->inc.get(), n);
   PBGPU_LAUNCHED(c);
   PBGPU_CUDA(c, cudaStreamSynchronize(c->stream));
   c->have_incidence = true;

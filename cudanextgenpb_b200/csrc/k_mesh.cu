@@ -18,6 +18,7 @@
 // 2D bin per ray, the intervals sorted by (lo, hi) and merged.  Compiled
 // without FMA contraction, so positions and normals are bit-identical.
 #include <cub/cub.cuh>
+#include <math_constants.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -281,23 +282,124 @@ __global__ void k_cast_fill(const uint64_t* __restrict__ keys, int64_t nk, int a
   }
 }
 
-// pass 3: sort each ray's intervals by (lo, hi), merge overlapping ones and
-// write the crossings (position, sphere) at twice the ray's offset
+// pass 3: sort each ray's intervals by (lo, hi), keeping the fill order of
+// equal ones, merge overlapping ones and write the crossings (position,
+// sphere) at twice the ray's offset.  One warp per ray: the intervals are
+// sorted in registers by a bitonic network on the key (lo, hi, fill index),
+// which gives the order of a stable insertion sort, then lane 0 merges them.
+// A ray of more than 128 intervals is sorted by lane 0 alone.
+
+__device__ __forceinline__ bool iv_less(double alo, double ahi, int aid, double blo, double bhi, int bid) {
+  return alo < blo || (alo == blo && (ahi < bhi || (ahi == bhi && aid < bid)));
+}
+
+template <int E>
+__device__ __forceinline__ void iv_cmp_swap(double (&lo)[E], double (&hi)[E], int (&id)[E], int e, int f, bool up) {
+  // positions e < f in this lane; ascending (up) keeps the smaller at e
+  const bool fl = iv_less(lo[f], hi[f], id[f], lo[e], hi[e], id[e]);
+  if (fl == up) {
+    const double tl = lo[e], th = hi[e];
+    const int ti = id[e];
+    lo[e] = lo[f];
+    hi[e] = hi[f];
+    id[e] = id[f];
+    lo[f] = tl;
+    hi[f] = th;
+    id[f] = ti;
+  }
+}
+
+// bitonic sort of 32 * E keys, element g = lane * E + e
+template <int E>
+__device__ __forceinline__ void warp_bitonic_iv(double (&lo)[E], double (&hi)[E], int (&id)[E], int lane) {
+  constexpr unsigned kFull = 0xffffffffu;
+  for (int k = 2; k <= 32 * E; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= E) {
+        const int lj = j / E;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int g = lane * E + e;
+          const double olo = __shfl_xor_sync(kFull, lo[e], lj);
+          const double ohi = __shfl_xor_sync(kFull, hi[e], lj);
+          const int oid = __shfl_xor_sync(kFull, id[e], lj);
+          const bool up = (g & k) == 0, lower = (g & j) == 0;
+          const bool other_less = iv_less(olo, ohi, oid, lo[e], hi[e], id[e]);
+          if (lower == up ? other_less : !other_less) {
+            lo[e] = olo;
+            hi[e] = ohi;
+            id[e] = oid;
+          }
+        }
+      } else if (j == 1) {
+#pragma unroll
+        for (int e = 0; e < E; e += 2) iv_cmp_swap<E>(lo, hi, id, e, e + 1, ((lane * E + e) & k) == 0);
+      } else if (E >= 4 && j == 2) {
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          if ((e & 2) == 0) iv_cmp_swap<E>(lo, hi, id, e, e + 2, ((lane * E + e) & k) == 0);
+      }
+    }
+  }
+}
+
+template <int E>
+__device__ __forceinline__ void warp_sort_ray(Interval* a, int m, int lane) {
+  double lo[E], hi[E];
+  int id[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int g = lane * E + e;
+    if (g < m) {
+      lo[e] = a[g].lo;
+      hi[e] = a[g].hi;
+      id[e] = g;
+    } else {
+      lo[e] = CUDART_INF;
+      hi[e] = CUDART_INF;
+      id[e] = 0x7fffffff;
+    }
+  }
+  warp_bitonic_iv<E>(lo, hi, id, lane);
+  Interval v[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e)
+    if (lane * E + e < m) v[e] = a[id[e]];
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < E; ++e)
+    if (lane * E + e < m) a[lane * E + e] = v[e];
+  __syncwarp();
+}
+
 __global__ void k_cast_merge(int64_t nk, const int64_t* __restrict__ off, Interval* __restrict__ iv,
                              double* __restrict__ xs, int32_t* __restrict__ xsph, int64_t* __restrict__ ncr) {
-  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (r >= nk) return;
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= nk) return;  // whole warps: blockDim is a multiple of 32
   Interval* a = iv + off[r];
   const int m = (int)(off[r + 1] - off[r]);
-  for (int i = 1; i < m; ++i) {  // insertion sort: a ray meets tens of spheres
-    const Interval e = a[i];
-    int j = i - 1;
-    while (j >= 0 && (a[j].lo > e.lo || (a[j].lo == e.lo && a[j].hi > e.hi))) {
-      a[j + 1] = a[j];
-      --j;
+  if (m > 128) {
+    if (lane == 0) {
+      for (int i = 1; i < m; ++i) {
+        const Interval e = a[i];
+        int j = i - 1;
+        while (j >= 0 && (a[j].lo > e.lo || (a[j].lo == e.lo && a[j].hi > e.hi))) {
+          a[j + 1] = a[j];
+          --j;
+        }
+        a[j + 1] = e;
+      }
     }
-    a[j + 1] = e;
+    __syncwarp();
+  } else if (m > 64) {
+    warp_sort_ray<4>(a, m, lane);
+  } else if (m > 32) {
+    warp_sort_ray<2>(a, m, lane);
+  } else if (m > 1) {
+    warp_sort_ray<1>(a, m, lane);
   }
+  if (lane != 0) return;
   int64_t w = 2 * off[r];
   int64_t nc = 0;
   if (m > 0) {
@@ -493,83 +595,80 @@ __global__ void k_split_fill(const int4* __restrict__ in, const uint8_t* __restr
     out[w + c] = make_int4(q.x + (c & 1) * h, q.y + ((c >> 1) & 1) * h, q.z + ((c >> 2) & 1) * h, q.w + 1);
 }
 
+// The balance kernels give each seed a group of kBalLanes lanes, which split
+// the seed's neighbour lookups (each a binary search over the leaf keys)
+// between them: on a small tree the grid is a fraction of one wave, and the
+// kernel takes as long as one thread's chain of dependent lookups.
+constexpr int kBalLanes = 8;
+
 // a leaf X is too coarse when a level-(l+1) cell touching it from outside is
-// itself refined (host touches_too_fine)
-__device__ bool touches_too_fine(const Tree& t, const int4 X) {
-  const int32_t S = qsize(X.w), h = S >> 1;
-  for (int dz = -1; dz <= 1; ++dz)
-    for (int dy = -1; dy <= 1; ++dy)
-      for (int dx = -1; dx <= 1; ++dx) {
-        if (!dx && !dy && !dz) continue;
-        const int d[3] = {dx, dy, dz};
-        const int32_t base[3] = {X.x, X.y, X.z};
-        int32_t opts[3][2];
-        int nopt[3];
-        for (int a = 0; a < 3; ++a) {
-          if (d[a] < 0) {
-            opts[a][0] = base[a] - h;
-            nopt[a] = 1;
-          } else if (d[a] > 0) {
-            opts[a][0] = base[a] + S;
-            nopt[a] = 1;
-          } else {
-            opts[a][0] = base[a];
-            opts[a][1] = base[a] + h;
-            nopt[a] = 2;
-          }
-        }
-        for (int i = 0; i < nopt[0]; ++i)
-          for (int j = 0; j < nopt[1]; ++j)
-            for (int k = 0; k < nopt[2]; ++k) {
-              const int32_t sx = opts[0][i], sy = opts[1][j], sz = opts[2][k];
-              if (!inside_root(sx, sy, sz)) continue;
-              if (containing_leaf_upto(t, sx, sy, sz, X.w + 1) < 0) return true;
-            }
-      }
+// itself refined (host touches_too_fine).  The cells to look at: per axis,
+// offset -h (the side below), 0 or h (alongside, two half cells) or S (the
+// side above), every combination but the 8 inside X, 56 in all; lane r of the
+// group looks at combinations r, r + kBalLanes, ...
+__device__ bool touches_too_fine_part(const Tree& t, const int4 X, int r) {
+  const int32_t h = qsize(X.w) >> 1;
+  for (int u = r; u < 64; u += kBalLanes) {
+    // offset (a - 1) h for a = 0 .. 3: -h, 0, h, S
+    const int a0 = u & 3, a1 = (u >> 2) & 3, a2 = (u >> 4) & 3;
+    if ((a0 == 1 || a0 == 2) && (a1 == 1 || a1 == 2) && (a2 == 1 || a2 == 2)) continue;
+    const int32_t sx = X.x + (a0 - 1) * h, sy = X.y + (a1 - 1) * h, sz = X.z + (a2 - 1) * h;
+    if (!inside_root(sx, sy, sz)) continue;
+    if (containing_leaf_upto(t, sx, sy, sz, X.w + 1) < 0) return true;
+  }
   return false;
+}
+
+__device__ __forceinline__ void mark_once(uint8_t* marks, int64_t j, unsigned long long* nmark) {
+  // byte flags: mark once, count the first marker
+  unsigned* word = reinterpret_cast<unsigned*>(marks + (j & ~int64_t(3)));
+  const unsigned bit = 1u << (8 * (j & 3));
+  if (!(atomicOr(word, bit) & bit)) atomicAdd(nmark, 1ull);
 }
 
 __global__ void k_balance_coarse(Tree t, const int4* __restrict__ seeds, int64_t ns, uint8_t* __restrict__ marks,
                                  unsigned long long* __restrict__ nmark) {
-  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t s = gt / kBalLanes;
+  const int r = (int)(gt % kBalLanes);
   if (s >= ns) return;
   const int4 P = seeds[s];
   const int32_t sz = qsize(P.w);
-  for (int dz = -1; dz <= 1; ++dz)
-    for (int dy = -1; dy <= 1; ++dy)
-      for (int dx = -1; dx <= 1; ++dx) {
-        if (!dx && !dy && !dz) continue;
-        const int32_t nx = P.x + dx * sz, ny = P.y + dy * sz, nz = P.z + dz * sz;
-        if (!inside_root(nx, ny, nz)) continue;
-        const int64_t j = containing_leaf_upto(t, nx, ny, nz, P.w - 1);
-        if (j >= 0) {
-          // byte flags: mark once, count the first marker
-          unsigned* word = reinterpret_cast<unsigned*>(marks + (j & ~int64_t(3)));
-          const unsigned bit = 1u << (8 * (j & 3));
-          if (!(atomicOr(word, bit) & bit)) atomicAdd(nmark, 1ull);
-        }
-      }
+  for (int u = r; u < 27; u += kBalLanes) {
+    if (u == 13) continue;  // the seed itself
+    const int dx = u % 3 - 1, dy = (u / 3) % 3 - 1, dz = u / 9 - 1;
+    const int32_t nx = P.x + dx * sz, ny = P.y + dy * sz, nz = P.z + dz * sz;
+    if (!inside_root(nx, ny, nz)) continue;
+    const int64_t j = containing_leaf_upto(t, nx, ny, nz, P.w - 1);
+    if (j >= 0) mark_once(marks, j, nmark);
+  }
 }
 
+// every lane of the grid reaches the group vote: the block size is a multiple
+// of 32 and kBalLanes divides 32, so groups never straddle warps
 __global__ void k_balance_fine(Tree t, const int4* __restrict__ seeds, int64_t ns, uint8_t* __restrict__ marks,
                                unsigned long long* __restrict__ nmark) {
-  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (s >= ns) return;
-  const int4 X = seeds[s];
-  int64_t j;
-  if (t.hk) {
-    j = leaf_index(t, X.x, X.y, X.z, X.w);
-    if (j < 0) return;  // no longer a leaf
-  } else {
-    j = find_leaf(t.keys, t.n, X.x, X.y, X.z);
-    const int4 L = t.leaves[j];
-    if (L.w != X.w || L.x != X.x || L.y != X.y || L.z != X.z) return;  // no longer a leaf
+  const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t s = gt / kBalLanes;
+  const int r = (int)(gt % kBalLanes);
+  bool active = s < ns;
+  int64_t j = -1;
+  int4 X = make_int4(0, 0, 0, 0);
+  if (active) {
+    X = seeds[s];
+    if (t.hk) {
+      j = leaf_index(t, X.x, X.y, X.z, X.w);
+      active = j >= 0;  // else no longer a leaf
+    } else {
+      j = find_leaf(t.keys, t.n, X.x, X.y, X.z);
+      const int4 L = t.leaves[j];
+      active = L.w == X.w && L.x == X.x && L.y == X.y && L.z == X.z;
+    }
   }
-  if (touches_too_fine(t, X)) {
-    unsigned* word = reinterpret_cast<unsigned*>(marks + (j & ~int64_t(3)));
-    const unsigned bit = 1u << (8 * (j & 3));
-    if (!(atomicOr(word, bit) & bit)) atomicAdd(nmark, 1ull);
-  }
+  const bool hit = active && touches_too_fine_part(t, X, r);
+  const unsigned group = ((1u << kBalLanes) - 1u) << ((threadIdx.x & 31) & ~(kBalLanes - 1));
+  const unsigned any = __ballot_sync(0xffffffffu, hit) & group;
+  if (any && r == 0) mark_once(marks, j, nmark);
 }
 
 __global__ void k_parent_of(int4* __restrict__ q, int64_t n) {
@@ -985,7 +1084,7 @@ struct Builder {
     PBGPU_CUDA(c, cudaMemcpyAsync(ioff.get(), off.get(), (nk + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice, st()));
     k_cast_fill<<<grid_for(nk, 128), 128, 0, st()>>>(rk, nk, axis, S, D, ioff.get(), iv.get());
     PBGPU_LAUNCHED(c);
-    k_cast_merge<<<grid_for(nk, 128), 128, 0, st()>>>(nk, ioff.get(), iv.get(), xs.get(), xsph.get(), ncr.get());
+    k_cast_merge<<<grid_for(32 * nk, 128), 128, 0, st()>>>(nk, ioff.get(), iv.get(), xs.get(), xsph.get(), ncr.get());
     PBGPU_LAUNCHED(c);
     PBGPU_CUDA(c, cudaMemcpyAsync(cnt.get(), ncr.get(), (nk + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice, st()));
     int64_t nc = 0;
@@ -1078,11 +1177,12 @@ struct Builder {
       // the ripple, which measured slower than the searches it saves
       const Tree ht = tree();
       if (nc > 0) {
-        k_balance_coarse<<<grid_for(nc, 128), 128, 0, st()>>>(ht, coarse.get(), nc, marks.get(), nmark.get());
+        k_balance_coarse<<<grid_for(nc * kBalLanes, 128), 128, 0, st()>>>(ht, coarse.get(), nc, marks.get(),
+                                                                           nmark.get());
         PBGPU_LAUNCHED(c);
       }
       if (nf > 0) {
-        k_balance_fine<<<grid_for(nf, 128), 128, 0, st()>>>(ht, fine.get(), nf, marks.get(), nmark.get());
+        k_balance_fine<<<grid_for(nf * kBalLanes, 128), 128, 0, st()>>>(ht, fine.get(), nf, marks.get(), nmark.get());
         PBGPU_LAUNCHED(c);
       }
       unsigned long long hm_ = 0;

@@ -185,6 +185,7 @@ enum ScratchSlot {
   kScMkOvf, kScMkFlags, kScMkSel, kScMkNsel,
   kScDenCnt, kScDenK0, kScDenK1, kScDenV0, kScDenV1,
   kScAsmOvf, kScAsmK0, kScAsmK1, kScAsmId0, kScAsmElems, kScAsmNnz, kScAsmCond, kScAsmKd, kScAsmFr,
+  kScAsmCols, kScAsmUcnt, kScAsmOrd, kScAsmOrdKey, kScAsmOrdKey2, kScAsmOrdId,
   kScKrBad, kScKrRh32, kScKrV32, kScKrS32, kScKrT32, kScKrPh32, kScKrSh32,
   kScEnPhi, kScEnQ, kScEnAcc, kScEnUsed, kScEnSlotRay, kScEnSel, kScEnNsel, kScEnNextra, kScEnXp, kScEnXd,
   kScEnP, kScEnD, kScEnXk, kScEnXk2, kScEnXi, kScEnXi2, kScPfAtoms, kScPfPart, kScPfOut,
@@ -214,6 +215,10 @@ struct Scratch {
     return e;
   }
   T* get() const { return p; }
+  void release() {
+    slot->release();
+    p = nullptr;
+  }
 };
 
 struct Context {

@@ -530,3 +530,30 @@ def test_padded_and_unpadded_slices_agree(monkeypatch, group, method, precision)
         assert np.array_equal(a, b)
     assert i1 == i0 and np.array_equal(p1, p0)
     g.close()
+
+
+def test_assembly_overflow_paths_agree(monkeypatch):
+    """The incidence sort and the row gathers keep each row in shared-memory
+    slots and fall back to global / local memory for a row that does not fit.
+    PBGPU_ASM_SLOTS=4 shrinks the slots so that most rows take the fallback:
+    the markers, density, matrix, right-hand side and the right-hand sides of
+    new charge vectors (the right-hand-side-only gather) agree bit for bit."""
+    from cudanextgenpb_b200 import solve_charges
+    prob = CASES["mol150"]().build()
+    pos, q, _ = prob.atoms()
+    Q = np.stack([q, q[::-1].copy()])
+    opts = solver_opts("cg", tol=1e-10)
+    res = {}
+    for slots in ("0", "4"):
+        monkeypatch.setenv("PBGPU_ASM_SLOTS", slots)
+        g = GpuPath().load(prob)
+        g.create_markers()
+        g.create_density_map()
+        g.assemble()
+        es, ss = solve_charges(g, Q, opts)
+        res[slots] = (g.density(), g.system(), [e["sum"] for e in es], [s.iterations for s in ss])
+        g.close()
+    (d0, s0, e0, i0), (d4, s4, e4, i4) = res["0"], res["4"]
+    for a, b in zip(d0 + s0, d4 + s4):
+        assert np.array_equal(a, b)
+    assert e0 == e4 and i0 == i4
