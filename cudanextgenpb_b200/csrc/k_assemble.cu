@@ -4,16 +4,19 @@
 // written straight into a SELL-C-sigma matrix.
 //
 // Each matrix row is gathered by one thread from the node's incidence list
-// (octant, corner), so no atomics touch the values.  Per incidence the thread
-// rebuilds the octant's local coefficients it needs (the corner's 3 edge
-// conductances, the lumped reaction, V/8 * rho) and spreads them over the
-// independent nodes behind each local corner (a hanging corner over its parents
-// with weight 1/num_parents: A = P^T K P).  Pass 1 counts each row's distinct
-// columns, the SELL layout is derived from those lengths (rows sorted by length
-// inside windows of sigma rows, slices of C rows as wide as their longest
-// row), pass 2 writes values and columns in SELL numbering.  Dirichlet
-// nodes become identity rows and are eliminated from the other rows into the
-// right-hand side, which keeps the matrix symmetric.
+// (octant, corner), so no atomics touch the values.  The octants' local
+// coefficients (12 edge conductances, 8 lumped diagonal terms, 8 V/8 * rho
+// terms) are computed once per octant; per incidence the thread spreads the
+// corner's terms over the independent nodes behind each local corner (a
+// hanging corner over its parents with weight 1/num_parents: A = P^T K P),
+// accumulating them in a per-thread hash map in shared memory.  Pass 1 runs
+// in node order, so the rows of a warp share octants, and writes each row's
+// distinct columns and values, sorted, into a line of its own; the SELL
+// layout is derived from the row lengths (rows sorted by length inside
+// windows of sigma rows, slices of C rows as wide as their longest row), and
+// pass 2 copies the lines in SELL order, so every store is a warp-wide one.
+// Dirichlet nodes become identity rows and are eliminated from the other rows
+// into the right-hand side, which keeps the matrix symmetric.
 #include <algorithm>
 #include <cstdlib>
 #include <cub/cub.cuh>
@@ -42,17 +45,24 @@ struct AsmView {
   double lo[3], len[3];
 };
 
+// v / np for a hanging node's parent count: 2 and 4 (the counts a 2:1 tree
+// has) are powers of two, so the product with 1/2 or 1/4 is the quotient
+// exactly, without the cost of a double division.
+__device__ __forceinline__ double div_np(double v, int np) {
+  return np == 2 ? v * 0.5 : np == 4 ? v * 0.25 : v / np;
+}
+
 __device__ __forceinline__ double corner_val(const double* __restrict__ v, int32_t nd, const AsmView& A) {
   if (nd < A.n) return v[nd];
   const int64_t h = nd - A.n;
   const int4 p = A.hang_par[h];
   const int np = A.hang_np[h];
   double t = 0.0;
-  t += v[p.x] / np;
-  t += v[p.y] / np;
+  t += div_np(v[p.x], np);
+  t += div_np(v[p.y], np);
   if (np == 4) {
-    t += v[p.z] / np;
-    t += v[p.w] / np;
+    t += div_np(v[p.z], np);
+    t += div_np(v[p.w], np);
   }
   return t;
 }
@@ -71,7 +81,7 @@ __device__ __forceinline__ int expand(int32_t nd, const AsmView& A, int32_t g[4]
   g[1] = p.y;
   g[2] = p.z;
   g[3] = p.w;
-  const double wi = 1.0 / np;
+  const double wi = div_np(1.0, np);
   for (int j = 0; j < 4; ++j) w[j] = wi;
   return np;
 }
@@ -81,17 +91,17 @@ __device__ __forceinline__ int expand(int32_t nd, const AsmView& A, int32_t g[4]
 // [k * kAsmBlock + t], so the lanes of a warp hit distinct banks whichever
 // slots they are at).
 constexpr int kAsmBlock = 128;
-// The first pass writes each row's distinct columns, sorted, into a 128-byte
-// line of kColLine entries, of which the first kShRow may be used; rows of a
-// 2:1 balanced octree hold at most ~25.  A row with more is gathered into the
-// local-memory accumulator (kMaxRow slots) instead.
-// PBGPU_ASM_SLOTS=4 lowers both limits to 4, which sends most rows down that
-// path (for tests of it).
-constexpr int kColLine = 32;
-constexpr int kHashSlots = 64;  // per-thread hash set of the first pass (at most kColLine used)
+// The gather pass writes each row's distinct columns, sorted, with their
+// values into lines of kLine entries; rows of a 2:1 balanced octree hold at
+// most ~25.  A row with more is gathered into the local-memory accumulator
+// (kMaxRow slots) instead, in both passes.  PBGPU_ASM_SLOTS=4 lowers the limit
+// to 4, which sends most rows down that path (for tests of it).
+constexpr int kLine = 28;
+constexpr int kHash = 32;  // hash slots per thread: more than kLine, so a probe always ends
+constexpr int kGatherNB = 4;  // incidences whose loads a gather issues together (measured: 2: 12.3 ms, 4: 11.6 ms)
 constexpr uint8_t kWideRow = 0xff;
-constexpr int kShRow = 28;
 constexpr int kShFew = 4;
+static_assert(kLine < kHash && (kHash & (kHash - 1)) == 0, "a probe needs a free slot");
 
 static bool asm_few_slots() {
   const char* e = std::getenv("PBGPU_ASM_SLOTS");
@@ -128,45 +138,16 @@ struct RowAcc {
   }
 };
 
-// The same accumulator in shared memory (the right-hand-side-only gather).
-template <int K>
-struct ShAcc {
-  int32_t* col;  // this thread's slot 0; slot k at col[k * kAsmBlock]
-  double* val;
-  int m = 0;
-  bool overflow = false;
-  __device__ __forceinline__ int32_t c_at(int j) const { return col[j * kAsmBlock]; }
-  __device__ __forceinline__ double v_at(int j) const { return val[j * kAsmBlock]; }
-  __device__ __forceinline__ void add(int32_t c, double v) {
-    if (overflow) return;
-    int j = m - 1;
-    while (j >= 0 && col[j * kAsmBlock] > c) --j;
-    if (j >= 0 && col[j * kAsmBlock] == c) {
-      val[j * kAsmBlock] += v;
-      return;
-    }
-    if (m == K) {
-      overflow = true;
-      return;
-    }
-    for (int k = m - 1; k > j; --k) {
-      col[(k + 1) * kAsmBlock] = col[k * kAsmBlock];
-      val[(k + 1) * kAsmBlock] = val[k * kAsmBlock];
-    }
-    col[(j + 1) * kAsmBlock] = c;
-    val[(j + 1) * kAsmBlock] = v;
-    ++m;
-  }
-};
-
 // Local box-method coefficients of every octant, computed once per octant
 // with the expressions (and accumulation order) of the local matrix: the 12
 // edge conductances wha(eps_i1, eps_i2, f) * area_h, the 8 diagonal entries
 // (sum of the corner's 3 conductances in edge order, then the lumped reaction
 // kappa_c * V/8 * w_c, w_c the product of the corner's half-edge shares), and
 // the 8 right-hand-side terms V/8 * rho_c.
-__global__ void k_octant_local(AsmView A, int64_t n_oct, double* __restrict__ cond, double* __restrict__ kd,
-                               double* __restrict__ fr) {
+// 8 blocks of 128 per SM (64 registers): measured faster than the 108-register
+// build at 4, its spills notwithstanding.
+__global__ void __launch_bounds__(128, 8) k_octant_local(AsmView A, int64_t n_oct, double* __restrict__ cond,
+                                                         double* __restrict__ kd, double* __restrict__ fr) {
   const int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (o >= n_oct) return;
   const int4 q = A.oct[o];
@@ -231,233 +212,177 @@ __device__ __forceinline__ void corner_edges(int a, int ed[3], int ax[3]) {
       }
 }
 
-// Gather row i of A and its right-hand side entry (before Dirichlet handling)
-// from the octants' local coefficients: A = P^T K P over the node's incidences.
-template <class Acc>
-__device__ void gather_row(int64_t i, const AsmView& A, const LocalView& L, Acc& R, double& rhs) {
-  rhs = 0.0;
-  for (int64_t e = A.inc_ptr[i]; e < A.inc_ptr[i + 1]; ++e) {
-    const uint32_t t = A.inc[e];
-    const int64_t o = t >> 3;
-    const int a = (int)(t & 7);
-    const int32_t nda = A.oct_nodes[t];
-    const double wa = nda < A.n ? 1.0 : 1.0 / A.hang_np[nda - A.n];
-    const double kaa = L.kd[t];
-    int ed[3], ax[3];
-    corner_edges(a, ed, ax);
-    int32_t g[4];
-    double w[4];
-    int ng = expand(nda, A, g, w);
-    for (int j = 0; j < ng; ++j) R.add(g[j], wa * kaa * w[j]);
-    for (int u = 0; u < 3; ++u) {
-      const int32_t ndb = A.oct_nodes[8 * o + (a ^ (1 << ax[u]))];
-      const double kab = 0.0 - L.cond[12 * o + ed[u]];
-      ng = expand(ndb, A, g, w);
-      for (int j = 0; j < ng; ++j) R.add(g[j], wa * kab * w[j]);
-    }
-    rhs += wa * L.fr[t];
+// One incidence's loads: the corner's node and its 3 edge neighbours, the
+// corner's diagonal term, the 3 edge conductances (negated) and V/8 rho.
+struct IncLoads {
+  int32_t nd[4];
+  double k[4];
+  double fr;
+};
+
+__device__ __forceinline__ void load_inc(uint32_t t, const AsmView& A, const LocalView& L, IncLoads& d) {
+  const int64_t o = t >> 3;
+  const int a = (int)(t & 7);
+  int ed[3], ax[3];
+  corner_edges(a, ed, ax);
+  d.nd[0] = A.oct_nodes[t];
+  d.k[0] = L.kd[t];
+  d.fr = L.fr[t];
+#pragma unroll
+  for (int u = 0; u < 3; ++u) {
+    d.nd[1 + u] = A.oct_nodes[8 * o + (a ^ (1 << ax[u]))];
+    d.k[1 + u] = 0.0 - L.cond[12 * o + ed[u]];
   }
 }
 
-// Sorted set of column ids held by one thread (pass 1 needs no values), in
-// local memory (kMaxRow slots, the overflow path) or in shared memory with the
-// slot layout of ShAcc.
-struct ColSet {
-  int32_t col[kMaxRow];
-  int m = 0;
-  bool overflow = false;
-  __device__ __forceinline__ int32_t c_at(int j) const { return col[j]; }
-  __device__ __forceinline__ void add(int32_t c) {
-    int j = m - 1;
-    while (j >= 0 && col[j] > c) --j;
-    if (j >= 0 && col[j] == c) return;
-    if (m == kMaxRow) {
-      overflow = true;
-      return;
-    }
-    for (int k = m - 1; k > j; --k) col[k + 1] = col[k];
-    col[j + 1] = c;
-    ++m;
+template <class Acc>
+__device__ __forceinline__ void apply_inc(const IncLoads& d, const AsmView& A, Acc& R, double& rhs) {
+  const double wa = d.nd[0] < A.n ? 1.0 : div_np(1.0, A.hang_np[d.nd[0] - A.n]);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    int32_t g[4];
+    double w[4];
+    const int ng = expand(d.nd[r], A, g, w);
+    for (int j = 0; j < ng; ++j) R.add(g[j], wa * d.k[r] * w[j]);
   }
-};
+  rhs += wa * d.fr;
+}
 
-// Set of column ids of one thread in shared memory: open addressing over
-// kHashSlots slots (empty = -1), at most `limit` (< kHashSlots) ids, so a
-// probe always ends at the id or at an empty slot.  One add is a hash and
-// usually one probe, whatever the row's length.
-struct HashSet {
-  int32_t* tab;  // this thread's slot 0; slot k at tab[k * kAsmBlock]
+// Gather row i of A and its right-hand side entry (before Dirichlet handling)
+// from the octants' local coefficients: A = P^T K P over the node's
+// incidences, in incidence order (for each, the corner's own term, then its 3
+// edges in ascending edge id, each spread over the independent nodes behind
+// the node it reaches).  The loads of NB incidences are issued before any of
+// them is accumulated.
+template <int NB, class Acc>
+__device__ void gather_row(int64_t i, const AsmView& A, const LocalView& L, Acc& R, double& rhs) {
+  rhs = 0.0;
+  const int64_t e0 = A.inc_ptr[i], e1 = A.inc_ptr[i + 1];
+  for (int64_t e = e0; e < e1; e += NB) {
+    IncLoads d[NB];
+#pragma unroll
+    for (int q = 0; q < NB; ++q) load_inc(A.inc[e + q < e1 ? e + q : e], A, L, d[q]);
+#pragma unroll
+    for (int q = 0; q < NB; ++q)
+      if (e + q < e1) apply_inc(d[q], A, R, rhs);
+  }
+}
+
+// (column, value) map of one thread in shared memory: open addressing over
+// kHash slots (empty key = -1), at most `limit` (<= kLine) columns.  An add is
+// a hash and usually one probe; a column's first add stores its value and
+// later ones add to it, so each column sums its contributions in arrival
+// order, exactly as the insertion accumulator does.
+struct HashMap {
+  int32_t* key;  // this thread's slot 0; slot k at key[k * kAsmBlock]
+  double* val;
   int limit;
   int m = 0;
   bool overflow = false;
   __device__ __forceinline__ void clear() {
 #pragma unroll 8
-    for (int k = 0; k < kHashSlots; ++k) tab[k * kAsmBlock] = -1;
+    for (int k = 0; k < kHash; ++k) key[k * kAsmBlock] = -1;
   }
-  __device__ __forceinline__ void add(int32_t c) {
+  __device__ __forceinline__ void add(int32_t c, double v) {
     if (overflow) return;
-    uint32_t h = ((uint32_t)c * 2654435761u) >> (32 - 6);
+    uint32_t h = ((uint32_t)c * 2654435761u) >> 27;  // top 5 bits: kHash = 32
     for (;;) {
-      const int32_t v = tab[h * kAsmBlock];
-      if (v == c) return;
-      if (v < 0) {
+      const int32_t k = key[h * kAsmBlock];
+      if (k == c) {
+        val[h * kAsmBlock] += v;
+        return;
+      }
+      if (k < 0) {
         if (m == limit) {
           overflow = true;
           return;
         }
-        tab[h * kAsmBlock] = c;
+        key[h * kAsmBlock] = c;
+        val[h * kAsmBlock] = v;
         ++m;
         return;
       }
-      h = (h + 1) & (kHashSlots - 1);
+      h = (h + 1) & (kHash - 1);
     }
   }
-  // moves the ids to slots 0 .. m-1 in ascending order (in place: the write
-  // position never passes the slot being read)
+  // moves the entries to slots 0 .. m-1 in ascending column order (in place:
+  // the write position never passes the slot being read)
   __device__ __forceinline__ void compact_sorted() {
     int w = 0;
-    for (int k = 0; k < kHashSlots; ++k) {
-      const int32_t v = tab[k * kAsmBlock];
-      if (v < 0) continue;
+    for (int s = 0; s < kHash; ++s) {
+      const int32_t k = key[s * kAsmBlock];
+      if (k < 0) continue;
+      const double v = val[s * kAsmBlock];
       int j = w - 1;
-      while (j >= 0 && tab[j * kAsmBlock] > v) {
-        tab[(j + 1) * kAsmBlock] = tab[j * kAsmBlock];
+      while (j >= 0 && key[j * kAsmBlock] > k) {
+        key[(j + 1) * kAsmBlock] = key[j * kAsmBlock];
+        val[(j + 1) * kAsmBlock] = val[j * kAsmBlock];
         --j;
       }
-      tab[(j + 1) * kAsmBlock] = v;
+      key[(j + 1) * kAsmBlock] = k;
+      val[(j + 1) * kAsmBlock] = v;
       ++w;
     }
   }
 };
-static_assert(kHashSlots == 64 && kShRow <= kColLine && kColLine < kHashSlots,
-              "the hash takes the top 6 bits; a probe needs a free slot; a row fits its line");
+static_assert(kHash == 32, "HashMap::add takes the top 5 bits of the product");
 
-template <class Set>
-__device__ __forceinline__ void add_expanded(int32_t nd, const AsmView& A, Set& S) {
-  if (nd < A.n) {
-    S.add(nd);
-    return;
-  }
-  const int64_t h = nd - A.n;
-  const int4 p = A.hang_par[h];
-  S.add(p.x);
-  S.add(p.y);
-  if (A.hang_np[h] == 4) {
-    S.add(p.z);
-    S.add(p.w);
-  }
-}
-
-// Distinct columns of row i before Dirichlet elimination.
-template <class Set>
-__device__ __forceinline__ void row_columns(int64_t i, const AsmView& A, Set& S) {
-  for (int64_t e = A.inc_ptr[i]; e < A.inc_ptr[i + 1]; ++e) {
-    const uint32_t t = A.inc[e];
-    const int64_t o = t >> 3;
-    const int a = (int)(t & 7);
-    add_expanded(A.oct_nodes[t], A, S);
-    for (int d = 0; d < 3; ++d) add_expanded(A.oct_nodes[8 * o + (a ^ (1 << d))], A, S);
-  }
-}
-
-template <class Set>
-__device__ __forceinline__ int32_t live_columns(const Set& S, const AsmView& A) {
-  int32_t m = 0;
-  for (int j = 0; j < S.m; ++j) m += A.dirichlet[S.c_at(j)] ? 0 : 1;
-  return m;
-}
-
-// Pass 1 (topology only): each row's distinct columns before Dirichlet
-// elimination, sorted, into its line of `cols` (kColLine entries from
-// i * kColLine), their number into ucnt, and the number of stored columns
-// (Dirichlet columns removed) into rowlen.  A row with more than `limit`
-// distinct columns gets ucnt = kWideRow and is counted by the local-memory
-// set.  Thread k takes row order[k]: rows sorted by incidence count, so the
-// lanes of a warp walk incidence lists of one length.
-__global__ void __launch_bounds__(kAsmBlock) k_row_cols(AsmView A, const int32_t* __restrict__ order, int limit,
-                                                        int32_t* __restrict__ rowlen, int32_t* __restrict__ cols,
-                                                        uint8_t* __restrict__ ucnt, int* __restrict__ overflow) {
-  __shared__ int32_t s_tab[kHashSlots * kAsmBlock];
-  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (k >= A.n) return;
-  const int64_t i = order[k];
+// Pass 1: one thread per row in node order (neighbouring rows share octants,
+// so their gathers meet in L1).  Each row's distinct columns, sorted, and
+// their values (before Dirichlet elimination) go to its lines of `cols` and
+// `vals` (kLine entries from i * kLine), their number to ucnt, the sum of its
+// V/8 rho terms to rhs_part, and, unless rowlen is null (right-hand side
+// only), the number of stored columns (Dirichlet columns removed) to rowlen.
+// A row with more than `limit` columns gets ucnt = kWideRow and is gathered
+// again by the second pass.
+template <int NB>
+__global__ void __launch_bounds__(kAsmBlock) k_row_gather(AsmView A, LocalView L, int limit,
+                                                          int32_t* __restrict__ rowlen, int32_t* __restrict__ cols,
+                                                          double* __restrict__ vals, double* __restrict__ rhs_part,
+                                                          uint8_t* __restrict__ ucnt, int* __restrict__ overflow) {
+  __shared__ int32_t s_key[kHash * kAsmBlock];
+  __shared__ double s_val[kHash * kAsmBlock];
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
   if (A.dirichlet[i]) {
-    rowlen[i] = 1;
+    if (rowlen) rowlen[i] = 1;
     ucnt[i] = 0;
     return;
   }
-  HashSet S{s_tab + threadIdx.x, limit};
-  S.clear();
-  row_columns(i, A, S);
-  if (!S.overflow) {
-    S.compact_sorted();
-    int32_t* line = cols + i * kColLine;
-    int32_t live = 0;
-    for (int j = 0; j < S.m; ++j) {
-      const int32_t c = S.tab[j * kAsmBlock];
-      line[j] = c;
+  HashMap R{s_key + threadIdx.x, s_val + threadIdx.x, limit};
+  R.clear();
+  double rhs;
+  gather_row<NB>(i, A, L, R, rhs);
+  int32_t live = 0;
+  if (!R.overflow) {
+    R.compact_sorted();
+    int32_t* cl = cols + i * kLine;
+    double* vl = vals + i * kLine;
+    for (int j = 0; j < R.m; ++j) {
+      const int32_t c = R.key[j * kAsmBlock];
+      cl[j] = c;
+      vl[j] = R.val[j * kAsmBlock];
       live += A.dirichlet[c] ? 0 : 1;
     }
-    rowlen[i] = live;
-    ucnt[i] = (uint8_t)S.m;
-    return;
+    ucnt[i] = (uint8_t)R.m;
+    rhs_part[i] = rhs;
+  } else {
+    RowAcc Q;
+    gather_row<1>(i, A, L, Q, rhs);
+    if (Q.overflow) atomicExch(overflow, 1);
+    for (int j = 0; j < Q.m; ++j) live += A.dirichlet[Q.col[j]] ? 0 : 1;
+    ucnt[i] = kWideRow;
   }
-  ColSet W;
-  row_columns(i, A, W);
-  if (W.overflow) atomicExch(overflow, 1);
-  rowlen[i] = live_columns(W, A);
-  ucnt[i] = kWideRow;
+  if (rowlen) rowlen[i] = live;
 }
 
-// Rows ordered by incidence count (keys of the ordering sort).
-__global__ void k_inc_count_keys(const int64_t* __restrict__ inc_ptr, int64_t n, uint8_t* __restrict__ key,
-                                 int32_t* __restrict__ id) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int64_t c = inc_ptr[i + 1] - inc_ptr[i];
-  key[i] = (uint8_t)(c < 255 ? c : 255);
-  id[i] = (int32_t)i;
-}
-
-// Accumulator over a row's known sorted columns (the line pass 1 wrote),
-// staged in shared memory with the values: an add finds its column by binary
-// search and adds into the column's value slot.  The value slots start at
-// -0.0, so the first add leaves exactly its own value, and every column sums
-// its contributions in arrival order: the same values as the insertion
-// accumulators.
-struct LineAcc {
-  int32_t* col;  // this thread's slot 0; slot k at col[k * kAsmBlock]
-  double* val;
+// A row's lines as an accumulator view for emit_row.
+struct LineView {
+  const int32_t* col;
+  const double* val;
   int m;
-  bool overflow = false;
-  __device__ __forceinline__ int32_t c_at(int j) const { return col[j * kAsmBlock]; }
-  __device__ __forceinline__ double v_at(int j) const { return val[j * kAsmBlock]; }
-  // the line is 128-byte aligned: four columns per 16-byte load
-  __device__ __forceinline__ void load(const int32_t* __restrict__ line) {
-    const int4* l4 = reinterpret_cast<const int4*>(line);
-    for (int j = 0; j < m; j += 4) {
-      const int4 q = __ldg(l4 + (j >> 2));
-      col[j * kAsmBlock] = q.x;
-      if (j + 1 < m) col[(j + 1) * kAsmBlock] = q.y;
-      if (j + 2 < m) col[(j + 2) * kAsmBlock] = q.z;
-      if (j + 3 < m) col[(j + 3) * kAsmBlock] = q.w;
-    }
-    for (int j = 0; j < m; ++j) val[j * kAsmBlock] = -0.0;
-  }
-  __device__ __forceinline__ void add(int32_t c, double v) {
-    int lo = 0, hi = m;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if (col[mid * kAsmBlock] < c)
-        lo = mid + 1;
-      else
-        hi = mid;
-    }
-    if (lo < m && col[lo * kAsmBlock] == c)
-      val[lo * kAsmBlock] += v;
-    else
-      overflow = true;  // not in the line: cannot happen for lines of pass 1
-  }
+  __device__ __forceinline__ int32_t c_at(int j) const { return __ldg(col + j); }
+  __device__ __forceinline__ double v_at(int j) const { return __ldg(val + j); }
 };
 
 struct SellOut {
@@ -505,14 +430,17 @@ __device__ __forceinline__ int emit_row(const Acc& R, double rhs, int64_t p, int
   return j;
 }
 
-// Pass 2: values, columns (SELL numbering), right-hand side, 1/diagonal.
-// One thread per SELL position p < n (row perm[p]), so the 32 lanes of a warp
-// fill one slice and every store of element j is one contiguous warp store.
-__global__ void __launch_bounds__(kAsmBlock) k_row_fill(AsmView A, LocalView L, SellOut S,
+// Pass 2: values, columns (SELL numbering), right-hand side, 1/diagonal, from
+// the lines of pass 1.  One thread per SELL position p < n (row perm[p]), so
+// the 32 lanes of a warp fill one slice and every store of element j is one
+// contiguous warp store.  RHS_ONLY: the right-hand side alone (new charges on
+// an assembled system).
+template <bool RHS_ONLY>
+__global__ void __launch_bounds__(kAsmBlock) k_row_emit(AsmView A, LocalView L, SellOut S,
                                                         const int32_t* __restrict__ cols,
+                                                        const double* __restrict__ vals,
+                                                        const double* __restrict__ rhs_part,
                                                         const uint8_t* __restrict__ ucnt) {
-  __shared__ int32_t s_col[kShRow * kAsmBlock];
-  __shared__ double s_val[kShRow * kAsmBlock];
   const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p >= A.n) return;
   const int64_t i = S.perm[p];
@@ -520,60 +448,28 @@ __global__ void __launch_bounds__(kAsmBlock) k_row_fill(AsmView A, LocalView L, 
   int j = 0;
   if (A.dirichlet[i]) {
     S.b[p] = A.gval[i];
+    if (RHS_ONLY) return;
     const int64_t k = sell_index(S, p, W, j++);
     S.scol[k] = (int32_t)p;
     S.sval[k] = 1.0;
     S.dinv[p] = 1.0;
   } else {
     const uint8_t m = ucnt[i];
-    bool done = false;
-    double rhs;
     if (m != kWideRow) {
-      LineAcc R{s_col + threadIdx.x, s_val + threadIdx.x, m};
-      R.load(cols + i * kColLine);
-      gather_row(i, A, L, R, rhs);
-      if (!R.overflow) {
-        j = emit_row<false>(R, rhs, p, i, W, A, S);
-        done = true;
-      }
-    }
-    if (!done) {
+      const LineView R{cols + i * kLine, vals + i * kLine, m};
+      j = emit_row<RHS_ONLY>(R, rhs_part[i], p, i, W, A, S);
+    } else {
       RowAcc Q;
-      gather_row(i, A, L, Q, rhs);
-      j = emit_row<false>(Q, rhs, p, i, W, A, S);
+      double rhs;
+      gather_row<1>(i, A, L, Q, rhs);
+      j = emit_row<RHS_ONLY>(Q, rhs, p, i, W, A, S);
     }
+    if (RHS_ONLY) return;
   }
   for (; j < W; ++j) {
     const int64_t k = sell_index(S, p, W, j);
     S.scol[k] = (int32_t)p;
     S.sval[k] = 0.0;
-  }
-}
-
-// The right-hand side alone (new charges on an assembled system): the
-// values are gathered again into a shared-memory insertion accumulator, for
-// the Dirichlet columns' elimination.
-template <int K>
-__global__ void __launch_bounds__(kAsmBlock) k_row_rhs(AsmView A, LocalView L, SellOut S) {
-  __shared__ int32_t s_col[K * kAsmBlock];
-  __shared__ double s_val[K * kAsmBlock];
-  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (p >= A.n) return;
-  const int64_t i = S.perm[p];
-  const int W = S.slice_w[p / S.C];
-  if (A.dirichlet[i]) {
-    S.b[p] = A.gval[i];
-    return;
-  }
-  ShAcc<K> R{s_col + threadIdx.x, s_val + threadIdx.x};
-  double rhs;
-  gather_row(i, A, L, R, rhs);
-  if (!R.overflow) {
-    emit_row<true>(R, rhs, p, i, W, A, S);
-  } else {
-    RowAcc Q;
-    gather_row(i, A, L, Q, rhs);
-    emit_row<true>(Q, rhs, p, i, W, A, S);
   }
 }
 
@@ -732,32 +628,27 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   Scratch<int> ovf(c, kScAsmOvf);
   PBGPU_CUDA(c, ovf.alloc(1));
   PBGPU_CUDA(c, cudaMemsetAsync(ovf.get(), 0, sizeof(int), c->stream));
-  // pass 1 walks the rows in order of incidence count (a one-byte radix sort)
-  Scratch<uint8_t> okey(c, kScAsmOrdKey), okey2(c, kScAsmOrdKey2);
-  Scratch<int32_t> oid(c, kScAsmOrdId), ord(c, kScAsmOrd);
-  PBGPU_CUDA(c, okey.alloc(n));
-  PBGPU_CUDA(c, okey2.alloc(n));
-  PBGPU_CUDA(c, oid.alloc(n));
-  PBGPU_CUDA(c, ord.alloc(n));
-  k_inc_count_keys<<<grid_for(n, 256), 256, 0, c->stream>>>(c->inc_ptr.get(), n, okey.get(), oid.get());
+  // local coefficients of every octant, once
+  Scratch<double> ocond(c, kScAsmCond), okd(c, kScAsmKd), ofr(c, kScAsmFr);
+  PBGPU_CUDA(c, ocond.alloc(12 * c->n_oct));
+  PBGPU_CUDA(c, okd.alloc(8 * c->n_oct));
+  PBGPU_CUDA(c, ofr.alloc(8 * c->n_oct));
+  k_octant_local<<<grid_for(c->n_oct, 128), 128, 0, c->stream>>>(A, c->n_oct, ocond.get(), okd.get(), ofr.get());
   PBGPU_LAUNCHED(c);
-  {
-    size_t ob = 0;
-    PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(nullptr, ob, okey.get(), okey2.get(), oid.get(), ord.get(), (int)n,
-                                                  0, 8, c->stream));
-    PBGPU_CUDA(c, ensure_tmp(c, ob));
-    PBGPU_CUDA(c, cub::DeviceRadixSort::SortPairs(c->tmp.get(), ob, okey.get(), okey2.get(), oid.get(), ord.get(),
-                                                  (int)n, 0, 8, c->stream));
-    c->launches += cub_radix_launches(n, 8);
-  }
-  Scratch<int32_t> ucols(c, kScAsmCols);
+  const LocalView L{ocond.get(), okd.get(), ofr.get()};
+  // pass 1: every row's columns and values into its lines (336 B per row,
+  // freed after pass 2).  A row longer than kMaxRow raises the flag, which
+  // is read with the matrix size below, before any row is written.
+  Scratch<int32_t> lcols(c, kScAsmCols);
+  Scratch<double> lvals(c, kScAsmVals), rpart(c, kScAsmRhs);
   Scratch<uint8_t> ucnt(c, kScAsmUcnt);
-  PBGPU_CUDA(c, ucols.alloc(n * kColLine));
+  PBGPU_CUDA(c, lcols.alloc(n * kLine));
+  PBGPU_CUDA(c, lvals.alloc(n * kLine));
+  PBGPU_CUDA(c, rpart.alloc(n));
   PBGPU_CUDA(c, ucnt.alloc(n));
-  // a row longer than kMaxRow keeps kMaxRow in rowlen and raises the flag,
-  // which is read with the matrix size below, before any row is filled
-  k_row_cols<<<grid_for(n, kAsmBlock), kAsmBlock, 0, c->stream>>>(A, ord.get(), asm_few_slots() ? kShFew : kShRow,
-                                                                  c->rowlen.get(), ucols.get(), ucnt.get(), ovf.get());
+  k_row_gather<kGatherNB><<<grid_for(n, kAsmBlock), kAsmBlock, 0, c->stream>>>(
+      A, L, asm_few_slots() ? kShFew : kLine, c->rowlen.get(), lcols.get(), lvals.get(), rpart.get(), ucnt.get(),
+      ovf.get());
   PBGPU_LAUNCHED(c);
 
   // SELL-C-sigma permutation
@@ -821,17 +712,11 @@ int run_assemble(Context* c, const pbgpu_sell_opts* o) {
   PBGPU_CUDA(c, c->dinv.alloc(n_pad));
   SellOut S{c->slice_ptr.get(), c->slice_w.get(), c->iperm.get(), c->perm.get(), c->scol.get(), c->sval.get(),
             c->b.get(), c->dinv.get(), C, G};
-  // local coefficients of every octant, once
-  Scratch<double> ocond(c, kScAsmCond), okd(c, kScAsmKd), ofr(c, kScAsmFr);
-  PBGPU_CUDA(c, ocond.alloc(12 * c->n_oct));
-  PBGPU_CUDA(c, okd.alloc(8 * c->n_oct));
-  PBGPU_CUDA(c, ofr.alloc(8 * c->n_oct));
-  k_octant_local<<<grid_for(c->n_oct, 128), 128, 0, c->stream>>>(A, c->n_oct, ocond.get(), okd.get(), ofr.get());
+  k_row_emit<false><<<grid_for(n, kAsmBlock), kAsmBlock, 0, c->stream>>>(A, L, S, lcols.get(), lvals.get(),
+                                                                          rpart.get(), ucnt.get());
   PBGPU_LAUNCHED(c);
-  const LocalView L{ocond.get(), okd.get(), ofr.get()};
-  k_row_fill<<<grid_for(n, kAsmBlock), kAsmBlock, 0, c->stream>>>(A, L, S, ucols.get(), ucnt.get());
-  PBGPU_LAUNCHED(c);
-  ucols.release();  // 128 B per row, needed by the fill alone (freed in stream order)
+  lcols.release();  // freed in stream order, after pass 2
+  lvals.release();
   if (n_pad > n) {
     k_pad_rows<<<grid_for(n_pad - n, 128), 128, 0, c->stream>>>(S, n, n_pad);
     PBGPU_LAUNCHED(c);
@@ -866,11 +751,23 @@ int run_rhs(Context* c) {
   k_octant_local<<<grid_for(c->n_oct, 128), 128, 0, c->stream>>>(A, c->n_oct, ocond.get(), okd.get(), ofr.get());
   PBGPU_LAUNCHED(c);
   const LocalView L{ocond.get(), okd.get(), ofr.get()};
-  if (asm_few_slots())
-    k_row_rhs<kShFew><<<grid_for(n, kAsmBlock), kAsmBlock, 0, c->stream>>>(A, L, S);
-  else
-    k_row_rhs<kShRow><<<grid_for(n, kAsmBlock), kAsmBlock, 0, c->stream>>>(A, L, S);
+  Scratch<int32_t> lcols(c, kScAsmCols);
+  Scratch<double> lvals(c, kScAsmVals), rpart(c, kScAsmRhs);
+  Scratch<uint8_t> ucnt(c, kScAsmUcnt);
+  Scratch<int> ovf(c, kScAsmOvf);
+  PBGPU_CUDA(c, lcols.alloc(n * kLine));
+  PBGPU_CUDA(c, lvals.alloc(n * kLine));
+  PBGPU_CUDA(c, rpart.alloc(n));
+  PBGPU_CUDA(c, ucnt.alloc(n));
+  PBGPU_CUDA(c, ovf.alloc(1));
+  k_row_gather<kGatherNB><<<grid_for(n, kAsmBlock), kAsmBlock, 0, c->stream>>>(
+      A, L, asm_few_slots() ? kShFew : kLine, nullptr, lcols.get(), lvals.get(), rpart.get(), ucnt.get(), ovf.get());
   PBGPU_LAUNCHED(c);
+  k_row_emit<true><<<grid_for(n, kAsmBlock), kAsmBlock, 0, c->stream>>>(A, L, S, lcols.get(), lvals.get(),
+                                                                         rpart.get(), ucnt.get());
+  PBGPU_LAUNCHED(c);
+  lcols.release();
+  lvals.release();
   return PBGPU_OK;
 }
 

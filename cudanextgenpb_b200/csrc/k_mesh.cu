@@ -619,15 +619,13 @@ __device__ bool touches_too_fine_part(const Tree& t, const int4 X, int r) {
   return false;
 }
 
-__device__ __forceinline__ void mark_once(uint8_t* marks, int64_t j, unsigned long long* nmark) {
-  // byte flags: mark once, count the first marker
+__device__ __forceinline__ void mark_once(uint8_t* marks, int64_t j) {
+  // byte flags set with a word-wide OR (other threads mark the neighbouring bytes)
   unsigned* word = reinterpret_cast<unsigned*>(marks + (j & ~int64_t(3)));
-  const unsigned bit = 1u << (8 * (j & 3));
-  if (!(atomicOr(word, bit) & bit)) atomicAdd(nmark, 1ull);
+  atomicOr(word, 1u << (8 * (j & 3)));
 }
 
-__global__ void k_balance_coarse(Tree t, const int4* __restrict__ seeds, int64_t ns, uint8_t* __restrict__ marks,
-                                 unsigned long long* __restrict__ nmark) {
+__global__ void k_balance_coarse(Tree t, const int4* __restrict__ seeds, int64_t ns, uint8_t* __restrict__ marks) {
   const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t s = gt / kBalLanes;
   const int r = (int)(gt % kBalLanes);
@@ -640,14 +638,13 @@ __global__ void k_balance_coarse(Tree t, const int4* __restrict__ seeds, int64_t
     const int32_t nx = P.x + dx * sz, ny = P.y + dy * sz, nz = P.z + dz * sz;
     if (!inside_root(nx, ny, nz)) continue;
     const int64_t j = containing_leaf_upto(t, nx, ny, nz, P.w - 1);
-    if (j >= 0) mark_once(marks, j, nmark);
+    if (j >= 0) mark_once(marks, j);
   }
 }
 
 // every lane of the grid reaches the group vote: the block size is a multiple
 // of 32 and kBalLanes divides 32, so groups never straddle warps
-__global__ void k_balance_fine(Tree t, const int4* __restrict__ seeds, int64_t ns, uint8_t* __restrict__ marks,
-                               unsigned long long* __restrict__ nmark) {
+__global__ void k_balance_fine(Tree t, const int4* __restrict__ seeds, int64_t ns, uint8_t* __restrict__ marks) {
   const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t s = gt / kBalLanes;
   const int r = (int)(gt % kBalLanes);
@@ -668,7 +665,7 @@ __global__ void k_balance_fine(Tree t, const int4* __restrict__ seeds, int64_t n
   const bool hit = active && touches_too_fine_part(t, X, r);
   const unsigned group = ((1u << kBalLanes) - 1u) << ((threadIdx.x & 31) & ~(kBalLanes - 1));
   const unsigned any = __ballot_sync(0xffffffffu, hit) & group;
-  if (any && r == 0) mark_once(marks, j, nmark);
+  if (any && r == 0) mark_once(marks, j);
 }
 
 __global__ void k_parent_of(int4* __restrict__ q, int64_t n) {
@@ -975,7 +972,6 @@ struct Builder {
   int64_t n = 0;
   DBuf<uint8_t> marks, hm, fam;
   DBuf<int64_t> cnt, off;
-  DBuf<unsigned long long> nmark;
   DBuf<int> bad;
 
   // table of the current leaves for exact-cell lookups (k_hanging), rebuilt
@@ -1032,8 +1028,9 @@ struct Builder {
     return PBGPU_OK;
   }
 
-  // sort + unique of m 64-bit keys in `k` (reordered in place); *nu unique
-  int sort_unique(DBuf<uint64_t>& k, int64_t m, int64_t* nu) {
+  // sort + unique of m keys in `k` (reordered in place) that use the low
+  // `bits` bits (40 for ray keys, 60 for Morton codes of node points); *nu unique
+  int sort_unique(DBuf<uint64_t>& k, int64_t m, int64_t* nu, int bits) {
     DBuf<uint64_t> k2;
     DBuf<int64_t> nsel;
     PBGPU_CUDA(c, k2.alloc(m > 0 ? m : 1));
@@ -1043,10 +1040,10 @@ struct Builder {
       return PBGPU_OK;
     }
     size_t bytes = 0;
-    PBGPU_CUDA(c, cub::DeviceRadixSort::SortKeys(nullptr, bytes, k.get(), k2.get(), (int)m, 0, 64, st()));
+    PBGPU_CUDA(c, cub::DeviceRadixSort::SortKeys(nullptr, bytes, k.get(), k2.get(), (int)m, 0, bits, st()));
     PBGPU_CUDA(c, ensure_tmp(c, bytes));
-    PBGPU_CUDA(c, cub::DeviceRadixSort::SortKeys(c->tmp.get(), bytes, k.get(), k2.get(), (int)m, 0, 64, st()));
-    c->launches += cub_radix_launches(m, 64);
+    PBGPU_CUDA(c, cub::DeviceRadixSort::SortKeys(c->tmp.get(), bytes, k.get(), k2.get(), (int)m, 0, bits, st()));
+    c->launches += cub_radix_launches(m, bits);
     bytes = 0;
     PBGPU_CUDA(c, cub::DeviceSelect::Unique(nullptr, bytes, k2.get(), k.get(), nsel.get(), (int)m, st()));
     PBGPU_CUDA(c, ensure_tmp(c, bytes));
@@ -1122,7 +1119,7 @@ struct Builder {
     k_zcol_fill<<<grid_for(n, 256), 256, 0, st()>>>(tree(), hm.get(), off.get(), zk.get());
     PBGPU_LAUNCHED(c);
     int64_t nu = 0;
-    if ((rc = sort_unique(zk, nzk, &nu)) != PBGPU_OK) return rc;
+    if ((rc = sort_unique(zk, nzk, &nu, kRayKeyBits)) != PBGPU_OK) return rc;
     DBuf<int64_t> coff;
     DBuf<double> inters;
     if ((rc = cast(zk.get(), nu, 2, coff, inters, nullptr)) != PBGPU_OK) return rc;
@@ -1141,6 +1138,10 @@ struct Builder {
     PBGPU_LAUNCHED(c);
     int64_t nn = 0;
     if ((rc = scan(n, &nn)) != PBGPU_OK) return rc;
+    if (nn == n) {  // nothing marked: the tree stays as it is
+      *np = 0;
+      return PBGPU_OK;
+    }
     DBuf<int64_t> nsel;
     PBGPU_CUDA(c, nsel.alloc(1));
     PBGPU_CUDA(c, parents.alloc(n > 0 ? n : 1));
@@ -1168,29 +1169,25 @@ struct Builder {
   // seeds (leaves that must not touch anything two levels finer)
   int balance(DBuf<int4>& coarse, int64_t nc, DBuf<int4>& fine, int64_t nf, bool fine_children) {
     int rc;
-    PBGPU_CUDA(c, nmark.alloc(1));
     for (int guard = 0; (nc > 0 || nf > 0) && guard < 64; ++guard) {
       PBGPU_CUDA(c, marks.alloc((n + 3) & ~int64_t(3)));
       PBGPU_CUDA(c, cudaMemsetAsync(marks.get(), 0, (n + 3) & ~int64_t(3), st()));
-      PBGPU_CUDA(c, cudaMemsetAsync(nmark.get(), 0, sizeof(unsigned long long), st()));
       // binary searches here: the table would be rebuilt after every pass of
       // the ripple, which measured slower than the searches it saves
       const Tree ht = tree();
       if (nc > 0) {
-        k_balance_coarse<<<grid_for(nc * kBalLanes, 128), 128, 0, st()>>>(ht, coarse.get(), nc, marks.get(),
-                                                                           nmark.get());
+        k_balance_coarse<<<grid_for(nc * kBalLanes, 128), 128, 0, st()>>>(ht, coarse.get(), nc, marks.get());
         PBGPU_LAUNCHED(c);
       }
       if (nf > 0) {
-        k_balance_fine<<<grid_for(nf * kBalLanes, 128), 128, 0, st()>>>(ht, fine.get(), nf, marks.get(), nmark.get());
+        k_balance_fine<<<grid_for(nf * kBalLanes, 128), 128, 0, st()>>>(ht, fine.get(), nf, marks.get());
         PBGPU_LAUNCHED(c);
       }
-      unsigned long long hm_ = 0;
-      PBGPU_CUDA(c, readback(c, &hm_, nmark.get(), sizeof(hm_)));
-      PBGPU_CUDA(c, cudaStreamSynchronize(st()));
-      if (hm_ == 0) return PBGPU_OK;
+      // the split's scan total is the only read of the pass: no split, no
+      // change, the ripple has settled
       int64_t np = 0;
       if ((rc = split(coarse, &np)) != PBGPU_OK) return rc;
+      if (np == 0) return PBGPU_OK;
       nc = np;
       nf = 0;
       if (fine_children) {
@@ -1375,11 +1372,12 @@ extern "C" int pbgpu_build_mesh(pbgpu_ctx* h, const pbgpu_mesh_build* in) {
   PBGPU_LAUNCHED(c);
   {
     size_t bytes = 0;
-    PBGPU_CUDA(c, cub::DeviceRadixSort::SortKeys(nullptr, bytes, codes.get(), codes2.get(), (int)ni, 0, 64, c->stream));
-    PBGPU_CUDA(c, ensure_tmp(c, bytes));
-    PBGPU_CUDA(c, cub::DeviceRadixSort::SortKeys(c->tmp.get(), bytes, codes.get(), codes2.get(), (int)ni, 0, 64,
+    PBGPU_CUDA(c, cub::DeviceRadixSort::SortKeys(nullptr, bytes, codes.get(), codes2.get(), (int)ni, 0, kMortonBits,
                                                  c->stream));
-    c->launches += cub_radix_launches(ni, 64);
+    PBGPU_CUDA(c, ensure_tmp(c, bytes));
+    PBGPU_CUDA(c, cub::DeviceRadixSort::SortKeys(c->tmp.get(), bytes, codes.get(), codes2.get(), (int)ni, 0,
+                                                 kMortonBits, c->stream));
+    c->launches += cub_radix_launches(ni, kMortonBits);
     std::swap(codes.p, codes2.p);
     std::swap(codes.n, codes2.n);
     std::swap(codes.acct, codes2.acct);
@@ -1393,7 +1391,7 @@ extern "C" int pbgpu_build_mesh(pbgpu_ctx* h, const pbgpu_mesh_build* in) {
   k_hang_fill<<<grid_for(no, 256), 256, 0, c->stream>>>(B.tree(), B.hm.get(), B.off.get(), hcodes.get());
   PBGPU_LAUNCHED(c);
   int64_t nh = 0;
-  if ((rc = B.sort_unique(hcodes, nhc, &nh)) != PBGPU_OK) return rc;
+  if ((rc = B.sort_unique(hcodes, nhc, &nh, kMortonBits)) != PBGPU_OK) return rc;
   if (ni + nh >= (int64_t(1) << 31)) return c->fail(PBGPU_ERR_CAPACITY, "build_mesh: too many nodes");
   PBGPU_CUDA(c, B.bad.alloc(1));
   PBGPU_CUDA(c, cudaMemsetAsync(B.bad.get(), 0, sizeof(int), c->stream));
@@ -1433,7 +1431,7 @@ extern "C" int pbgpu_build_mesh(pbgpu_ctx* h, const pbgpu_mesh_build* in) {
                                                                     rk.get());
     PBGPU_LAUNCHED(c);
     int64_t nk = 0;
-    if ((rc = B.sort_unique(rk, ni + nh, &nk)) != PBGPU_OK) return rc;
+    if ((rc = B.sort_unique(rk, ni + nh, &nk, kRayKeyBits)) != PBGPU_OK) return rc;
     Rays& R = c->rays[axis];
     DBuf<int64_t> coff;
     if ((rc = B.cast(rk.get(), nk, axis, coff, R.inters, &R.normals)) != PBGPU_OK) return rc;

@@ -185,7 +185,7 @@ enum ScratchSlot {
   kScMkOvf, kScMkFlags, kScMkSel, kScMkNsel,
   kScDenCnt, kScDenK0, kScDenK1, kScDenV0, kScDenV1,
   kScAsmOvf, kScAsmK0, kScAsmK1, kScAsmId0, kScAsmElems, kScAsmNnz, kScAsmCond, kScAsmKd, kScAsmFr,
-  kScAsmCols, kScAsmUcnt, kScAsmOrd, kScAsmOrdKey, kScAsmOrdKey2, kScAsmOrdId,
+  kScAsmCols, kScAsmVals, kScAsmRhs, kScAsmUcnt,
   kScKrBad, kScKrRh32, kScKrV32, kScKrS32, kScKrT32, kScKrPh32, kScKrSh32,
   kScEnPhi, kScEnQ, kScEnAcc, kScEnUsed, kScEnSlotRay, kScEnSel, kScEnNsel, kScEnNextra, kScEnXp, kScEnXd,
   kScEnP, kScEnD, kScEnXk, kScEnXk2, kScEnXi, kScEnXi2, kScPfAtoms, kScPfPart, kScPfOut,
@@ -421,6 +421,12 @@ __device__ __forceinline__ uint64_t spread3(uint64_t v) {
 __device__ __forceinline__ uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
   return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
 }
+
+// Point coordinates run 0 .. 2^kRootLog (kRootLog + 1 bits): a Morton code
+// of a point uses 3 (kRootLog + 1) bits, a ray key 2 (kRootLog + 1).
+constexpr int kMortonBits = 3 * (kRootLog + 1);
+constexpr int kRayKeyBits = 2 * (kRootLog + 1);
+static_assert(kRootLog + 1 <= 20, "ray keys hold 20 bits per coordinate");
 
 __device__ __forceinline__ uint64_t ray_key(int32_t a, int32_t b) {
   return ((uint64_t)(uint32_t)a << 20) | (uint64_t)(uint32_t)b;

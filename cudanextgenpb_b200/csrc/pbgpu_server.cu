@@ -178,7 +178,7 @@ int64_t pbgpu_request_bytes_estimate(const pbgpu_request* r) {
     const int levels = b->refine ? std::max(0, b->maxlevel - top) : 0;
     double no = (double)b->n_oct;
     for (int l = 0; l < levels; ++l) no *= 4.0;
-    return (int64_t)(980.0 * no + 1000.0 * (double)b->n_spheres) + ((int64_t)64 << 20);
+    return (int64_t)(1120.0 * no + 1000.0 * (double)b->n_spheres) + ((int64_t)64 << 20);
   }
   const double no = (double)r->mesh->n_oct, n = (double)r->mesh->n_nodes, nh = (double)r->mesh->n_hang;
   // mesh, incidence lists, per-octant local coefficients (assembly scratch),
@@ -186,11 +186,10 @@ int64_t pbgpu_request_bytes_estimate(const pbgpu_request* r) {
   // FP32), energy scratch; per unit of each size.  Measured on B200 after
   // set-up, a mixed-precision batch solve, energy and pot_field, contexts
   // held 810-860 B per octant (nodes ~0.7 and hanging nodes ~0.55 per
-  // octant) before the assembly's row ordering (10 B per node, kept) and
-  // column lines (128 B per node, freed after the assembly) were added; these
-  // coefficients give 980 B per octant, an upper bound that includes the
-  // lines.
-  return (int64_t)(500.0 * no + 660.0 * n + 40.0 * nh) + ((int64_t)64 << 20);
+  // octant) before the assembly kept 9 B per node more and, while it runs,
+  // 336 B per node of row lines (freed at its end); these coefficients give
+  // 1,120 B per octant, an upper bound that includes the lines.
+  return (int64_t)(500.0 * no + 850.0 * n + 40.0 * nh) + ((int64_t)64 << 20);
 }
 
 void pbgpu_default_server_opts(pbgpu_server_opts* o) {
