@@ -194,22 +194,17 @@ struct LocalView {
   const double* fr;
 };
 
-// The 3 edges at corner a in ascending edge id, with their axes.
+// The 3 edges at corner a in ascending edge id, with their axes: the z edge
+// (8-11) is always the last, the x and y edges (0-7) in either order.
 __device__ __forceinline__ void corner_edges(int a, int ed[3], int ax[3]) {
-  for (int d = 0; d < 3; ++d) {
-    ed[d] = edge_of(a, d);
-    ax[d] = d;
-  }
-  for (int u = 0; u < 3; ++u)
-    for (int v = u + 1; v < 3; ++v)
-      if (ed[v] < ed[u]) {
-        int tmp = ed[u];
-        ed[u] = ed[v];
-        ed[v] = tmp;
-        tmp = ax[u];
-        ax[u] = ax[v];
-        ax[v] = tmp;
-      }
+  const int e0 = edge_of(a, 0), e1 = edge_of(a, 1);
+  const bool sw = e1 < e0;
+  ed[0] = sw ? e1 : e0;
+  ax[0] = sw ? 1 : 0;
+  ed[1] = sw ? e0 : e1;
+  ax[1] = sw ? 0 : 1;
+  ed[2] = edge_of(a, 2);
+  ax[2] = 2;
 }
 
 // One incidence's loads: the corner's node and its 3 edge neighbours, the
@@ -220,9 +215,13 @@ struct IncLoads {
   double fr;
 };
 
+// t = 8 * octant + corner fits 32 bits (the incidence build checks 8 n_oct <
+// 2^32), so the corner entries of t's octant are t with its low 3 bits
+// replaced; the 12 conductances per octant need 64-bit offsets.
 __device__ __forceinline__ void load_inc(uint32_t t, const AsmView& A, const LocalView& L, IncLoads& d) {
-  const int64_t o = t >> 3;
   const int a = (int)(t & 7);
+  const uint32_t t0 = t & ~7u;
+  const int64_t c0 = (int64_t)(t >> 3) * 12;
   int ed[3], ax[3];
   corner_edges(a, ed, ax);
   d.nd[0] = A.oct_nodes[t];
@@ -230,8 +229,8 @@ __device__ __forceinline__ void load_inc(uint32_t t, const AsmView& A, const Loc
   d.fr = L.fr[t];
 #pragma unroll
   for (int u = 0; u < 3; ++u) {
-    d.nd[1 + u] = A.oct_nodes[8 * o + (a ^ (1 << ax[u]))];
-    d.k[1 + u] = 0.0 - L.cond[12 * o + ed[u]];
+    d.nd[1 + u] = A.oct_nodes[t0 | (uint32_t)(a ^ (1 << ax[u]))];
+    d.k[1 + u] = 0.0 - L.cond[c0 + ed[u]];
   }
 }
 

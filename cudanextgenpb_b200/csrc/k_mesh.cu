@@ -139,10 +139,54 @@ __global__ void k_tree_keys(int4* __restrict__ leaves, int64_t n, uint64_t* __re
   if (i < n) keys[i] = morton3(leaves[i].x, leaves[i].y, leaves[i].z);
 }
 
+// Are the 6 cells of `level` with lower corners (x[j], y[j], z[j]) leaves?  With
+// the tree's table, the first probes of all 6 are loaded before any is
+// resolved (a cell outside the root is not a leaf).
+__device__ __forceinline__ void leaves_at6(const Tree& t, const int32_t (&x)[6], const int32_t (&y)[6],
+                                           const int32_t (&z)[6], int level, bool (&out)[6]) {
+  if (!t.hk) {
+#pragma unroll
+    for (int j = 0; j < 6; ++j) out[j] = is_leaf_at(t, x[j], y[j], z[j], level);
+    return;
+  }
+  const uint64_t mask = (1ull << t.cap_log) - 1;
+  uint64_t key[6], slot[6], first[6];
+  bool in[6];
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    in[j] = inside_root(x[j], y[j], z[j]);
+    key[j] = leaf_hash_key(x[j], y[j], z[j], level);
+    slot[j] = hash_slot(key[j], t.cap_log);
+  }
+#pragma unroll
+  for (int j = 0; j < 6; ++j) first[j] = in[j] ? t.hk[slot[j]] : kEmptyKey;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    bool found = false;
+    if (in[j]) {
+      uint64_t k = first[j], s = slot[j];
+      for (uint64_t probe = 0; probe <= mask; ++probe) {
+        if (k == key[j]) {
+          found = true;
+          break;
+        }
+        if (k == kEmptyKey) break;
+        s = (s + 1) & mask;
+        k = t.hk[s];
+      }
+    }
+    out[j] = found;
+  }
+}
+
 // Hanging corners (host Octree::hanging_masks): corner c of leaf q (child k of
 // parent P) lies at a parent-edge midpoint when c ^ k has one bit set, at a
 // parent-face centre when it has two; it hangs when a level-(L-1) cell
-// sharing that edge (face) with P is a leaf.
+// sharing that edge (face) with P is a leaf.  Those cells lie on k's side of
+// P on every axis: the 3 across P's faces and the 3 across its edges next to
+// k.  A midpoint of P's edge along axis a hangs when the face cell across
+// either other axis, or the edge cell across both, is a leaf; a face centre
+// with normal axis a hangs when the face cell across a is.
 __global__ void k_hanging(Tree t, uint8_t* __restrict__ mask) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= t.n) return;
@@ -153,40 +197,40 @@ __global__ void k_hanging(Tree t, uint8_t* __restrict__ mask) {
   }
   const int L = q.w;
   const int32_t PS = 1 << (kRootLog - L + 1);
-  const int32_t Px = q.x & ~(PS - 1), Py = q.y & ~(PS - 1), Pz = q.z & ~(PS - 1);
-  int8_t nb[27];
-#pragma unroll
-  for (int u = 0; u < 27; ++u) nb[u] = -1;
-  auto nbr = [&](int dx, int dy, int dz) -> bool {
-    const int u = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
-    if (nb[u] < 0) nb[u] = is_leaf_at(t, Px + dx * PS, Py + dy * PS, Pz + dz * PS, L - 1) ? 1 : 0;
-    return nb[u] == 1;
-  };
+  const int32_t P[3] = {q.x & ~(PS - 1), q.y & ~(PS - 1), q.z & ~(PS - 1)};
   const int k = child_id(q);
+  int32_t off[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) off[a] = ((k >> a) & 1) ? PS : -PS;
+  // cells 0-2: across the face normal to axis a; 3-5: across the edge along axis a
+  int32_t cx[6], cy[6], cz[6];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    cx[a] = P[0] + (a == 0 ? off[0] : 0);
+    cy[a] = P[1] + (a == 1 ? off[1] : 0);
+    cz[a] = P[2] + (a == 2 ? off[2] : 0);
+    cx[3 + a] = P[0] + (a == 0 ? 0 : off[0]);
+    cy[3 + a] = P[1] + (a == 1 ? 0 : off[1]);
+    cz[3 + a] = P[2] + (a == 2 ? 0 : off[2]);
+  }
+  bool leaf[6];
+  leaves_at6(t, cx, cy, cz, L - 1, leaf);
+  unsigned bits = 0;  // bit j: cell j is a leaf
+#pragma unroll
+  for (int j = 0; j < 6; ++j) bits |= leaf[j] ? 1u << j : 0u;
   uint8_t m8 = 0;
+#pragma unroll
   for (int c = 0; c < 8; ++c) {
     const int m = c ^ k;
     const int pc = __popc(m);
-    if (pc == 0 || pc == 3) continue;
-    int side[3];
-    for (int a = 0; a < 3; ++a) side[a] = (((k >> a) & 1) + ((c >> a) & 1)) == 0 ? -1 : 1;
-    bool hang;
+    unsigned need = 0;  // the cells that make corner c hang
     if (pc == 1) {
       const int a = __ffs(m) - 1;
-      const int b = (a + 1) % 3, cc = (a + 2) % 3;
-      int d1[3] = {0, 0, 0}, d2[3] = {0, 0, 0}, d3[3] = {0, 0, 0};
-      d1[b] = side[b];
-      d2[cc] = side[cc];
-      d3[b] = side[b];
-      d3[cc] = side[cc];
-      hang = nbr(d1[0], d1[1], d1[2]) || nbr(d2[0], d2[1], d2[2]) || nbr(d3[0], d3[1], d3[2]);
-    } else {
-      const int nrm = __ffs(~m & 7) - 1;
-      int d[3] = {0, 0, 0};
-      d[nrm] = side[nrm];
-      hang = nbr(d[0], d[1], d[2]);
+      need = (1u << ((a + 1) % 3)) | (1u << ((a + 2) % 3)) | (1u << (3 + a));
+    } else if (pc == 2) {
+      need = 1u << (__ffs(~m & 7) - 1);
     }
-    if (hang) m8 |= (uint8_t)(1u << c);
+    if (bits & need) m8 |= (uint8_t)(1u << c);
   }
   mask[i] = m8;
 }

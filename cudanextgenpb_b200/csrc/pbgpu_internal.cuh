@@ -475,19 +475,13 @@ __device__ __constant__ static const int8_t d_edge_axis[12] = {0, 1, 0, 1, 0, 1,
 // Edges meeting at corner c: the edge along axis a is the one whose corner
 // pair is (c with bit a cleared, c with bit a set).
 __device__ __forceinline__ int edge_of(int c, int axis) {
-  // lower corner of the edge along `axis` through c
-  const int lowc = c & ~(1 << axis);
-  // edges along x: 0 (0-1), 2 (2-3), 4 (4-5), 6 (6-7)  -> by lowc>>1
-  // edges along y: 3 (0-2), 1 (1-3), 7 (4-6), 5 (5-7)
-  // edges along z: 8 (0-4), 9 (1-5), 11 (2-6), 10 (3-7)
-  if (axis == 0) return 2 * (lowc >> 1);
-  if (axis == 1) {
-    const int t = (lowc & 1) | ((lowc >> 2) << 1);  // (x bit, z bit)
-    const int tbl[4] = {3, 1, 7, 5};
-    return tbl[t];
-  }
-  const int tbl[4] = {8, 9, 11, 10};
-  return tbl[lowc & 3];
+  // edges along x: 0 (0-1), 2 (2-3), 4 (4-5), 6 (6-7): 2 * (c >> 1)
+  // edges along y: 3 (0-2), 1 (1-3), 7 (4-6), 5 (5-7): by the x and z bits
+  // edges along z: 8 (0-4), 9 (1-5), 11 (2-6), 10 (3-7): 8 + Gray code of (x, y)
+  if (axis == 0) return c & 6;
+  if (axis == 1) return 3 + 4 * ((c >> 2) & 1) - 2 * (c & 1);
+  const int t = c & 3;
+  return 8 + (t ^ (t >> 1));
 }
 
 __device__ __forceinline__ double wha(double e1, double e2, double f) { return 1.0 / (f / e1 + (1 - f) / e2); }
