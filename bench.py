@@ -892,11 +892,12 @@ def serve_stream(srv, reqs, arrivals=None):
 
 
 def spmv_roofline(local):
-    """The SpMV roofline on the 2,000-atom molecule at 2 surface levels (3.3 M
-    DoF, matrix > L2), plain FP64 CG solves with CUDA events around every SpMV
+    """The SpMV roofline on the 2,000-atom molecule at 3 surface levels (14.5 M
+    DoF, 161 M nonzeros, matrix far larger than L2: the single-molecule FP64
+    configuration), plain FP64 CG solves with CUDA events around every SpMV
     launch on the context's stream."""
     from cudanextgenpb_b200 import GpuPath, configs, solver_opts
-    na, rad, net, seed, scale, levels = WORKLOADS["mol2000l2"]
+    na, rad, net, seed, scale, levels = WORKLOADS["mol2000"]
     prob = configs.make_globular_problem(na, rad, net, seed, scale=scale, levels=levels)
     g = prob.build_on_gpu(GpuPath(local))
     g.create_markers()
@@ -923,7 +924,7 @@ def spmv_roofline(local):
             "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind_text(kind),
             "traffic": traffic, "algorithmic_bytes_per_launch": cnt["spmv_bytes"], "avg_launch_ms": avg,
             "launches_timed": cnt["spmv_launches"],
-            "workload": "2,000-atom molecule, 2 surface levels (%d DoF, nnz %d), plain FP64 Jacobi-CG, %d iterations "
+            "workload": "2,000-atom molecule, 3 surface levels (%d DoF, nnz %d), plain FP64 Jacobi-CG, %d iterations "
                         "per solve, 3 solves" % (g.n, nnz, st.iterations)}
 
 

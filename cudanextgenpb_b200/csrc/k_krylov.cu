@@ -260,7 +260,8 @@ __global__ void __launch_bounds__(kBlock, spmv_min_blocks<G>()) k_cg_spmv(SellT<
 
 template <typename T>
 __global__ void k_cg_update(int64_t n, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
-                            const T* __restrict__ q, const T* __restrict__ dinv, KrylovScalars* ks, double* partials) {
+                            const T* __restrict__ q, const T* __restrict__ dinv, KrylovScalars* ks, double* partials,
+                            int ru_ok) {
   if (ks->done) return;
   const T alpha = (T)ks->alpha;
   double v[3] = {0.0, 0.0, 0.0};
@@ -280,10 +281,10 @@ __global__ void k_cg_update(int64_t n, T* __restrict__ x, T* __restrict__ r, con
     if (!finite(v[0]) || !finite(v[1])) {
       ks->status = PBGPU_BREAKDOWN;
       ks->done = 1;
-    } else if (ks->reliable && (conv_met(ks, v[1], v[2]) || v[1] <= ks->delta2 * ks->rr_ref)) {
+    } else if (ks->reliable && ru_ok && (conv_met(ks, v[1], v[2]) || v[1] <= ks->delta2 * ks->rr_ref)) {
       ks->ru = 1;  // the FP64 residual (k_ru_residual) decides and supplies beta
-    } else if (conv_met(ks, v[1], v[2])) {
-      ks->done = 1;
+    } else if (!ks->reliable && conv_met(ks, v[1], v[2])) {
+      ks->done = 1;  // (with reliable updates only the FP64 residual ends the solve)
     } else if (ks->iter >= ks->max_iter) {
       ks->status = PBGPU_NOT_CONVERGED;
       ks->done = 1;
@@ -299,9 +300,19 @@ __global__ void k_cg_update(int64_t n, T* __restrict__ x, T* __restrict__ r, con
 // residual has fallen by delta since the last FP64 residual (or meets the
 // target), b - A (x + d) is computed in FP64 with the FP32 correction d, CG
 // continues from it keeping its search direction, and the p-update of the
-// same iteration folds d into x (x += d, d = 0), so the solve needs the
-// iterations of FP64 CG and one kernel per iteration more than it (the
-// residual, which returns at once unless an update is due).
+// same iteration folds d into x (x += d, d = 0).  The residual kernel runs on
+// every kRuPeriod-th iteration of a captured chunk and on its last one (it
+// returns at once unless an update is due); the updates in between may not
+// ask for one, so an update (and the FP64 check that ends the solve) comes at
+// most kRuPeriod - 1 iterations after its trigger, and the solve launches
+// about 3 + 1/kRuPeriod kernels per iteration.
+constexpr int kRuPeriod = 4;
+
+// Iteration k of a chunk of check_every runs the residual kernel: every
+// kRuPeriod-th, and the chunk's last one, so every chunk can end the solve.
+static inline bool ru_iteration(int k, int check_every) {
+  return k % kRuPeriod == kRuPeriod - 1 || k == check_every - 1;
+}
 
 // y_p = sum_j A(p, j) (x_j + d_j) in the order of sell_row, x_j + d_j formed
 // first (the value x_j takes once d is folded in)
@@ -1117,7 +1128,7 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
   int kernels_per_chunk = 0;
   for (int k = 0; k < check_every; ++k) {
     kernels_per_chunk += (method == PBGPU_CG ? 3 : method == PBGPU_CGS ? 4 : 5) + (bj ? (method == PBGPU_CG ? 1 : 2) : 0) +
-                         (K.x64 && method == PBGPU_CG ? 1 : 0);
+                         (K.x64 && method == PBGPU_CG && ru_iteration(k, check_every) ? 1 : 0);
     if (method == PBGPU_CG) {
       mark(k, 0, 0);
       if (tg)
@@ -1125,14 +1136,16 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
       else
         k_cg_spmv<T, GW><<<Gs, kBlock, 0, c->stream>>>(K.A, K.p, K.q, ks, part);
       mark(k, 0, 1);
-      k_cg_update<T><<<G, kBlock, 0, c->stream>>>(n, K.x, K.r, K.p, K.q, K.dinv, ks, part);
+      const bool ru_here = K.x64 && ru_iteration(k, check_every);
+      k_cg_update<T><<<G, kBlock, 0, c->stream>>>(n, K.x, K.r, K.p, K.q, K.dinv, ks, part, ru_here ? 1 : 0);
       bool folded = false;
       if constexpr (std::is_same<T, float>::value) {
         if (K.x64) {
           // the FP64 residual b - A (x + d) when an update is due, then the
           // p-update that also folds d into x
-          k_ru_residual<<<wave_grid(c, (const void*)k_ru_residual, K.A64->n_pad), kBlock, 0, c->stream>>>(
-              *K.A64, K.n_rows, K.b64, K.x64, K.x, K.r, K.dinv, ks, part);
+          if (ru_here)
+            k_ru_residual<<<wave_grid(c, (const void*)k_ru_residual, K.A64->n_pad), kBlock, 0, c->stream>>>(
+                *K.A64, K.n_rows, K.b64, K.x64, K.x, K.r, K.dinv, ks, part);
           k_cg_pupdate_fold<<<G, kBlock, 0, c->stream>>>(n, K.p, K.r, K.dinv, K.x64, K.x, ks);
           folded = true;
         }
