@@ -932,25 +932,41 @@ def peak_kind_text(kind):
     return "of measured (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else "of fallback"
 
 
-def oracle_serve_parity(pool, ids, e_plain, e_served):
+def oracle_serve_parity(pool, ids, e_plain, e_served, local, tol):
     """Energies of pool molecules `ids` from the CPU oracle (host-built mesh,
-    tight CG) against the plain FP64 and served energies of the same molecules."""
+    tight CG) against the plain FP64 and served energies of the same molecules,
+    and the potential at every node against the oracle's: of the plain FP64
+    path and of the served solver (FP32-inner / FP64-refined CG) on the mesh
+    built on the GPU (the host's nodes, in the host's order)."""
     from oracle_lib import Oracle
-    from cudanextgenpb_b200 import configs
-    out = {"molecules": [], "max_rel_err_plain": 0.0, "max_rel_err_served": 0.0}
+    from cudanextgenpb_b200 import GpuPath, configs, solver_opts
+    out = {"molecules": [], "max_rel_err_plain": 0.0, "max_rel_err_served": 0.0,
+           "max_phi_rel_l2_plain": 0.0, "max_phi_rel_l2_mixed": 0.0}
     for k in ids:
         na, rad, net, seed, lv = pool[k].spec
         prob = configs.make_globular_problem(na, rad, net, seed, scale=2.0, levels=lv).build()
         o = Oracle(prob)
-        oe, _, it, rel = o.run("cg", 1e-12)
+        oe, ophi, it, rel = o.run("cg", 1e-12)
         o.close()
         prob.close()
+        g = GpuPath(local)
+        plain_request(g, pool[k], solver_opts("cg", tol=tol, max_iter=50000))
+        phi64 = g.phi().copy()
+        g.solve(solver_opts("cg", tol=tol, max_iter=50000, precision="mixed", inner_tol=1e-4))
+        phim = g.phi().copy()
+        g.close()
+        nrm = np.linalg.norm(ophi)
+        dp = float(np.linalg.norm(phi64 - ophi) / nrm) if phi64.shape == ophi.shape else None
+        dm = float(np.linalg.norm(phim - ophi) / nrm) if phim.shape == ophi.shape else None
         ep = abs(e_plain[k] - oe["sum"]) / abs(oe["sum"])
         es = abs(e_served[k] - oe["sum"]) / abs(oe["sum"])
         out["molecules"].append({"atoms": na, "levels": lv, "oracle_kT": oe["sum"], "plain_kT": e_plain[k],
-                                 "served_kT": e_served[k], "rel_err_plain": ep, "rel_err_served": es})
+                                 "served_kT": e_served[k], "rel_err_plain": ep, "rel_err_served": es,
+                                 "phi_rel_l2_plain": dp, "phi_rel_l2_mixed": dm})
         out["max_rel_err_plain"] = max(out["max_rel_err_plain"], ep)
         out["max_rel_err_served"] = max(out["max_rel_err_served"], es)
+        for key, v in (("max_phi_rel_l2_plain", dp), ("max_phi_rel_l2_mixed", dm)):
+            out[key] = max(out[key], v) if v is not None and out[key] is not None else None
     return out
 
 
@@ -1089,7 +1105,7 @@ def run_serve(args, rank, world, local):
                     "and energy excluded from the bytes but not from the time"}
         # the oracle on the three smallest molecules the stream served (tight solve)
         served_ids = sorted(set(int(k) for k in timed), key=lambda k: pool[k].spec[0])[:3]
-        parity = oracle_serve_parity(pool, served_ids, e_plain, e_served)
+        parity = oracle_serve_parity(pool, served_ids, e_plain, e_served, local, args.tol)
         roof = spmv_roofline(local)
         n_dof = [0]
         result = {
