@@ -839,8 +839,29 @@ __global__ void k_node_xyz(const uint64_t* __restrict__ codes, int64_t n, int4* 
   xyz[j] = make_int4(p[0], p[1], p[2], flag);
 }
 
-__device__ __forceinline__ int64_t code_index(const uint64_t* __restrict__ codes, int64_t n, uint64_t k) {
-  return find_key(codes, n, k);
+// Index of each of K keys in the n sorted, distinct codes, or -1: K branch-free
+// binary searches in lockstep, so the K loads of every halving step are in
+// flight together.  The answer stays in [base, base + len): a step keeps the
+// upper part when its first code is <= the key, else the lower one.
+template <int K>
+__device__ __forceinline__ void code_index_k(const uint64_t* __restrict__ codes, int64_t n, const uint64_t (&key)[K],
+                                             int64_t (&idx)[K]) {
+  if (n <= 0) {
+#pragma unroll
+    for (int c = 0; c < K; ++c) idx[c] = -1;
+    return;
+  }
+  int64_t base[K];
+#pragma unroll
+  for (int c = 0; c < K; ++c) base[c] = 0;
+  for (int64_t len = n; len > 1;) {
+    const int64_t half = len >> 1;
+#pragma unroll
+    for (int c = 0; c < K; ++c) base[c] = codes[base[c] + half] <= key[c] ? base[c] + half : base[c];
+    len -= half;
+  }
+#pragma unroll
+  for (int c = 0; c < K; ++c) idx[c] = codes[base[c]] == key[c] ? base[c] : -1;
 }
 
 // corner node ids; for hanging corners also the parents (every leaf that
@@ -854,22 +875,35 @@ __global__ void k_corner_nodes(Tree t, const uint8_t* __restrict__ hm, const uin
   const int4 q = t.leaves[i];
   const int32_t s = qsize(q.w);
   const int k = q.w > 0 ? child_id(q) : 0;
+  const unsigned hang = hm[i];
+  uint64_t key[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) key[c] = morton3(q.x + (c & 1) * s, q.y + ((c >> 1) & 1) * s, q.z + ((c >> 2) & 1) * s);
+  int64_t ji[8], jh[8];
+  code_index_k<8>(codes, n_indep, key, ji);
+  if (hang) {
+    code_index_k<8>(hcodes, n_hang, key, jh);
+  } else {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) jh[c] = -1;
+  }
+#pragma unroll
   for (int c = 0; c < 8; ++c) {
-    const int32_t p[3] = {q.x + (c & 1) * s, q.y + ((c >> 1) & 1) * s, q.z + ((c >> 2) & 1) * s};
-    const uint64_t key = morton3(p[0], p[1], p[2]);
-    if (!(hm[i] >> c & 1)) {
-      const int64_t j = code_index(codes, n_indep, key);
-      if (j < 0) *bad = 1;
-      oct_nodes[8 * i + c] = (int32_t)j;
+    if (!(hang >> c & 1)) {
+      if (ji[c] < 0) *bad = 1;
+      oct_nodes[8 * i + c] = (int32_t)ji[c];
       continue;
     }
-    const int64_t h = code_index(hcodes, n_hang, key);
+    const int64_t h = jh[c];
     if (h < 0) *bad = 1;
     oct_nodes[8 * i + c] = (int32_t)(n_indep + h);
     const int32_t PS = 1 << (kRootLog - q.w + 1);
     const int32_t P[3] = {q.x & ~(PS - 1), q.y & ~(PS - 1), q.z & ~(PS - 1)};
     const int m = c ^ k;
-    int32_t par[4];
+    // the parent's corners on the hanging node's edge (2) or face (4), in
+    // corner order: those that agree with the hanging point on every axis
+    // where it sits on the parent's boundary
+    uint64_t pkey[4];
     int np = 0;
     for (int pc = 0; pc < 8; ++pc) {
       bool on = true;
@@ -879,10 +913,19 @@ __global__ void k_corner_nodes(Tree t, const uint8_t* __restrict__ hm, const uin
         if (((pc >> a) & 1) != want) on = false;
       }
       if (!on || np == 4) continue;
-      const int64_t j = code_index(codes, n_indep, morton3(P[0] + (pc & 1) * PS, P[1] + ((pc >> 1) & 1) * PS,
-                                                           P[2] + ((pc >> 2) & 1) * PS));
-      if (j < 0) *bad = 1;
-      par[np++] = (int32_t)j;
+      pkey[np++] = morton3(P[0] + (pc & 1) * PS, P[1] + ((pc >> 1) & 1) * PS, P[2] + ((pc >> 2) & 1) * PS);
+    }
+    if (np == 0) {  // not a hanging point of this leaf's parent
+      *bad = 1;
+      continue;
+    }
+    for (int u = np; u < 4; ++u) pkey[u] = pkey[0];
+    int64_t pj[4];
+    code_index_k<4>(codes, n_indep, pkey, pj);
+    int32_t par[4];
+    for (int u = 0; u < np; ++u) {
+      if (pj[u] < 0) *bad = 1;
+      par[u] = (int32_t)pj[u];
     }
     // ascending; padded with the first parent as pbgpu_set_mesh stores them
     for (int a = 1; a < np; ++a)
