@@ -1247,7 +1247,6 @@ struct Builder {
     k_split_fill<<<grid_for(n, 256), 256, 0, st()>>>(leaves.get(), marks.get(), n, off.get(), leaves2.get());
     PBGPU_LAUNCHED(c);
     leaves.swap(leaves2);
-    std::swap(leaves.acct, leaves2.acct);
     n = nn;
     return rekey();
   }
@@ -1359,9 +1358,7 @@ struct Builder {
       k_parent_of<<<grid_for(nm, 256), 256, 0, st()>>>(merged.get(), nm);
       PBGPU_LAUNCHED(c);
     }
-    std::swap(leaves.p, leaves2.p);
-    std::swap(leaves.n, leaves2.n);
-    std::swap(leaves.acct, leaves2.acct);
+    leaves.swap(leaves2);
     n = nn;
     if ((rc = rekey()) != PBGPU_OK) return rc;
     return balance(none, 0, merged, nm, true);
@@ -1384,7 +1381,7 @@ extern "C" int pbgpu_build_mesh(pbgpu_ctx* h, const pbgpu_mesh_build* in) {
   for (int a = 0; a < 3; ++a)
     if (!(in->hi[a] > in->lo[a])) return c->fail(PBGPU_ERR_ARG, "build_mesh: empty domain box");
   AcctScope acct(&c->dev_bytes);
-  StreamScope sscope(c->stream);
+  StreamScope sscope(c->stream, &c->blk_cache);
   if (cudaSetDevice(c->device) != cudaSuccess) return c->fail(PBGPU_ERR_CUDA, "build_mesh: cudaSetDevice");
   cudaGetLastError();
   c->have_mesh = c->have_markers = c->have_incidence = c->have_density = c->have_system = c->have_phi = false;
@@ -1465,9 +1462,7 @@ extern "C" int pbgpu_build_mesh(pbgpu_ctx* h, const pbgpu_mesh_build* in) {
     PBGPU_CUDA(c, cub::DeviceRadixSort::SortKeys(c->tmp.get(), bytes, codes.get(), codes2.get(), (int)ni, 0,
                                                  kMortonBits, c->stream));
     c->launches += cub_radix_launches(ni, kMortonBits);
-    std::swap(codes.p, codes2.p);
-    std::swap(codes.n, codes2.n);
-    std::swap(codes.acct, codes2.acct);
+    codes.swap(codes2);
   }
   if ((rc = B.ensure_counts(no)) != PBGPU_OK) return rc;
   k_hang_count<<<grid_for(no, 256), 256, 0, c->stream>>>(B.tree(), B.hm.get(), B.cnt.get());

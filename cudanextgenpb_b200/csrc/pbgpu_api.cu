@@ -135,7 +135,7 @@ using namespace pbgpu;
 // is set), so it is not blamed on this call's launches.
 #define SET_DEVICE(C)                                                                         \
   AcctScope _acct(&(C)->dev_bytes);                                                           \
-  StreamScope _sscope((C)->stream);                                                           \
+  StreamScope _sscope((C)->stream, &(C)->blk_cache);                                         \
   do {                                                                                        \
     cudaError_t _e = cudaSetDevice((C)->device);                                              \
     if (_e != cudaSuccess) return cuda_fail((C), _e, "cudaSetDevice");                        \
@@ -176,6 +176,8 @@ int pbgpu_ctx_create(pbgpu_ctx** out, int device, void* cuda_stream) {
     }
     c->own_stream = true;
   }
+  c->blk_cache.s = c->stream;
+  c->blk_cache.acct = &c->dev_bytes;
   if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
       cudaMallocHost(&c->ks_host, sizeof(KrylovScalars)) != cudaSuccess ||
       cudaMallocHost(&c->rb_host, kReadbackBytes) != cudaSuccess) {
@@ -197,6 +199,7 @@ void pbgpu_ctx_destroy(pbgpu_ctx* h) {
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ks_host) cudaFreeHost(c->ks_host);
   if (c->rb_host) cudaFreeHost(c->rb_host);
+  c->blk_cache.flush();  // the cached blocks back to the pool, on the context's stream
   delete h;  // DBuf destructors free device memory (pool buffers on the stream)
   if (st) cudaStreamSynchronize(st);
   if (own && st) cudaStreamDestroy(st);

@@ -44,16 +44,70 @@ struct AcctScope {
 inline thread_local cudaStream_t tl_stream = nullptr;
 inline thread_local bool tl_pooled = false;
 
+// Pool blocks a context's buffers released inside one of its API calls,
+// kept for reuse by later allocations of the same context on the same stream
+// instead of going back to the pool: the mesh build and the set-up allocate
+// and free hundreds of temporaries per request, and a pool allocation costs
+// microseconds (tens while several contexts allocate at once).  Reuse on the
+// stream the block was freed on is ordered as the pool's own reuse is.  A
+// cached block counts as freed in the context's byte count, as memory the
+// pool caches does; at most kMaxBytes are kept, and flush() returns them to
+// the pool (when the context is destroyed, or when an allocation finds the
+// device full).
+struct BlockCache {
+  struct Blk {
+    void* p;
+    size_t bytes;
+  };
+  static constexpr size_t kMaxBlocks = 512;
+  static constexpr size_t kMaxBytes = size_t(128) << 20;
+  cudaStream_t s = nullptr;  // the context's stream
+  int64_t* acct = nullptr;   // the context's byte count (identifies the owner)
+  std::vector<Blk> blks;
+  size_t bytes = 0;
+  // the smallest cached block of want .. 2 want (+ 64 KiB) bytes, or null
+  void* take(size_t want, size_t* got) {
+    int best = -1;
+    for (size_t i = 0; i < blks.size(); ++i)
+      if (blks[i].bytes >= want && blks[i].bytes <= 2 * want + 65536 &&
+          (best < 0 || blks[i].bytes < blks[best].bytes))
+        best = (int)i;
+    if (best < 0) return nullptr;
+    void* q = blks[best].p;
+    *got = blks[best].bytes;
+    bytes -= *got;
+    blks[best] = blks.back();
+    blks.pop_back();
+    return q;
+  }
+  bool put(void* q, size_t nb) {
+    if (blks.size() >= kMaxBlocks || bytes + nb > kMaxBytes) return false;
+    blks.push_back(Blk{q, nb});
+    bytes += nb;
+    return true;
+  }
+  void flush() {
+    for (const Blk& b : blks) cudaFreeAsync(b.p, s);
+    blks.clear();
+    bytes = 0;
+  }
+};
+inline thread_local BlockCache* tl_cache = nullptr;
+
 struct StreamScope {
   cudaStream_t prev;
   bool prev_pooled;
-  explicit StreamScope(cudaStream_t s) : prev(tl_stream), prev_pooled(tl_pooled) {
+  BlockCache* prev_cache;
+  explicit StreamScope(cudaStream_t s, BlockCache* cache = nullptr)
+      : prev(tl_stream), prev_pooled(tl_pooled), prev_cache(tl_cache) {
     tl_stream = s;
     tl_pooled = true;
+    tl_cache = cache;
   }
   ~StreamScope() {
     tl_stream = prev;
     tl_pooled = prev_pooled;
+    tl_cache = prev_cache;
   }
 };
 
@@ -78,6 +132,7 @@ template <typename T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0;
+  size_t nbytes = 0;  // the block's size (a cached block may exceed n * sizeof(T))
   int64_t* acct = nullptr;
   cudaStream_t s = nullptr;  // stream of a pool allocation
   bool pooled = false;
@@ -87,14 +142,19 @@ struct DBuf {
   ~DBuf() { release(); }
   void release() {
     if (p) {
-      if (pooled)
-        cudaFreeAsync(p, s);
-      else
-        cudaFree(p);
-      if (acct) *acct -= (int64_t)(n * sizeof(T));
+      const bool kept = pooled && acct && tl_cache && tl_cache->s == s && tl_cache->acct == acct &&
+                        tl_cache->put(p, nbytes);
+      if (!kept) {
+        if (pooled)
+          cudaFreeAsync(p, s);
+        else
+          cudaFree(p);
+      }
+      if (acct) *acct -= (int64_t)nbytes;
     }
     p = nullptr;
     n = 0;
+    nbytes = 0;
     acct = nullptr;
     s = nullptr;
     pooled = false;
@@ -107,7 +167,25 @@ struct DBuf {
     cudaError_t e;
     cudaMemPool_t pool = (tl_pooled && !stream_capturing(tl_stream)) ? device_pool() : nullptr;
     if (pool) {
+      BlockCache* bc = (tl_acct && tl_cache && tl_cache->s == tl_stream && tl_cache->acct == tl_acct) ? tl_cache : nullptr;
+      size_t got = 0;
+      void* q = bc ? bc->take(bytes, &got) : nullptr;
+      if (q) {
+        p = reinterpret_cast<T*>(q);
+        pooled = true;
+        s = tl_stream;
+        n = got / sizeof(T);
+        nbytes = got;
+        acct = tl_acct;
+        *acct += (int64_t)got;
+        return cudaSuccess;
+      }
       e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), bytes, pool, tl_stream);
+      if (e == cudaErrorMemoryAllocation && bc && bc->bytes) {  // the cache's blocks first
+        cudaGetLastError();
+        bc->flush();
+        e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), bytes, pool, tl_stream);
+      }
       if (e == cudaSuccess) {
         pooled = true;
         s = tl_stream;
@@ -122,6 +200,7 @@ struct DBuf {
     }
     if (e == cudaSuccess) {
       n = count;
+      nbytes = bytes;
       acct = tl_acct;
       if (acct) *acct += (int64_t)bytes;
     } else {
@@ -133,6 +212,7 @@ struct DBuf {
   void swap(DBuf& o) {
     std::swap(p, o.p);
     std::swap(n, o.n);
+    std::swap(nbytes, o.nbytes);
     std::swap(acct, o.acct);
     std::swap(s, o.s);
     std::swap(pooled, o.pooled);
@@ -223,6 +303,7 @@ struct Scratch {
 
 struct Context {
   int64_t dev_bytes = 0;     // device memory held by this context's buffers
+  BlockCache blk_cache;      // blocks its buffers released, for reuse on its stream
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
