@@ -1205,24 +1205,43 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
   int rc = PBGPU_OK;
   const int max_chunks = max_iter / check_every + 2;
   int prev_iter = 0;
-  for (int chunk = 0; chunk < max_chunks; ++chunk) {
-    ce = cudaGraphLaunch(exec, c->stream);
-    if (ce == cudaSuccess)
-      ce = cudaMemcpyAsync(c->ks_host, ks, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, c->stream);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(c->stream);
-    if (ce != cudaSuccess) {
-      rc = cuda_fail(c, ce, "krylov chunk");
-      break;
+  // Chunk j leaves its scalars in the pinned slot ks_host[j % 2] and marks
+  // them with event evc[j % 2].  The next chunk is launched before the host
+  // waits for the current one, so the stream does not idle while the host
+  // reads a chunk's scalars and launches the graph again; a chunk launched
+  // after the solve ended does nothing (every kernel returns at once once
+  // ks->done is set, and none of them changes the scalars then).  With
+  // profiling on, each chunk is waited for before the next is launched: the
+  // chunks share the SpMV timing events.
+  const bool ahead = !c->profiling;
+  auto launch_chunk = [&](int j) -> cudaError_t {
+    cudaError_t e = cudaGraphLaunch(exec, c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(c->ks_host + (j & 1), ks, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c->evc[j & 1], c->stream);
+    return e;
+  };
+  int launched = 0;
+  const KrylovScalars* h = c->ks_host;
+  ce = launch_chunk(0);
+  if (ce == cudaSuccess) launched = 1;
+  for (int chunk = 0; ce == cudaSuccess && chunk < max_chunks; ++chunk) {
+    if (ahead && launched < max_chunks) {
+      ce = launch_chunk(launched);
+      if (ce != cudaSuccess) break;
+      ++launched;
     }
-    c->launches += kernels_per_chunk;
-    const int now = c->ks_host->iter;
+    ce = cudaEventSynchronize(c->evc[chunk & 1]);
+    if (ce != cudaSuccess) break;
+    h = c->ks_host + (chunk & 1);
+    const int now = h->iter;
     if (c->profiling) {
       // iteration k of this chunk did its SpMV(s) when it is below the count
       // of completed iterations; the t-SpMV of a BiCGStab iteration that
       // stopped on ||s|| did not run
       for (int k = 0; k < check_every && prev_iter + k < now; ++k)
         for (int w = 0; w < spmv_per_it; ++w) {
-          if (w == 1 && prev_iter + k == now - 1 && c->ks_host->s_conv) continue;
+          if (w == 1 && prev_iter + k == now - 1 && h->s_conv) continue;
           float ms = 0.f;
           if (cudaEventElapsedTime(&ms, ev[2 * (k * spmv_per_it + w)], ev[2 * (k * spmv_per_it + w) + 1]) ==
               cudaSuccess) {
@@ -1234,8 +1253,19 @@ static int krylov_g(Context* c, int method, const KrylovVecs<T>& K, ConvRule cr,
         }
     }
     prev_iter = now;
-    if (c->ks_host->done) break;
+    if (h->done) break;
+    if (!ahead && launched < max_chunks) {
+      ce = launch_chunk(launched);
+      if (ce != cudaSuccess) break;
+      ++launched;
+    }
   }
+  // the chunk launched past the last one waited for (its kernels return at once)
+  const cudaError_t e_drain = cudaStreamSynchronize(c->stream);
+  if (ce == cudaSuccess) ce = e_drain;
+  if (ce != cudaSuccess) rc = cuda_fail(c, ce, "krylov chunk");
+  c->launches += (int64_t)kernels_per_chunk * launched;
+  if (h != c->ks_host) std::memcpy(c->ks_host, h, sizeof(KrylovScalars));
   const cudaError_t e_exec = cudaGraphExecDestroy(exec);
   const cudaError_t e_graph = cudaGraphDestroy(graph);
   cudaError_t e_ev = cudaSuccess;

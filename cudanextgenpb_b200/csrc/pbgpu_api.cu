@@ -179,7 +179,9 @@ int pbgpu_ctx_create(pbgpu_ctx** out, int device, void* cuda_stream) {
   c->blk_cache.s = c->stream;
   c->blk_cache.acct = &c->dev_bytes;
   if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaMallocHost(&c->ks_host, sizeof(KrylovScalars)) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->evc[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->evc[1], cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost(&c->ks_host, 2 * sizeof(KrylovScalars)) != cudaSuccess ||
       cudaMallocHost(&c->rb_host, kReadbackBytes) != cudaSuccess) {
     pbgpu_ctx_destroy(h);
     return PBGPU_ERR_CUDA;
@@ -197,6 +199,8 @@ void pbgpu_ctx_destroy(pbgpu_ctx* h) {
   if (st) cudaStreamSynchronize(st);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  for (cudaEvent_t e : c->evc)
+    if (e) cudaEventDestroy(e);
   if (c->ks_host) cudaFreeHost(c->ks_host);
   if (c->rb_host) cudaFreeHost(c->rb_host);
   c->blk_cache.flush();  // the cached blocks back to the pool, on the context's stream

@@ -309,6 +309,7 @@ struct Context {
   bool own_stream = false;
   std::string err;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t evc[2] = {nullptr, nullptr};  // ends of the two Krylov chunks in flight
   double stage_ms[6] = {0, 0, 0, 0, 0, 0};
 
   // ---- mesh
